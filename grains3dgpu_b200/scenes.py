@@ -1,0 +1,411 @@
+"""Seeded synthetic packings of the benchmark configurations.
+
+Each generator returns a :class:`Scene`: the construction data that
+Grains::Construction would read from XML (Grains/Base/src/Grains.cpp:90-300)
+as plain arrays -- rigid bodies, per-particle rigid-body ids, transforms,
+velocities, obstacles (closed-box walls as Rectangle obstacles, the shape the
+reference uses for planar walls) and the contact-model table.
+
+All random draws come from one ``numpy.random.Generator(PCG64(seed))`` in a
+fixed order: shapes, centres, jitter, orientations, velocities.
+"""
+import dataclasses
+
+import numpy as np
+
+from . import abi
+
+# numpy views of the C structs (same field order, natural alignment)
+RB_DTYPE = np.dtype([("type", "<i4"), ("n_vertices", "<i4"), ("first_vertex", "<i8"),
+                     ("p", "<f8", (5,)), ("crust", "<f8"), ("density", "<f8"),
+                     ("material", "<i4"), ("reserved", "<i4")], align=True)
+assert RB_DTYPE.itemsize == abi.C.sizeof(abi.RigidBodyDesc)
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    config: dict
+    rbs: np.ndarray          # RB_DTYPE[n_rigid_bodies]
+    vertices: np.ndarray     # float64 [n_vertices, 3]
+    rb_ids: np.ndarray       # uint32 [N]
+    transforms: np.ndarray   # float64 [N, 12]
+    velocities: np.ndarray   # float64 [N, 6]
+    obstacles: np.ndarray    # RB_DTYPE[n_obstacles]
+    obstacle_transforms: np.ndarray  # float64 [n_obstacles, 12]
+    contact_models: list     # dicts, l(l+1)/2+s indexed
+    notes: str = ""
+
+    @property
+    def n(self):
+        return int(self.rb_ids.shape[0])
+
+    def make_config(self, **overrides):
+        kw = dict(self.config)
+        kw.update(overrides)
+        return abi.make_config(**kw)
+
+    def subset(self, idx):
+        """The particles `idx` (and their rigid bodies) as a scene of its own."""
+        idx = np.asarray(idx)
+        rb_used = np.unique(self.rb_ids[idx])
+        remap = np.full(self.rbs.shape[0], -1, np.int64)
+        remap[rb_used] = np.arange(rb_used.size)
+        rbs = self.rbs[rb_used].copy()
+        verts = self.vertices
+        if verts.shape[0]:
+            chunks, off = [], 0
+            for r in rbs:
+                if r["type"] == abi.GB_POLYHEDRON:
+                    s = int(r["first_vertex"])
+                    chunks.append(verts[s:s + int(r["n_vertices"])])
+                    r["first_vertex"] = off
+                    off += int(r["n_vertices"])
+            verts = np.concatenate(chunks) if chunks else np.zeros((0, 3))
+        cfg = dict(self.config)
+        cfg["n_particles"] = int(idx.size)
+        cfg["n_rigid_bodies"] = int(rb_used.size)
+        return Scene(self.name + "-subset", cfg, rbs, np.ascontiguousarray(verts),
+                     remap[self.rb_ids[idx]].astype(np.uint32),
+                     self.transforms[idx].copy(), self.velocities[idx].copy(),
+                     self.obstacles, self.obstacle_transforms, self.contact_models,
+                     self.notes)
+
+
+# ---------------------------------------------------------------------------
+def random_rotations(rng, n):
+    """Uniform random rotation matrices (row-major, 9 each) from unit quaternions."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return quat_to_matrix(q)
+
+
+def quat_to_matrix(q):
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    m = np.empty((q.shape[0], 9))
+    m[:, 0] = 1 - 2 * (y * y + z * z)
+    m[:, 1] = 2 * (x * y - w * z)
+    m[:, 2] = 2 * (x * z + w * y)
+    m[:, 3] = 2 * (x * y + w * z)
+    m[:, 4] = 1 - 2 * (x * x + z * z)
+    m[:, 5] = 2 * (y * z - w * x)
+    m[:, 6] = 2 * (x * z - w * y)
+    m[:, 7] = 2 * (y * z + w * x)
+    m[:, 8] = 1 - 2 * (x * x + y * y)
+    return m
+
+
+def lattice(box, pitch, margin, n, rng, jitter):
+    """n jittered cubic-lattice sites filling `box` layer by layer from z=0."""
+    counts = [int(np.floor((box[k] - 2 * margin) / pitch)) + 1 for k in range(3)]
+    cap = counts[0] * counts[1] * counts[2]
+    if cap < n:
+        raise ValueError(f"lattice holds {cap} sites < {n}")
+    k = np.arange(n)
+    ix = k % counts[0]
+    iy = (k // counts[0]) % counts[1]
+    iz = k // (counts[0] * counts[1])
+    pos = np.stack([margin + ix * pitch, margin + iy * pitch, margin + iz * pitch], 1)
+    pos += rng.uniform(-jitter, jitter, size=pos.shape)
+    return pos, counts
+
+
+def box_walls(box, material=1):
+    """Six Rectangle obstacles (density 0) bounding [0, box]; each normal
+    (the rectangle frame's z axis) points into the box."""
+    L = box
+    descs = np.zeros(6, RB_DTYPE)
+    trs = np.zeros((6, 12))
+    # (normal axis, side): basis columns chosen so that column 2 = inward normal
+    frames = [
+        ([[0, 0, 1], [0, 1, 0], [-1, 0, 0]], [0, L[1] / 2, L[2] / 2], (L[2], L[1])),   # x=0, n=+x
+        ([[0, 0, -1], [0, 1, 0], [1, 0, 0]], [L[0], L[1] / 2, L[2] / 2], (L[2], L[1])),  # x=L, n=-x
+        ([[1, 0, 0], [0, 0, 1], [0, -1, 0]], [L[0] / 2, 0, L[2] / 2], (L[0], L[2])),   # y=0, n=+y
+        ([[1, 0, 0], [0, 0, -1], [0, 1, 0]], [L[0] / 2, L[1], L[2] / 2], (L[0], L[2])),  # y=L, n=-y
+        ([[1, 0, 0], [0, 1, 0], [0, 0, 1]], [L[0] / 2, L[1] / 2, 0], (L[0], L[1])),    # z=0, n=+z
+        ([[1, 0, 0], [0, -1, 0], [0, 0, -1]], [L[0] / 2, L[1] / 2, L[2]], (L[0], L[1])),  # z=L, n=-z
+    ]
+    for i, (b, o, (lx, ly)) in enumerate(frames):
+        descs[i]["type"] = abi.GB_RECTANGLE
+        descs[i]["p"][:2] = [lx / 2, ly / 2]
+        descs[i]["material"] = material
+        trs[i, :9] = np.array(b, float).ravel()
+        trs[i, 9:] = o
+    return descs, trs
+
+
+def law(kn=1e4, en=0.7, muc=0.5, etat=0.0, kr=0.0, kt_ratio=0.8):
+    return dict(kn=kn, en=en, etat=etat, muc=muc, kr=kr, kt=kt_ratio * kn)
+
+
+def superquadric_semi_axes(r_eq, ba, ca, n1, n2):
+    """Semi-axis a such that the superquadric of axes (a, ba*a, ca*a) and
+    exponents (n1, n2) has the volume of a sphere of radius r_eq (volume
+    formula of Superquadric::computeVolume, Superquadric.cpp:81-90)."""
+    from math import gamma
+    e1, e2 = 2.0 / n1, 2.0 / n2
+    beta = lambda x, y: gamma(x) * gamma(y) / gamma(x + y)
+    unit = 2.0 / 3.0 * e1 * e2 * beta(e1, 0.5 * e1) * beta(0.5 * e2, 0.5 * e2)
+    v = 4.0 / 3.0 * np.pi * r_eq ** 3
+    return (v / (unit * ba * ca)) ** (1.0 / 3.0)
+
+
+# ---------------------------------------------------------------------------
+def config0(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000):
+    """2,000 identical superquadrics a=b=c=1 mm, n1=n2=4, on a 2.4 mm jittered
+    lattice (+-0.15 mm) with random orientations, in a closed box.  The box
+    is raised from 60 to 80 mm because 2,000 sites at 2.4 mm pitch do not fit
+    in 20x20x60 mm; crust = 5% of the semi-axis."""
+    rng = np.random.default_rng(seed)
+    rbs = np.zeros(1, RB_DTYPE)
+    rbs[0]["type"] = abi.GB_SUPERQUADRIC
+    rbs[0]["p"] = [1e-3, 1e-3, 1e-3, 4.0, 4.0]
+    rbs[0]["crust"] = 5e-5
+    rbs[0]["density"] = 2500.0
+    pos, _ = lattice(box, pitch, 1.6e-3, n, rng, 0.15e-3)
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = pos
+    walls, wtr = box_walls(box)
+    cfg = dict(n_particles=n, n_rigid_bodies=1, n_obstacles=6, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=2e-6, gravity=(0, 0, -9.81))
+    return Scene("config0", cfg, rbs, np.zeros((0, 3)), np.zeros(n, np.uint32), tr,
+                 np.zeros((n, 6)), walls, wtr, [law()] * 3,
+                 notes=f"box raised to {box[2]*1e3:.0f} mm; {steps} steps nominal")
+
+
+def ellipsoid_points(rng, axes, k):
+    """k points uniform in area on the ellipsoid of semi-axes `axes`
+    (rejection on the area-element factor of the sphere-to-ellipsoid map)."""
+    a, b, c = axes
+    gmax = max(b * c, a * c, a * b)
+    out = []
+    while len(out) < k:
+        u = rng.normal(size=(4 * k, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        g = np.sqrt((b * c * u[:, 0]) ** 2 + (a * c * u[:, 1]) ** 2 + (a * b * u[:, 2]) ** 2)
+        keep = rng.uniform(size=u.shape[0]) * gmax < g
+        out.extend(list(u[keep] * np.array(axes)))
+    return np.array(out[:k])
+
+
+def config1(seed=1, n=200_000, box=(0.100, 0.100, 0.400), pitch=2.6e-3,
+            hull_centroid=None):
+    """Convex polyhedra: each the hull of 8-32 points uniform on an ellipsoid
+    of semi-axes 1 mm x U(0.6,1.4) x U(0.6,1.4) mm, re-centred on the hull
+    centroid, on a 2.6 mm jittered lattice (+-0.1 mm) in a closed box."""
+    rng = np.random.default_rng(seed)
+    nv = rng.integers(8, 33, size=n)
+    axes = np.stack([np.full(n, 1e-3), rng.uniform(0.6e-3, 1.4e-3, n),
+                     rng.uniform(0.6e-3, 1.4e-3, n)], 1)
+    first = np.concatenate([[0], np.cumsum(nv)[:-1]])
+    verts = np.zeros((int(nv.sum()), 3))
+    for i in range(n):
+        verts[first[i]:first[i] + nv[i]] = ellipsoid_points(rng, axes[i], int(nv[i]))
+    if hull_centroid is not None:
+        for i in range(n):
+            sl = slice(first[i], first[i] + nv[i])
+            verts[sl] -= hull_centroid(verts[sl])
+    rbs = np.zeros(n, RB_DTYPE)
+    rbs["type"] = abi.GB_POLYHEDRON
+    rbs["n_vertices"] = nv
+    rbs["first_vertex"] = first
+    rbs["crust"] = 5e-5
+    rbs["density"] = 2500.0
+    pos, _ = lattice(box, pitch, 1.6e-3, n, rng, 0.1e-3)
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = pos
+    walls, wtr = box_walls(box)
+    cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
+    return Scene("config1", cfg, rbs, verts, np.arange(n, dtype=np.uint32), tr,
+                 np.zeros((n, 6)), walls, wtr, [law()] * 3)
+
+
+def config2(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
+    """Polydisperse superquadrics: r_eq lognormal (median 1 mm, sigma 0.25)
+    clipped to [0.5, 2] mm, b/a and c/a ~ U(0.5, 2), n1, n2 ~ U(2, 10), on the
+    densest jittered cubic lattice that holds n sites in the box."""
+    rng = np.random.default_rng(seed)
+    r_eq = np.clip(1e-3 * np.exp(rng.normal(0.0, 0.25, n)), 0.5e-3, 2e-3)
+    ba = rng.uniform(0.5, 2.0, n)
+    ca = rng.uniform(0.5, 2.0, n)
+    n1 = rng.uniform(2.0, 10.0, n)
+    n2 = rng.uniform(2.0, 10.0, n)
+    a = np.array([superquadric_semi_axes(r_eq[i], ba[i], ca[i], n1[i], n2[i])
+                  for i in range(n)]) if n < 50_000 else _sq_axes_vec(r_eq, ba, ca, n1, n2)
+    rbs = np.zeros(n, RB_DTYPE)
+    rbs["type"] = abi.GB_SUPERQUADRIC
+    rbs["p"] = np.stack([a, ba * a, ca * a, n1, n2], 1)
+    rbs["crust"] = 0.05 * np.minimum(a, np.minimum(ba * a, ca * a))
+    rbs["density"] = 2500.0
+    margin = 2.5e-3
+    if pitch is None:
+        vol = np.prod([box[k] - 2 * margin for k in range(3)])
+        pitch = (vol / n) ** (1 / 3)
+        while True:
+            cnt = [int(np.floor((box[k] - 2 * margin) / pitch)) + 1 for k in range(3)]
+            if cnt[0] * cnt[1] * cnt[2] >= n:
+                break
+            pitch *= 0.995
+    pos, _ = lattice(box, pitch, margin, n, rng, 0.05 * pitch)
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = pos
+    walls, wtr = box_walls(box)
+    cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
+    return Scene("config2", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
+                 tr, np.zeros((n, 6)), walls, wtr, [law()] * 3,
+                 notes=f"lattice pitch {pitch*1e3:.3f} mm")
+
+
+def _sq_axes_vec(r_eq, ba, ca, n1, n2):
+    from scipy.special import gamma
+    e1, e2 = 2.0 / n1, 2.0 / n2
+    beta = lambda x, y: gamma(x) * gamma(y) / gamma(x + y)
+    unit = 2.0 / 3.0 * e1 * e2 * beta(e1, 0.5 * e1) * beta(0.5 * e2, 0.5 * e2)
+    v = 4.0 / 3.0 * np.pi * r_eq ** 3
+    return (v / (unit * ba * ca)) ** (1.0 / 3.0)
+
+
+def config3(seed=3, n=10_000, column_height=None):
+    """Superquadrics with n1, n2 ~ U(2, 8) and semi-axes ~ U(0.8, 1.2) mm in a
+    column resting on a plate (its bottom layer within crust range of the
+    plate, so contacts exist within the 2,000-step window); initial
+    velocities N(0, 0.05 m/s) per component."""
+    rng = np.random.default_rng(seed)
+    axes = rng.uniform(0.8e-3, 1.2e-3, size=(n, 3))
+    ns = rng.uniform(2.0, 8.0, size=(n, 2))
+    rbs = np.zeros(n, RB_DTYPE)
+    rbs["type"] = abi.GB_SUPERQUADRIC
+    rbs["p"] = np.concatenate([axes, ns], 1)
+    rbs["crust"] = 0.05 * axes.min(1)
+    rbs["density"] = 2500.0
+    side = int(np.ceil(np.sqrt(n / 40)))
+    pitch = 2.6e-3
+    box = (side * pitch + 2e-3, side * pitch + 2e-3, 0.2)
+    pos, _ = lattice(box, pitch, 1.0e-3 + 0.5 * pitch - 1.2e-3, n, rng, 0.1e-3)
+    pos[:, 2] += 1.2e-3 - pos[:, 2].min() + 2e-5
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = pos
+    vel = np.zeros((n, 6))
+    vel[:, :3] = rng.normal(0.0, 0.05, size=(n, 3))
+    walls, wtr = box_walls(box)
+    cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=2e-6, gravity=(0, 0, -9.81))
+    return Scene("config3", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
+                 tr, vel, walls, wtr, [law()] * 3)
+
+
+# ---------------------------------------------------------------------------
+class System:
+    """Applies a Scene to one engine library bound by abi.Bound (gb_, or_ or
+    ref_ prefix) and exposes the hot-path calls with numpy in/out."""
+
+    def __init__(self, lib, scene, **config_overrides):
+        self.lib = lib
+        self.scene = scene
+        self.cfg = scene.make_config(**config_overrides)
+        st = abi.C.c_int32(0)
+        self.ctx = lib.create(abi.C.byref(self.cfg), abi.C.byref(st))
+        if not self.ctx:
+            raise RuntimeError(f"{lib.prefix}create failed: {st.value}")
+        rbs = np.ascontiguousarray(scene.rbs)
+        verts = np.ascontiguousarray(scene.vertices, dtype=np.float64)
+        self._check(lib.set_rigid_bodies(
+            self.ctx, rbs.ctypes.data_as(abi.C.POINTER(abi.RigidBodyDesc)),
+            abi.dptr(verts) if verts.size else None, verts.shape[0]), "set_rigid_bodies")
+        cms = abi.contact_model_array(scene.contact_models)
+        self._check(lib.set_contact_models(self.ctx, cms), "set_contact_models")
+        if self.cfg.n_obstacles:
+            ob = np.ascontiguousarray(scene.obstacles)
+            self._check(lib.set_obstacles(
+                self.ctx, ob.ctypes.data_as(abi.C.POINTER(abi.RigidBodyDesc)),
+                abi.dptr(np.ascontiguousarray(scene.obstacle_transforms))), "set_obstacles")
+        self._check(lib.set_rigid_body_ids(self.ctx, abi.u32ptr(np.ascontiguousarray(scene.rb_ids))),
+                    "set_rigid_body_ids")
+        self.set_transforms(scene.transforms)
+        self.set_velocities(scene.velocities)
+
+    def _check(self, st, what):
+        if st not in (abi.GB_OK, abi.GB_E_OUT_OF_DOMAIN):
+            raise RuntimeError(f"{self.lib.prefix}{what} returned {st}")
+        return st
+
+    @property
+    def n(self):
+        return self.cfg.n_particles
+
+    def set_transforms(self, tr):
+        self._check(self.lib.set_transforms(self.ctx, abi.dptr(np.ascontiguousarray(tr, np.float64))),
+                    "set_transforms")
+
+    def set_velocities(self, kin):
+        self._check(self.lib.set_velocities(self.ctx, abi.dptr(np.ascontiguousarray(kin, np.float64))),
+                    "set_velocities")
+
+    def transforms(self):
+        out = np.zeros((self.n, 12))
+        self._check(self.lib.get_transforms(self.ctx, abi.dptr(out)), "get_transforms")
+        return out
+
+    def velocities(self):
+        out = np.zeros((self.n, 6))
+        self._check(self.lib.get_velocities(self.ctx, abi.dptr(out)), "get_velocities")
+        return out
+
+    def torces(self):
+        out = np.zeros((self.n, 6))
+        self._check(self.lib.get_torces(self.ctx, abi.dptr(out)), "get_torces")
+        return out
+
+    def rb_props(self, i):
+        p = abi.RigidBodyProps()
+        self._check(self.lib.get_rigid_body_props(self.ctx, i, abi.C.byref(p)), "get_rigid_body_props")
+        return p
+
+    def detect(self, result=None):
+        return self._check(self.lib.detect_collision_and_compute_contact_forces(
+            self.ctx, abi.i32ptr(result)), "detect")
+
+    def add_external_forces(self):
+        return self._check(self.lib.add_external_forces(self.ctx), "add_external_forces")
+
+    def move(self):
+        return self._check(self.lib.move_particles(self.ctx), "move_particles")
+
+    def step(self, n=1):
+        return self._check(self.lib.step(self.ctx, n), "step")
+
+    def stats(self):
+        s = abi.Stats()
+        self._check(self.lib.get_stats(self.ctx, abi.C.byref(s)), "get_stats")
+        return s
+
+    def dump(self, kind):
+        cnt = abi.C.c_int64(0)
+        self._check(self.lib.debug_dump(self.ctx, kind, None, 0, abi.C.byref(cnt)), "debug_dump")
+        dt = np.float64 if kind == abi.GB_DUMP_CONTACT_INFO else np.uint32
+        out = np.zeros(max(1, cnt.value), dt)
+        self._check(self.lib.debug_dump(self.ctx, kind, out.ctypes.data_as(abi.C.c_void_p),
+                                        cnt.value, abi.C.byref(cnt)), "debug_dump")
+        out = out[:cnt.value]
+        if kind in (abi.GB_DUMP_CANDIDATE_PAIRS, abi.GB_DUMP_CONTACT_PAIRS):
+            out = out.reshape(-1, 2)
+        elif kind == abi.GB_DUMP_CONTACT_INFO:
+            out = out.reshape(-1, 7)
+        return out
+
+    def close(self):
+        if self.ctx:
+            self.lib.destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,235 @@
+/*
+ * grains_b200.h -- C ABI of the B200 DEM time-step engine.
+ *
+ * The engine replaces the per-time-step loop of Grains3D's ComponentManager
+ * (Grains/Component/include/ComponentManager.hh:130-182): linked-cell broad
+ * phase, GJK narrow phase, contact law, per-particle reduction and time
+ * integration, run as sm_100a CUDA kernels on one GPU.  Every entry point
+ * uses plain C types (pointers, sizes, PODs) so that a C++ ComponentManager
+ * subclass, a ctypes binding or any other FFI can bind it directly.
+ *
+ * Conventions
+ *   - Every call returns GB_OK (0) or a negative GB_E_* status; nothing
+ *     exits or aborts.  gb_status_string() names a status.
+ *   - A context owns all device memory and one CUDA stream.  Calls on one
+ *     context are not thread-safe; different contexts are independent.
+ *   - Host buffers are plain row-major double arrays.  A transform is 12
+ *     doubles: the 3x3 basis row-major (Mxx Mxy Mxz Myx ... Mzz) followed by
+ *     the origin (Ox Oy Oz), the layout of Grains' Transform3 buffer
+ *     (Grains/Geometry/src/Transform3.cpp:26-29, :133-137).
+ *   - Calls that read state back to the host synchronise the context stream.
+ */
+#ifndef GRAINS_B200_H
+#define GRAINS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB_ABI_VERSION 1
+
+/* ---- status codes --------------------------------------------------------- */
+#define GB_OK 0
+#define GB_E_INVALID_ARG (-1)   /* bad pointer, size or enum value            */
+#define GB_E_CUDA (-2)          /* a CUDA runtime call failed                  */
+#define GB_E_OUT_OF_MEMORY (-3) /* device allocation failed                    */
+#define GB_E_NOT_READY (-4)     /* call order: e.g. a step before set_state    */
+#define GB_E_OUT_OF_DOMAIN (-5) /* a particle centre left the linked-cell grid */
+#define GB_E_NONFINITE (-6)     /* NaN/Inf found in the particle state         */
+#define GB_E_NO_DEVICE (-7)     /* no usable CUDA device                       */
+#define GB_E_CAPACITY (-8)      /* a fixed-size buffer is too small            */
+#define GB_E_UNSUPPORTED (-9)   /* feature/shape combination not available     */
+
+/* ---- convex types: the values of Grains' ConvexType enum
+ *      (Grains/Geometry/include/Convex.hh:7-16) -------------------------------
+ * p[] holds
+ *   GB_SPHERE        r
+ *   GB_BOX           half edge lengths ex ey ez   (Box(T x, T y, T z), Box.cpp:6-8)
+ *   GB_SUPERQUADRIC  a b c n1 n2                  (Superquadric.cpp:10-17)
+ *   GB_POLYHEDRON    (unused) vertices come from the vertex pool
+ *   GB_RECTANGLE     half edge lengths LX/2 LY/2  (plane z=0 of its frame)
+ */
+#define GB_SPHERE 0
+#define GB_BOX 1
+#define GB_CYLINDER 2 /* not provided: GB_E_UNSUPPORTED */
+#define GB_CONE 3     /* not provided: GB_E_UNSUPPORTED */
+#define GB_SUPERQUADRIC 4
+#define GB_POLYHEDRON 5
+#define GB_RECTANGLE 6
+
+#define GB_MAX_POLY_VERTICES 64
+
+/* ---- run modes -------------------------------------------------------------- */
+#define GB_FP64 0  /* every kernel in double precision                         */
+#define GB_MIXED 1 /* FP32 bulk; FP64 positions, FP64 GJK polish near contact  */
+
+#define GB_LAW_HOOKE 0         /* HookeContactForceModel (parity)          */
+#define GB_LAW_HOOKE_HISTORY 1 /* spring-dashpot + Coulomb-capped tangential
+                                  spring with per-pair history               */
+
+#define GB_FIRST_ORDER_EXPLICIT 0 /* FirstOrderExplicit (parity)             */
+#define GB_VELOCITY_VERLET 1      /* velocity-Verlet / leapfrog              */
+
+#define GB_GJK_JH 0       /* Johnson sub-algorithm with cached determinants */
+#define GB_GJK_SV 1       /* signed-volume sub-algorithm                    */
+#define GB_GJK_NESTEROV 2 /* Nesterov-accelerated GJK                       */
+
+/* ---- plain-data descriptors ---------------------------------------------------*/
+typedef struct gb_convex {
+    int32_t type;         /* GB_SPHERE ... GB_RECTANGLE                          */
+    int32_t n_vertices;   /* GB_POLYHEDRON: vertex count (4..GB_MAX_POLY_VERTICES)*/
+    int64_t first_vertex; /* GB_POLYHEDRON: first vertex index in the pool        */
+    double p[5];
+} gb_convex;
+
+/* One Grains RigidBody (Grains/Geometry/src/RigidBody.cpp:19-59):
+ * RigidBody(convex, crustThickness, material, density). */
+typedef struct gb_rigid_body_desc {
+    gb_convex convex;
+    double crust_thickness;
+    double density; /* 0 for obstacles: mass and inertia are 0 */
+    int32_t material;
+    int32_t reserved;
+} gb_rigid_body_desc;
+
+/* Derived rigid-body properties, as RigidBody computes them. */
+typedef struct gb_rigid_body_props {
+    double volume;
+    double mass;
+    double circumscribed_radius;
+    double bounding_box[3]; /* half extents of the local bounding box */
+    double inertia[6];      /* xx xy xz yy yz zz, times density     */
+    double inertia_inv[6];  /* inverse, divided by density           */
+} gb_rigid_body_props;
+
+/* Contact-law parameters of one material pair: HookeContactForceModel's
+ * kn, en, etat, muc, kr (HookeContactForceModel.cpp:48-57) plus the tangential
+ * spring stiffness kt of the history law.  The table is indexed like
+ * ContactForceModelBuilderFactory::computeHash: l*(l+1)/2 + s with
+ * l = max(matA, matB), s = min(matA, matB). */
+typedef struct gb_contact_model {
+    double kn, en, etat, muc, kr, kt;
+} gb_contact_model;
+
+typedef struct gb_config {
+    int32_t n_particles;
+    int32_t n_rigid_bodies; /* entries of the rigid-body table               */
+    int32_t n_obstacles;
+    int32_t n_materials;
+    double origin[3];         /* GrainsParameters::m_origin (LinkedCell min)  */
+    double max_coordinate[3]; /* GrainsParameters::m_maxCoordinate            */
+    double cell_size_factor;  /* LinkedCell CellSizeFactor, clamped to >= 1   */
+    int32_t pad_grid;         /* 1: max += one cell size per axis so that the
+                                 floored cell count covers the whole box      */
+    int32_t precision;        /* GB_FP64 | GB_MIXED                           */
+    double dt;
+    double gravity[3];
+    int32_t contact_law; /* GB_LAW_*          */
+    int32_t integrator;  /* GB_FIRST_ORDER_EXPLICIT | GB_VELOCITY_VERLET */
+    int32_t gjk_variant; /* GB_GJK_*          */
+    int32_t device;      /* CUDA device ordinal */
+    int64_t pair_capacity; /* initial candidate-pair capacity, 0 = automatic */
+} gb_config;
+
+/* Counters of the last completed step (or of the last detect call). */
+typedef struct gb_stats {
+    int64_t steps_done;
+    int64_t candidate_pairs;  /* ordered pairs passing the bounding-sphere test */
+    int64_t contacts;         /* ordered particle pairs with overlap < 0         */
+    int64_t obstacle_contacts;
+    int64_t gjk_calls;
+    int64_t gjk_iterations;
+    int32_t status_flags; /* bit i set: device-side error (1 << -GB_E_x)    */
+    int32_t n_cells;
+    int32_t cells_per_dir[3];
+    int32_t key_bits;
+    double cell_size;
+    double grid_max[3]; /* linked-cell max corner actually used */
+} gb_stats;
+
+/* ---- debug dump kinds -------------------------------------------------------- */
+#define GB_DUMP_CELL_HASH 0       /* uint32[N]: cell hash per particle id          */
+#define GB_DUMP_SORTED_IDS 1      /* uint32[N]: particle ids sorted by (cell, id)  */
+#define GB_DUMP_CELL_START 2      /* uint32[C+1]: first sorted index of each cell  */
+#define GB_DUMP_CANDIDATE_PAIRS 3 /* uint32[2P]: (A,B) ordered candidate pairs     */
+#define GB_DUMP_CONTACT_PAIRS 4   /* uint32[2K]: (A,B) pairs with overlap < 0      */
+#define GB_DUMP_CONTACT_INFO 5    /* double[7K]: contact point, vector, overlap    */
+#define GB_DUMP_NEIGHBORS 6       /* uint32[27C]: neighbour table (UINT32_MAX out) */
+
+typedef struct gb_ctx gb_ctx;
+
+/* ---- lifetime ------------------------------------------------------------------ */
+gb_ctx* gb_create(const gb_config* cfg, int* status);
+int gb_destroy(gb_ctx* ctx);
+const char* gb_status_string(int status);
+int gb_abi_version(void);
+
+/* ---- set-up (Grains::Construction, Grains/Base/src/Grains.cpp:90-300) ----------- */
+/* Rigid-body table; `vertices` holds 3 doubles per polyhedron vertex. */
+int gb_set_rigid_bodies(gb_ctx* ctx, const gb_rigid_body_desc* rbs,
+                        const double* vertices, int64_t n_vertices);
+int gb_get_rigid_body_props(gb_ctx* ctx, int32_t rb, gb_rigid_body_props* out);
+/* n_materials*(n_materials+1)/2 entries. */
+int gb_set_contact_models(gb_ctx* ctx, const gb_contact_model* table);
+/* Obstacles: n_obstacles rigid bodies (density 0) and their transforms. */
+int gb_set_obstacles(gb_ctx* ctx, const gb_rigid_body_desc* obstacles,
+                     const double* transforms);
+
+/* ---- particle state (ComponentManager set/get, ComponentManager.hh:37-104) ------ */
+int gb_set_rigid_body_ids(gb_ctx* ctx, const uint32_t* ids);
+int gb_set_transforms(gb_ctx* ctx, const double* transforms); /* 12 per particle */
+int gb_set_velocities(gb_ctx* ctx, const double* kin);        /* v(3) omega(3)   */
+int gb_get_transforms(gb_ctx* ctx, double* transforms);
+int gb_get_velocities(gb_ctx* ctx, double* kin);
+/* Torce per particle: force(3) torque(3), accumulated since the last move. */
+int gb_get_torces(gb_ctx* ctx, double* torce);
+
+/* ---- the time step: the ComponentManager hot-path calls ---------------------- */
+/* ComponentManager::updateLinks (ComponentManagerCPU.cpp:278-296). */
+int gb_update_links(gb_ctx* ctx);
+/* ComponentManager::detectCollisionAndComputeContactForces
+ * (ComponentManagerCPU.cpp:428-443): updateLinks, particle-particle and
+ * particle-obstacle contacts, forces added to the torces.  `result` (host,
+ * n_particles ints, may be NULL) is incremented per particle by the number of
+ * ordered contacts, like the reference's `int* result`. */
+int gb_detect_collision_and_compute_contact_forces(gb_ctx* ctx, int32_t* result);
+/* ComponentManager::addExternalForces (ComponentManagerCPU.cpp:448-460). */
+int gb_add_external_forces(gb_ctx* ctx);
+/* ComponentManager::moveParticles (ComponentManagerCPU.cpp:465-500). */
+int gb_move_particles(gb_ctx* ctx);
+/* n_steps of GrainsCPU::simulate's loop body (GrainsCPU.cpp:55-66), fused. */
+int gb_step(gb_ctx* ctx, int32_t n_steps);
+
+/* ---- diagnostics ---------------------------------------------------------------- */
+int gb_get_stats(gb_ctx* ctx, gb_stats* out);
+/* Copies a dump (GB_DUMP_*) of the last detect step to `out` (host memory of
+ * `capacity` elements); *count receives the number of elements available. */
+int gb_debug_dump(gb_ctx* ctx, int32_t kind, void* out, int64_t capacity,
+                  int64_t* count);
+/* Device pointers of the SoA state for zero-copy consumers (torch, CUDA code).
+ * names: "pos_x" "pos_y" "pos_z" (double), "quat_w" "quat_x" "quat_y"
+ * "quat_z" "vel_x" ... "omega_z" "force_x" ... "torque_z" (double in GB_FP64,
+ * float in GB_MIXED), "rb_id" (uint32). */
+int gb_device_pointer(gb_ctx* ctx, const char* name, void** ptr);
+/* Synchronises the context stream and returns the device-side status flags. */
+int gb_synchronize(gb_ctx* ctx);
+
+/* ---- host set-up helpers (no context needed) ------------------------------------- */
+/* Volume, mass, circumscribed radius, bounding box and inertia of a rigid
+ * body as RigidBody::RigidBody computes them; polyhedra use their convex
+ * hull.  `vertices` may be NULL unless the convex is a polyhedron. */
+int gb_rigid_body_properties(const gb_rigid_body_desc* rb, const double* vertices,
+                             gb_rigid_body_props* out);
+/* Convex hull of n points (n <= GB_MAX_POLY_VERTICES): writes the hull's
+ * centroid to centroid[3] and its volume to *volume. */
+int gb_convex_hull_centroid(const double* points, int32_t n, double* centroid,
+                            double* volume);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAINS_B200_H */
