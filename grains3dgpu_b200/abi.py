@@ -23,7 +23,8 @@ GB_SPHERE, GB_BOX, GB_CYLINDER, GB_CONE = 0, 1, 2, 3
 GB_SUPERQUADRIC, GB_POLYHEDRON, GB_RECTANGLE = 4, 5, 6
 GB_MAX_POLY_VERTICES = 64
 
-GB_FP64, GB_MIXED = 0, 1
+GB_FP64, GB_MIXED, GB_FP64_STRICT = 0, 1, 2
+GB_FLAG_RECORD_CONTACT_INFO = 1
 GB_LAW_HOOKE, GB_LAW_HOOKE_HISTORY = 0, 1
 GB_FIRST_ORDER_EXPLICIT, GB_VELOCITY_VERLET = 0, 1
 GB_GJK_JH, GB_GJK_SV, GB_GJK_NESTEROV = 0, 1, 2
@@ -68,7 +69,8 @@ class Config(C.Structure):
                 ("precision", C.c_int32), ("dt", C.c_double),
                 ("gravity", C.c_double * 3), ("contact_law", C.c_int32),
                 ("integrator", C.c_int32), ("gjk_variant", C.c_int32),
-                ("device", C.c_int32), ("pair_capacity", C.c_int64)]
+                ("device", C.c_int32), ("pair_capacity", C.c_int64),
+                ("flags", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Stats(C.Structure):

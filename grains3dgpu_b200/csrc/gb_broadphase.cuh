@@ -1,0 +1,317 @@
+// gb_broadphase.cuh -- linked-cell broad phase on the GPU: cell hash per
+// particle, a stable LSD radix sort of (cell, particle id), the cell-start
+// table, and device-wide exclusive scans.  Integer work: HBM-bound, no atomics
+// on the data path (only shared-memory histogram counters).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gb
+{
+
+constexpr int kBlock = 256;           // threads per block for the streaming kernels
+constexpr int kItems = 8;             // elements per thread in sort/scan tiles
+constexpr int kTile  = kBlock * kItems;
+constexpr int kWarps = kBlock / 32;
+
+// device status bits (bit i <-> GB_E_* == -i)
+constexpr int kFlagOutOfDomain = 1 << 5;
+constexpr int kFlagNonFinite   = 1 << 6;
+constexpr int kFlagCapacity    = 1 << 8;
+
+// ---- cell hash: LinkedCell::computeCellId / computeLinearCellHash
+//      (Grains/Component/src/LinkedCell.cpp:117-159): floor((p - min)/extent)
+//      in IEEE double, linear hash (z*ny + y)*nx + x.  Out-of-grid centres are
+//      clamped to the grid and flagged (the reference indexes out of bounds).
+__global__ void k_hash(int n, const double* __restrict__ px, const double* __restrict__ py,
+                       const double* __restrict__ pz, double mnx, double mny, double mnz,
+                       double cell, uint32_t nx, uint32_t ny, uint32_t nz,
+                       uint32_t* __restrict__ keys, uint32_t* __restrict__ ids,
+                       int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const double p[3]  = {px[i], py[i], pz[i]};
+    const double mn[3] = {mnx, mny, mnz};
+    const uint32_t dim[3] = {nx, ny, nz};
+    uint32_t       c[3];
+    int            bad = 0;
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+        const double f = floor(__ddiv_rn(__dsub_rn(p[k], mn[k]), cell));
+        if(!(f >= 0.0))
+        {
+            c[k] = 0;
+            bad |= (f != f) ? kFlagNonFinite : kFlagOutOfDomain;
+        }
+        else if(f >= (double)dim[k])
+        {
+            c[k] = dim[k] - 1;
+            bad |= kFlagOutOfDomain;
+        }
+        else
+            c[k] = (uint32_t)f;
+    }
+    keys[i] = (c[2] * ny + c[1]) * nx + c[0];
+    ids[i]  = (uint32_t)i;
+    if(bad)
+        atomicOr(flags, bad);
+}
+
+// ---- radix sort, pass 1: per-block digit histograms, digit-major layout
+//      hist[d * nblocks + block] so that one exclusive scan gives every
+//      block's scatter base for every digit.
+__global__ void __launch_bounds__(kBlock) k_radix_hist(const uint32_t* __restrict__ keys,
+                                                       int n, int shift, uint32_t mask,
+                                                       uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t h[256];
+    const int           nb = (int)mask + 1;
+    for(int b = threadIdx.x; b < nb; b += kBlock)
+        h[b] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kTile;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+    {
+        const int idx = base + j * kBlock + threadIdx.x;
+        if(idx < n)
+            atomicAdd(&h[(keys[idx] >> shift) & mask], 1u);
+    }
+    __syncthreads();
+    for(int b = threadIdx.x; b < nb; b += kBlock)
+        hist[(size_t)b * gridDim.x + blockIdx.x] = h[b];
+}
+
+// ---- radix sort, pass 2: stable scatter.  Warp w of a block owns the
+//      contiguous chunk [base + 256 w, base + 256 (w+1)) of the tile, so warp
+//      order is index order.  Each warp counts its digits (leader lanes of
+//      __match_any_sync groups, warp-private rows), a per-digit scan across
+//      the warps turns the counts into absolute output positions, and a
+//      second walk scatters with in-warp ranks.  Equal keys keep input order.
+__global__ void __launch_bounds__(kBlock)
+    k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int n,
+                    int shift, uint32_t mask, const uint32_t* __restrict__ hist_scan)
+{
+    __shared__ uint32_t cnt[kWarps][256];
+    const int           tid  = threadIdx.x;
+    const int           w    = tid >> 5;
+    const int           lane = tid & 31;
+    const unsigned      lt   = (1u << lane) - 1u;
+    const int           nb   = (int)mask + 1;
+    for(int i = tid; i < kWarps * 256; i += kBlock)
+        (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    const int chunk = blockIdx.x * kTile + w * (32 * kItems);
+    uint32_t  k[kItems], dg[kItems];
+#pragma unroll
+    for(int r = 0; r < kItems; ++r)
+    {
+        const int  idx = chunk + r * 32 + lane;
+        const bool v   = idx < n;
+        k[r]           = v ? keys_in[idx] : 0u;
+        dg[r]          = v ? ((k[r] >> shift) & mask) : (256u + (uint32_t)lane);
+        const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+        if(v && lane == __ffs(peers) - 1)
+            cnt[w][dg[r]] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    if(tid < nb)
+    {
+        uint32_t run = hist_scan[(size_t)tid * gridDim.x + blockIdx.x];
+#pragma unroll
+        for(int ww = 0; ww < kWarps; ++ww)
+        {
+            const uint32_t t = cnt[ww][tid];
+            cnt[ww][tid]     = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for(int r = 0; r < kItems; ++r)
+    {
+        const int      idx   = chunk + r * 32 + lane;
+        const bool     v     = idx < n;
+        const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+        const int      lead  = __ffs(peers) - 1;
+        uint32_t       off   = 0;
+        if(v)
+            off = cnt[w][dg[r]];
+        __syncwarp();
+        if(v)
+        {
+            const uint32_t pos = off + __popc(peers & lt);
+            keys_out[pos]      = k[r];
+            vals_out[pos]      = vals_in[idx];
+            if(lane == lead)
+                cnt[w][dg[r]] = off + __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// ---- exclusive scan of uint32 (three kernels, no inter-block waiting) -------
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if(lane >= o)
+            x += y;
+    }
+    return x;
+}
+
+// exclusive scan of one value per thread across the block; returns the
+// exclusive prefix and writes the block total to *total
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t x, uint32_t* total)
+{
+    __shared__ uint32_t ws[32];
+    const int           lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int           nw   = (blockDim.x + 31) >> 5;
+    const uint32_t      inc  = warp_incl_scan(x);
+    if(lane == 31)
+        ws[w] = inc;
+    __syncthreads();
+    if(w == 0)
+    {
+        uint32_t s = lane < nw ? ws[lane] : 0u;
+        s          = warp_incl_scan(s);
+        ws[lane]   = s;
+    }
+    __syncthreads();
+    const uint32_t before = w ? ws[w - 1] : 0u;
+    if(total)
+        *total = ws[nw - 1];
+    __syncthreads();
+    return before + inc - x;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_reduce(const uint32_t* __restrict__ in,
+                                                        int64_t n, uint32_t* __restrict__ partial)
+{
+    const int64_t base = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
+    uint32_t      s    = 0;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+        if(base + j < n)
+            s += in[base + j];
+    uint32_t tot;
+    block_excl_scan(s, &tot);
+    if(threadIdx.x == 0)
+        partial[blockIdx.x] = tot;
+}
+
+// single block: exclusive scan of the per-tile partial sums, in chunks
+__global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* __restrict__ partial, int m,
+                                                        uint32_t* __restrict__ grand_total)
+{
+    uint32_t carry = 0;
+    for(int c = 0; c < m; c += 1024)
+    {
+        const int      i = c + threadIdx.x;
+        const uint32_t x = i < m ? partial[i] : 0u;
+        uint32_t       tot;
+        const uint32_t ex = block_excl_scan(x, &tot);
+        if(i < m)
+            partial[i] = carry + ex;
+        carry += tot;
+    }
+    if(threadIdx.x == 0 && grand_total)
+        *grand_total = carry;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_apply(const uint32_t* __restrict__ in,
+                                                       uint32_t* __restrict__ out, int64_t n,
+                                                       const uint32_t* __restrict__ partial)
+{
+    const int64_t base = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
+    uint32_t      v[kItems];
+    uint32_t      s = 0;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+    {
+        v[j] = base + j < n ? in[base + j] : 0u;
+        s += v[j];
+    }
+    uint32_t run = partial[blockIdx.x] + block_excl_scan(s, nullptr);
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+        if(base + j < n)
+        {
+            out[base + j] = run;
+            run += v[j];
+        }
+}
+
+// ---- cell-start table: start[c] = first sorted index whose key >= c, for all
+//      c in [0, ncells] (so cell c holds [start[c], start[c+1]); empty cells
+//      get an empty range).  A block covers kCellsPerBlock consecutive cells:
+//      it locates its key range with two binary searches, stages those sorted
+//      keys in shared memory, and answers each cell from there.
+constexpr int kCellsPerBlock = 1024;
+constexpr int kStageCap      = 4096;
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t key)
+{
+    uint32_t lo = 0, hi = n;
+    while(lo < hi)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if(a[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kBlock) k_cell_start(const uint32_t* __restrict__ skeys,
+                                                       uint32_t n, uint32_t ncells,
+                                                       uint32_t* __restrict__ start)
+{
+    __shared__ uint32_t range[2];
+    __shared__ uint32_t sk[kStageCap];
+    const uint32_t      c0 = blockIdx.x * kCellsPerBlock;
+    if(threadIdx.x < 2)
+        range[threadIdx.x] = lower_bound_u32(skeys, n, c0 + threadIdx.x * kCellsPerBlock);
+    __syncthreads();
+    const uint32_t lo = range[0], hi = range[1];
+    const uint32_t m  = hi - lo;
+    const bool     staged = m <= (uint32_t)kStageCap;
+    if(staged)
+        for(uint32_t i = threadIdx.x; i < m; i += kBlock)
+            sk[i] = skeys[lo + i];
+    __syncthreads();
+    for(int j = threadIdx.x; j < kCellsPerBlock; j += kBlock)
+    {
+        const uint32_t c = c0 + j;
+        if(c > ncells)
+            break;
+        const uint32_t r = staged ? lower_bound_u32(sk, m, c) : lower_bound_u32(skeys + lo, m, c);
+        start[c]         = lo + r;
+    }
+}
+
+// positions and bounding radii in sorted order, for contiguous neighbour reads
+__global__ void k_gather_sorted(int n, const uint32_t* __restrict__ sids,
+                                const double* __restrict__ px, const double* __restrict__ py,
+                                const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
+                                const double* __restrict__ rcirc, double4* __restrict__ out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= n)
+        return;
+    const uint32_t i = sids[t];
+    out[t]           = make_double4(px[i], py[i], pz[i], rcirc[rb_id[i]]);
+}
+
+} // namespace gb

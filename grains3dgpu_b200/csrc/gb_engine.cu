@@ -1,0 +1,1315 @@
+// gb_engine.cu -- the C ABI of include/grains_b200.h: context, device memory,
+// host<->device conversion of the Grains state layout, and the launch
+// sequence of one time step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "gb_step.cuh"
+
+using namespace gb;
+
+namespace
+{
+
+thread_local cudaError_t g_last_cuda = cudaSuccess;
+
+#define GB_CK(x)                               \
+    do                                         \
+    {                                          \
+        cudaError_t e_ = (x);                  \
+        if(e_ != cudaSuccess)                  \
+        {                                      \
+            g_last_cuda = e_;                  \
+            return e_ == cudaErrorMemoryAllocation ? GB_E_OUT_OF_MEMORY : GB_E_CUDA; \
+        }                                      \
+    } while(0)
+
+#define GB_TRY(x)            \
+    do                       \
+    {                        \
+        int st_ = (x);       \
+        if(st_ != GB_OK)     \
+            return st_;      \
+    } while(0)
+
+inline int blocks(int64_t n, int b)
+{
+    return (int)((n + b - 1) / b);
+}
+
+template <typename T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if(count == 0)
+        count = 1;
+    GB_CK(cudaMalloc((void**)p, count * sizeof(T)));
+    return GB_OK;
+}
+
+template <typename T>
+void dfree(T*& p)
+{
+    if(p)
+        cudaFree((void*)p);
+    p = nullptr;
+}
+
+} // namespace
+
+struct gb_ctx
+{
+    gb_config    cfg;
+    int          prec = GB_FP64;
+    cudaStream_t stream = nullptr;
+    int          n = 0, nrb = 0, nob = 0, nmat = 0;
+    bool         rb_set = false, law_set = false, ids_set = false, tr_set = false,
+         vel_set = false, obs_set = false;
+
+    // host copies of the set-up
+    std::vector<gb_rigid_body_desc>  rbs;
+    std::vector<gb_rigid_body_props> props;
+    std::vector<double>              verts;
+    std::vector<gb_rigid_body_desc>  obs;
+    std::vector<gb_rigid_body_props> obs_props;
+    std::vector<double>              obs_tr;
+    std::vector<gb_contact_model>    laws;
+    bool                             has_kr = false;
+
+    // linked cell
+    double   cell = 0, lc_max[3] = {0, 0, 0};
+    uint32_t dims[3] = {0, 0, 0};
+    uint32_t ncells = 0;
+    int      key_bits = 0;
+
+    // device tables (storage type of the run mode)
+    void*    d_shape = nullptr;
+    void*    d_inertia = nullptr;
+    void*    d_verts = nullptr;
+    void*    d_law = nullptr;
+    void*    d_obs_shape = nullptr;
+    double*  d_obs_tr = nullptr;
+    double*  d_obs_mass = nullptr;
+    double*  d_rcirc64 = nullptr;
+
+    // state
+    double*   d_pos = nullptr; // 3n
+    void*     d_rot = nullptr; // 9n (FP64) or 4n (mixed)
+    void*     d_vel = nullptr; // 3n
+    void*     d_omg = nullptr;
+    void*     d_frc = nullptr;
+    void*     d_trq = nullptr;
+    uint32_t* d_rb_id = nullptr;
+    bool      torce_dirty = false;
+
+    // broad phase
+    uint32_t *d_hash = nullptr, *d_iota = nullptr, *d_k[2] = {nullptr, nullptr},
+             *d_i[2] = {nullptr, nullptr};
+    uint32_t *d_skeys = nullptr, *d_sids = nullptr; // results (alias into d_k/d_i)
+    uint32_t *d_hist = nullptr, *d_part = nullptr, *d_cstart = nullptr;
+    double4*  d_spos = nullptr;
+    size_t    part_cap = 0, hist_cap = 0;
+
+    // pairs (double-buffered for the tangential history)
+    uint32_t* d_count = nullptr;
+    uint32_t* d_off[2] = {nullptr, nullptr};
+    uint32_t* d_pb[2] = {nullptr, nullptr};
+    uint32_t* d_pa = nullptr;
+    void*     d_pf = nullptr; // 9 * cap storage values: f, t, m
+    uint8_t*  d_pc = nullptr;
+    double*   d_info = nullptr;
+    void*     d_xi[2] = {nullptr, nullptr}; // 3 * cap each
+    int64_t   cap = 0;
+    int       cur = 0;
+    int64_t   npairs = 0, prev_npairs = 0;
+    bool      have_prev = false;
+
+    // counters and flags
+    int*                d_flags = nullptr;
+    unsigned long long* d_counters = nullptr; // [0] wall contacts [1] gjk iterations [2] contacts
+    int*                d_contacts = nullptr;  // per-particle contact count of the last detect
+    uint32_t*           h_pinned = nullptr;    // pair total
+    int64_t             steps_done = 0;
+    bool                verlet_started = false;
+    bool                links_valid = false, detect_valid = false;
+    gb_stats            last{};
+};
+
+namespace
+{
+
+size_t store_size(int prec)
+{
+    return prec == GB_MIXED ? sizeof(float) : sizeof(double);
+}
+
+int rot_count(int prec)
+{
+    return prec == GB_MIXED ? 4 : 9;
+}
+
+template <typename St>
+State<St> state_of(gb_ctx* c)
+{
+    State<St> s;
+    const int n = c->n;
+    for(int k = 0; k < 3; ++k)
+    {
+        s.pos[k] = c->d_pos + (size_t)k * n;
+        s.vel[k] = (St*)c->d_vel + (size_t)k * n;
+        s.omg[k] = (St*)c->d_omg + (size_t)k * n;
+        s.frc[k] = (St*)c->d_frc + (size_t)k * n;
+        s.trq[k] = (St*)c->d_trq + (size_t)k * n;
+    }
+    for(int k = 0; k < 9; ++k)
+        s.rot[k] = k < rot_count(c->prec) ? (St*)c->d_rot + (size_t)k * n : nullptr;
+    s.rb_id = c->d_rb_id;
+    return s;
+}
+
+template <typename S>
+Tables<S> tables_of(gb_ctx* c)
+{
+    using St = store_t<S>;
+    Tables<S> t;
+    t.shape     = (const RBShape<St>*)c->d_shape;
+    t.inertia   = (const RBInertia<St>*)c->d_inertia;
+    t.verts     = (const Vert<St>*)c->d_verts;
+    t.law       = (const Law<St>*)c->d_law;
+    t.obs_shape = (const RBShape<St>*)c->d_obs_shape;
+    t.obs_tr    = c->d_obs_tr;
+    t.obs_mass  = c->d_obs_mass;
+    t.n_obs     = c->nob;
+    return t;
+}
+
+template <typename St>
+RBShape<St> shape_record(const gb_rigid_body_desc& d, const gb_rigid_body_props& p)
+{
+    RBShape<St> r;
+    std::memset(&r, 0, sizeof(r));
+    r.type       = d.convex.type;
+    r.nverts     = d.convex.n_vertices;
+    r.first_vert = d.convex.type == GB_POLYHEDRON ? d.convex.first_vertex : 0;
+    for(int i = 0; i < 5; ++i)
+        r.p[i] = (St)d.convex.p[i];
+    if(d.convex.type == GB_SUPERQUADRIC)
+    {
+        const double a = d.convex.p[0], b = d.convex.p[1], c = d.convex.p[2],
+                     n1 = d.convex.p[3], n2 = d.convex.p[4];
+        r.k[0] = (St)(b / a);
+        r.k[1] = (St)(c / a);
+        r.k[2] = (St)(c / b);
+        r.k[3] = (St)(1.0 / (n1 - 1.0));
+        r.k[4] = (St)(1.0 / (n2 - 1.0));
+        r.k[5] = (St)((n1 - n2) / (n2 * (n1 - 1.0)));
+        r.k[6] = (St)(n1 / n2);
+        r.k[7] = (St)(1.0 / n1);
+    }
+    r.crust    = (St)d.crust_thickness;
+    r.rcirc    = (St)p.circumscribed_radius;
+    for(int k = 0; k < 3; ++k)
+        r.bb[k] = (St)p.bounding_box[k];
+    r.material = d.material;
+    return r;
+}
+
+template <typename St>
+int upload_tables(gb_ctx* c)
+{
+    std::vector<RBShape<St>>   sh(c->nrb);
+    std::vector<RBInertia<St>> in(c->nrb);
+    std::vector<double>        rc(c->nrb);
+    for(int i = 0; i < c->nrb; ++i)
+    {
+        sh[i] = shape_record<St>(c->rbs[i], c->props[i]);
+        std::memset(&in[i], 0, sizeof(in[i]));
+        in[i].mass = (St)c->props[i].mass;
+        for(int k = 0; k < 6; ++k)
+        {
+            in[i].I[k]  = (St)c->props[i].inertia[k];
+            in[i].I1[k] = (St)c->props[i].inertia_inv[k];
+        }
+        rc[i] = c->props[i].circumscribed_radius;
+    }
+    const size_t nv = c->verts.size() / 3;
+    std::vector<Vert<St>> vv(std::max<size_t>(nv, 1));
+    for(size_t i = 0; i < nv; ++i)
+        vv[i] = {(St)c->verts[3 * i], (St)c->verts[3 * i + 1], (St)c->verts[3 * i + 2], (St)0};
+    dfree(c->d_shape);
+    dfree(c->d_inertia);
+    dfree(c->d_verts);
+    dfree(c->d_rcirc64);
+    GB_TRY(dalloc((RBShape<St>**)&c->d_shape, sh.size()));
+    GB_TRY(dalloc((RBInertia<St>**)&c->d_inertia, in.size()));
+    GB_TRY(dalloc((Vert<St>**)&c->d_verts, vv.size()));
+    GB_TRY(dalloc(&c->d_rcirc64, rc.size()));
+    GB_CK(cudaMemcpy(c->d_shape, sh.data(), sh.size() * sizeof(sh[0]), cudaMemcpyHostToDevice));
+    GB_CK(cudaMemcpy(c->d_inertia, in.data(), in.size() * sizeof(in[0]), cudaMemcpyHostToDevice));
+    GB_CK(cudaMemcpy(c->d_verts, vv.data(), vv.size() * sizeof(vv[0]), cudaMemcpyHostToDevice));
+    GB_CK(cudaMemcpy(c->d_rcirc64, rc.data(), rc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return GB_OK;
+}
+
+template <typename St>
+int upload_laws(gb_ctx* c)
+{
+    const int         nl = c->nmat * (c->nmat + 1) / 2;
+    std::vector<Law<St>> L(nl);
+    c->has_kr = false;
+    for(int i = 0; i < nl; ++i)
+    {
+        const gb_contact_model& m = c->laws[i];
+        L[i].kn   = (St)m.kn;
+        // m_muen = log(en)/sqrt(PI^2 + log(en)^2) (HookeContactForceModel.cpp:56)
+        L[i].muen = (St)(std::log(m.en)
+                         / std::sqrt(3.1415926535897932385 * 3.1415926535897932385
+                                     + std::log(m.en) * std::log(m.en)));
+        L[i].etat = (St)m.etat;
+        L[i].muc  = (St)m.muc;
+        L[i].kr   = (St)m.kr;
+        L[i].kt   = (St)m.kt;
+        c->has_kr = c->has_kr || m.kr != 0.0;
+    }
+    dfree(c->d_law);
+    GB_TRY(dalloc((Law<St>**)&c->d_law, L.size()));
+    GB_CK(cudaMemcpy(c->d_law, L.data(), L.size() * sizeof(L[0]), cudaMemcpyHostToDevice));
+    return GB_OK;
+}
+
+template <typename St>
+int upload_obstacles(gb_ctx* c)
+{
+    std::vector<RBShape<St>> sh(std::max(c->nob, 1));
+    std::vector<double>      mass(std::max(c->nob, 1), 0.0);
+    for(int i = 0; i < c->nob; ++i)
+    {
+        sh[i]   = shape_record<St>(c->obs[i], c->obs_props[i]);
+        mass[i] = c->obs_props[i].mass;
+    }
+    dfree(c->d_obs_shape);
+    dfree(c->d_obs_tr);
+    dfree(c->d_obs_mass);
+    GB_TRY(dalloc((RBShape<St>**)&c->d_obs_shape, sh.size()));
+    GB_TRY(dalloc(&c->d_obs_tr, std::max<size_t>(c->obs_tr.size(), 12)));
+    GB_TRY(dalloc(&c->d_obs_mass, mass.size()));
+    GB_CK(cudaMemcpy(c->d_obs_shape, sh.data(), sh.size() * sizeof(sh[0]), cudaMemcpyHostToDevice));
+    if(!c->obs_tr.empty())
+        GB_CK(cudaMemcpy(c->d_obs_tr, c->obs_tr.data(), c->obs_tr.size() * sizeof(double),
+                         cudaMemcpyHostToDevice));
+    GB_CK(cudaMemcpy(c->d_obs_mass, mass.data(), mass.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return GB_OK;
+}
+
+// Quaternion::setQuaternion(Matrix3) on the host, for the mixed mode's
+// quaternion state (Quaternion.cpp:125-169).
+void basis_to_quat(const double* b, double q[4])
+{
+    enum { XX, XY, XZ, YX, YY, YZ, ZX, ZY, ZZ };
+    double den;
+    if(b[YY] > -b[ZZ] && b[XX] > -b[YY] && b[XX] > -b[ZZ])
+    {
+        den  = std::pow(1.0 + b[XX] + b[YY] + b[ZZ], 0.5);
+        q[0] = 0.5 * den;
+        q[1] = 0.5 * (b[ZY] - b[YZ]) / den;
+        q[2] = 0.5 * (b[XZ] - b[ZX]) / den;
+        q[3] = 0.5 * (b[YX] - b[XY]) / den;
+    }
+    else if(b[YY] < -b[ZZ] && b[XX] > b[YY] && b[XX] > b[ZZ])
+    {
+        den  = std::pow(1.0 + b[XX] - b[YY] - b[ZZ], 0.5);
+        q[0] = 0.5 * (b[ZY] - b[YZ]) / den;
+        q[1] = 0.5 * den;
+        q[2] = 0.5 * (b[XY] + b[YX]) / den;
+        q[3] = 0.5 * (b[ZX] + b[XZ]) / den;
+    }
+    else if(b[YY] > b[ZZ] && b[XX] < b[YY] && b[XX] < -b[ZZ])
+    {
+        den  = std::pow(1.0 - b[XX] + b[YY] - b[ZZ], 0.5);
+        q[0] = 0.5 * (b[XZ] - b[ZX]) / den;
+        q[1] = 0.5 * (b[XY] + b[YX]) / den;
+        q[2] = 0.5 * den;
+        q[3] = 0.5 * (b[YZ] + b[ZY]) / den;
+    }
+    else if(b[YY] < b[ZZ] && b[XX] < -b[YY] && b[XX] < b[ZZ])
+    {
+        den  = std::pow(1.0 - b[XX] - b[YY] + b[ZZ], 0.5);
+        q[0] = 0.5 * (b[YX] - b[XY]) / den;
+        q[1] = 0.5 * (b[ZX] + b[XZ]) / den;
+        q[2] = 0.5 * (b[YZ] + b[ZY]) / den;
+        q[3] = 0.5 * den;
+    }
+    else
+    {
+        q[0] = 1.0;
+        q[1] = q[2] = q[3] = 0.0;
+    }
+    const double nq = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for(int k = 0; k < 4; ++k)
+        q[k] /= nq;
+}
+
+void quat_to_basis(const double q[4], double* m)
+{
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    m[0] = 1 - 2 * (y * y + z * z);
+    m[1] = 2 * (x * y - w * z);
+    m[2] = 2 * (x * z + w * y);
+    m[3] = 2 * (x * y + w * z);
+    m[4] = 1 - 2 * (x * x + z * z);
+    m[5] = 2 * (y * z - w * x);
+    m[6] = 2 * (x * z - w * y);
+    m[7] = 2 * (y * z + w * x);
+    m[8] = 1 - 2 * (x * x + y * y);
+}
+
+int alloc_state(gb_ctx* c)
+{
+    const size_t n = c->n, ss = store_size(c->prec);
+    GB_TRY(dalloc(&c->d_pos, 3 * n));
+    GB_CK(cudaMalloc(&c->d_rot, std::max<size_t>(1, rot_count(c->prec) * n) * ss));
+    GB_CK(cudaMalloc(&c->d_vel, std::max<size_t>(1, 3 * n) * ss));
+    GB_CK(cudaMalloc(&c->d_omg, std::max<size_t>(1, 3 * n) * ss));
+    GB_CK(cudaMalloc(&c->d_frc, std::max<size_t>(1, 3 * n) * ss));
+    GB_CK(cudaMalloc(&c->d_trq, std::max<size_t>(1, 3 * n) * ss));
+    GB_CK(cudaMemset(c->d_frc, 0, std::max<size_t>(1, 3 * n) * ss));
+    GB_CK(cudaMemset(c->d_trq, 0, std::max<size_t>(1, 3 * n) * ss));
+    GB_TRY(dalloc(&c->d_rb_id, n));
+    GB_CK(cudaMemset(c->d_rb_id, 0, std::max<size_t>(1, n) * sizeof(uint32_t)));
+    GB_TRY(dalloc(&c->d_hash, n));
+    GB_TRY(dalloc(&c->d_iota, n));
+    for(int b = 0; b < 2; ++b)
+    {
+        GB_TRY(dalloc(&c->d_k[b], n));
+        GB_TRY(dalloc(&c->d_i[b], n));
+        GB_TRY(dalloc(&c->d_off[b], n + 1));
+    }
+    GB_TRY(dalloc(&c->d_spos, n));
+    GB_TRY(dalloc(&c->d_count, n + 1));
+    GB_TRY(dalloc(&c->d_contacts, n));
+    GB_TRY(dalloc(&c->d_flags, 1));
+    GB_TRY(dalloc(&c->d_counters, 4));
+    GB_CK(cudaMemset(c->d_flags, 0, sizeof(int)));
+    GB_CK(cudaMemset(c->d_counters, 0, 4 * sizeof(unsigned long long)));
+    GB_CK(cudaMemset(c->d_contacts, 0, std::max<size_t>(1, n) * sizeof(int)));
+    GB_CK(cudaMallocHost((void**)&c->h_pinned, 4 * sizeof(uint32_t)));
+    return GB_OK;
+}
+
+int ensure_pairs(gb_ctx* c, int64_t need)
+{
+    if(need <= c->cap)
+        return GB_OK;
+    int64_t ncap = std::max<int64_t>(need + need / 2, 1024);
+    const size_t ss = store_size(c->prec);
+    const bool   hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
+    // the previous step's history buffers must survive the growth
+    uint32_t* npb[2] = {nullptr, nullptr};
+    void*     nxi[2] = {nullptr, nullptr};
+    for(int b = 0; b < 2; ++b)
+    {
+        GB_TRY(dalloc(&npb[b], ncap));
+        if(hist)
+            GB_CK(cudaMalloc(&nxi[b], 3 * ncap * ss));
+    }
+    const int prev = 1 - c->cur;
+    if(c->have_prev && c->prev_npairs > 0)
+    {
+        GB_CK(cudaMemcpy(npb[prev], c->d_pb[prev], c->prev_npairs * sizeof(uint32_t),
+                         cudaMemcpyDeviceToDevice));
+        if(hist)
+            for(int k = 0; k < 3; ++k)
+                GB_CK(cudaMemcpy((char*)nxi[prev] + k * ncap * ss,
+                                 (char*)c->d_xi[prev] + k * c->cap * ss,
+                                 c->prev_npairs * ss, cudaMemcpyDeviceToDevice));
+    }
+    for(int b = 0; b < 2; ++b)
+    {
+        dfree(c->d_pb[b]);
+        c->d_pb[b] = npb[b];
+        dfree(c->d_xi[b]);
+        c->d_xi[b] = nxi[b];
+    }
+    dfree(c->d_pa);
+    dfree(c->d_pf);
+    dfree(c->d_pc);
+    dfree(c->d_info);
+    GB_TRY(dalloc(&c->d_pa, ncap));
+    GB_CK(cudaMalloc(&c->d_pf, 9 * ncap * ss));
+    GB_TRY(dalloc(&c->d_pc, ncap));
+    if(c->cfg.flags & GB_FLAG_RECORD_CONTACT_INFO)
+        GB_TRY(dalloc(&c->d_info, 7 * ncap));
+    c->cap = ncap;
+    return GB_OK;
+}
+
+// exclusive scan of n uint32 (in place allowed); *d_total (device) gets the sum
+int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total)
+{
+    const int nb = std::max(1, blocks(n, kTile));
+    if((size_t)nb > c->part_cap)
+    {
+        dfree(c->d_part);
+        GB_TRY(dalloc(&c->d_part, nb));
+        c->part_cap = nb;
+    }
+    k_scan_reduce<<<nb, kBlock, 0, c->stream>>>(in, n, c->d_part);
+    k_scan_partials<<<1, 1024, 0, c->stream>>>(c->d_part, nb, d_total);
+    k_scan_apply<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_part);
+    GB_CK(cudaGetLastError());
+    return GB_OK;
+}
+
+// hash -> stable radix sort of (cell, id) -> cell-start table -> sorted
+// positions (ComponentManager::updateLinks)
+int broad_phase(gb_ctx* c)
+{
+    const int n = c->n;
+    const int nb = std::max(1, blocks(n, kBlock));
+    cudaStream_t s = c->stream;
+    k_hash<<<nb, kBlock, 0, s>>>(n, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
+                                 c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2], c->cell,
+                                 c->dims[0], c->dims[1], c->dims[2], c->d_hash, c->d_iota,
+                                 c->d_flags);
+    GB_CK(cudaGetLastError());
+    const uint32_t* src_k = c->d_hash;
+    const uint32_t* src_i = c->d_iota;
+    const int       passes = c->key_bits == 0 ? 0 : (c->key_bits + 7) / 8;
+    const int       bits_per = passes ? (c->key_bits + passes - 1) / passes : 0;
+    const int       ntile = std::max(1, blocks(n, kTile));
+    int             dst = 0;
+    for(int p = 0; p < passes; ++p)
+    {
+        const int      shift = p * bits_per;
+        const int      b     = std::min(bits_per, c->key_bits - shift);
+        const uint32_t mask  = (1u << b) - 1u;
+        const size_t   hn    = (size_t)(mask + 1) * ntile;
+        if(hn > c->hist_cap)
+        {
+            dfree(c->d_hist);
+            GB_TRY(dalloc(&c->d_hist, hn));
+            c->hist_cap = hn;
+        }
+        k_radix_hist<<<ntile, kBlock, 0, s>>>(src_k, n, shift, mask, c->d_hist);
+        GB_TRY(scan_u32(c, c->d_hist, c->d_hist, (int64_t)hn, nullptr));
+        k_radix_scatter<<<ntile, kBlock, 0, s>>>(src_k, src_i, c->d_k[dst], c->d_i[dst], n, shift,
+                                                 mask, c->d_hist);
+        GB_CK(cudaGetLastError());
+        src_k = c->d_k[dst];
+        src_i = c->d_i[dst];
+        dst ^= 1;
+    }
+    if(passes == 0)
+    {
+        GB_CK(cudaMemcpyAsync(c->d_k[0], c->d_hash, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        GB_CK(cudaMemcpyAsync(c->d_i[0], c->d_iota, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        src_k = c->d_k[0];
+        src_i = c->d_i[0];
+    }
+    c->d_skeys = const_cast<uint32_t*>(src_k);
+    c->d_sids  = const_cast<uint32_t*>(src_i);
+    k_cell_start<<<blocks((int64_t)c->ncells + 1, kCellsPerBlock), kBlock, 0, s>>>(
+        c->d_skeys, (uint32_t)n, c->ncells, c->d_cstart);
+    k_gather_sorted<<<nb, kBlock, 0, s>>>(n, c->d_sids, c->d_pos, c->d_pos + n,
+                                          c->d_pos + 2 * (size_t)n, c->d_rb_id, c->d_rcirc64,
+                                          c->d_spos);
+    GB_CK(cudaGetLastError());
+    c->links_valid = true;
+    return GB_OK;
+}
+
+// candidate pairs: count -> scan -> (read total, grow) -> fill
+int build_pairs(gb_ctx* c)
+{
+    const int    n = c->n;
+    const int    nb = std::max(1, blocks(n, kBlock));
+    cudaStream_t s = c->stream;
+    const bool   strict = c->prec == GB_FP64_STRICT;
+    if(c->cfg.contact_law == GB_LAW_HOOKE_HISTORY)
+        c->cur ^= 1; // last step's pair list becomes the history
+    uint32_t* off = c->d_off[c->cur];
+    if(strict)
+        k_pairs<true, false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
+                                                    c->d_cstart, c->dims[0], c->dims[1],
+                                                    c->dims[2], c->d_count, nullptr, nullptr,
+                                                    nullptr, 0, c->d_flags);
+    else
+        k_pairs<false, false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
+                                                     c->d_cstart, c->dims[0], c->dims[1],
+                                                     c->dims[2], c->d_count, nullptr, nullptr,
+                                                     nullptr, 0, c->d_flags);
+    GB_CK(cudaGetLastError());
+    GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
+    GB_CK(cudaMemcpyAsync(c->h_pinned, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GB_CK(cudaStreamSynchronize(s));
+    const int64_t total = c->h_pinned[0];
+    GB_TRY(ensure_pairs(c, total));
+    if(strict)
+        k_pairs<true, true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, c->d_cstart,
+                                                   c->dims[0], c->dims[1], c->dims[2], nullptr, off,
+                                                   c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags);
+    else
+        k_pairs<false, true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
+                                                    c->d_cstart, c->dims[0], c->dims[1],
+                                                    c->dims[2], nullptr, off, c->d_pa,
+                                                    c->d_pb[c->cur], c->cap, c->d_flags);
+    GB_CK(cudaGetLastError());
+    c->npairs = total;
+    return GB_OK;
+}
+
+template <typename S>
+PairOut<store_t<S>> pair_out(gb_ctx* c)
+{
+    using St = store_t<S>;
+    PairOut<St> po;
+    const int64_t cap = c->cap;
+    for(int k = 0; k < 3; ++k)
+    {
+        po.f[k] = (St*)c->d_pf + k * cap;
+        po.t[k] = (St*)c->d_pf + (3 + k) * cap;
+        po.m[k] = (St*)c->d_pf + (6 + k) * cap;
+        po.xi[k] = c->d_xi[c->cur] ? (St*)c->d_xi[c->cur] + k * cap : nullptr;
+    }
+    po.contact  = c->d_pc;
+    po.info     = c->d_info;
+    const int prev = 1 - c->cur;
+    po.prev_off = c->d_off[prev];
+    po.prev_b   = c->d_pb[prev];
+    for(int k = 0; k < 3; ++k)
+        po.prev_xi[k] = c->d_xi[prev] ? (const St*)c->d_xi[prev] + k * cap : nullptr;
+    return po;
+}
+
+template <typename S>
+int run_detect(gb_ctx* c, int phases, int32_t* result)
+{
+    using St = store_t<S>;
+    cudaStream_t s = c->stream;
+    GB_TRY(broad_phase(c));
+    GB_TRY(build_pairs(c));
+    PairOut<St> po = pair_out<S>(c);
+    const bool hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
+    if(hist && !c->have_prev)
+    {
+        // no history yet: an empty previous list for every particle
+        GB_CK(cudaMemsetAsync(c->d_off[1 - c->cur], 0, (c->n + 1) * sizeof(uint32_t), s));
+    }
+    const State<St> st = state_of<St>(c);
+    const Tables<S> tb = tables_of<S>(c);
+    if(c->npairs > 0)
+    {
+        k_narrow<S><<<blocks(c->npairs, 128), 128, 0, s>>>(
+            c->npairs, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law, c->has_kr ? 1 : 0,
+            S(c->cfg.dt), c->d_counters + 1);
+        GB_CK(cudaGetLastError());
+    }
+    StepParams<S> sp;
+    sp.dt         = S(c->cfg.dt);
+    sp.h          = S(c->cfg.integrator == GB_VELOCITY_VERLET && !c->verlet_started
+                          ? 0.5 * c->cfg.dt
+                          : c->cfg.dt);
+    sp.g          = mk<S>(S(c->cfg.gravity[0]), S(c->cfg.gravity[1]), S(c->cfg.gravity[2]));
+    sp.integrator = c->cfg.integrator;
+    sp.law_kind   = c->cfg.contact_law;
+    sp.has_kr     = c->has_kr ? 1 : 0;
+    sp.phases     = phases;
+    k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, s>>>(
+        c->n, st, tb, c->d_off[c->cur], po, sp, c->d_contacts, c->d_counters, c->d_counters + 1);
+    GB_CK(cudaGetLastError());
+    if(phases & PHASE_MOVE)
+    {
+        c->verlet_started = true;
+        c->steps_done++;
+    }
+    c->detect_valid = true;
+    c->prev_npairs  = c->npairs;
+    c->have_prev    = hist;
+    if(result)
+    {
+        std::vector<int> cnt(c->n);
+        GB_CK(cudaMemcpyAsync(cnt.data(), c->d_contacts, c->n * sizeof(int), cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaStreamSynchronize(s));
+        for(int i = 0; i < c->n; ++i)
+            result[i] += cnt[i];
+    }
+    return GB_OK;
+}
+
+template <typename S>
+int run_particles(gb_ctx* c, int phases)
+{
+    using St = store_t<S>;
+    StepParams<S> sp;
+    sp.dt         = S(c->cfg.dt);
+    sp.h          = S(c->cfg.integrator == GB_VELOCITY_VERLET && !c->verlet_started
+                          ? 0.5 * c->cfg.dt
+                          : c->cfg.dt);
+    sp.g          = mk<S>(S(c->cfg.gravity[0]), S(c->cfg.gravity[1]), S(c->cfg.gravity[2]));
+    sp.integrator = c->cfg.integrator;
+    sp.law_kind   = c->cfg.contact_law;
+    sp.has_kr     = c->has_kr ? 1 : 0;
+    sp.phases     = phases;
+    PairOut<St> po = pair_out<S>(c);
+    k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, c->stream>>>(
+        c->n, state_of<St>(c), tables_of<S>(c), c->d_off[c->cur], po, sp, nullptr, c->d_counters,
+        c->d_counters + 1);
+    GB_CK(cudaGetLastError());
+    if(phases & PHASE_MOVE)
+    {
+        c->verlet_started = true;
+        c->steps_done++;
+    }
+    return GB_OK;
+}
+
+template <typename F>
+int dispatch(gb_ctx* c, F&& f)
+{
+    switch(c->prec)
+    {
+        case GB_FP64:
+            return f((double)0);
+        case GB_MIXED:
+            return f((float)0);
+        case GB_FP64_STRICT:
+            return f(dstrict(0.0));
+        default:
+            return GB_E_INVALID_ARG;
+    }
+}
+
+int ready(gb_ctx* c)
+{
+    if(!c)
+        return GB_E_INVALID_ARG;
+    if(!(c->rb_set && c->law_set && c->tr_set && (c->nob == 0 || c->obs_set)))
+        return GB_E_NOT_READY;
+    return GB_OK;
+}
+
+int finish(gb_ctx* c)
+{
+    // read and clear the device status flags; out-of-domain and non-finite
+    // states are reported, capacity overflow is an error
+    int flags = 0;
+    GB_CK(cudaMemcpyAsync(&flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GB_CK(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
+    GB_CK(cudaStreamSynchronize(c->stream));
+    c->last.status_flags |= flags;
+    if(flags & kFlagCapacity)
+        return GB_E_CAPACITY;
+    if(flags & kFlagNonFinite)
+        return GB_E_NONFINITE;
+    if(flags & kFlagOutOfDomain)
+        return GB_E_OUT_OF_DOMAIN;
+    return GB_OK;
+}
+
+} // namespace
+
+// ============================================================================
+extern "C" {
+
+int gb_abi_version(void)
+{
+    return GB_ABI_VERSION;
+}
+
+const char* gb_status_string(int status)
+{
+    switch(status)
+    {
+        case GB_OK:
+            return "ok";
+        case GB_E_INVALID_ARG:
+            return "invalid argument";
+        case GB_E_CUDA:
+            return g_last_cuda != cudaSuccess ? cudaGetErrorString(g_last_cuda) : "CUDA error";
+        case GB_E_OUT_OF_MEMORY:
+            return "device out of memory";
+        case GB_E_NOT_READY:
+            return "context not fully set up";
+        case GB_E_OUT_OF_DOMAIN:
+            return "a particle centre left the linked-cell grid";
+        case GB_E_NONFINITE:
+            return "non-finite particle state";
+        case GB_E_NO_DEVICE:
+            return "no usable CUDA device";
+        case GB_E_CAPACITY:
+            return "buffer capacity exceeded";
+        case GB_E_UNSUPPORTED:
+            return "unsupported feature";
+        default:
+            return "unknown status";
+    }
+}
+
+gb_ctx* gb_create(const gb_config* cfg, int* status)
+{
+    auto fail = [&](int st) -> gb_ctx* {
+        if(status)
+            *status = st;
+        return nullptr;
+    };
+    if(!cfg || cfg->n_particles < 0 || cfg->n_rigid_bodies < 1 || cfg->n_obstacles < 0
+       || cfg->n_materials < 1 || !(cfg->dt > 0.0)
+       || (cfg->precision != GB_FP64 && cfg->precision != GB_MIXED
+           && cfg->precision != GB_FP64_STRICT)
+       || (cfg->contact_law != GB_LAW_HOOKE && cfg->contact_law != GB_LAW_HOOKE_HISTORY)
+       || (cfg->integrator != GB_FIRST_ORDER_EXPLICIT && cfg->integrator != GB_VELOCITY_VERLET))
+        return fail(GB_E_INVALID_ARG);
+    if(cfg->gjk_variant != GB_GJK_JH)
+        return fail(GB_E_UNSUPPORTED);
+    int ndev = 0;
+    if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
+        return fail(GB_E_NO_DEVICE);
+    if(cudaSetDevice(cfg->device) != cudaSuccess)
+        return fail(GB_E_NO_DEVICE);
+    gb_ctx* c = new gb_ctx;
+    c->cfg    = *cfg;
+    c->prec   = cfg->precision;
+    c->n      = cfg->n_particles;
+    c->nrb    = cfg->n_rigid_bodies;
+    c->nob    = cfg->n_obstacles;
+    c->nmat   = cfg->n_materials;
+    int st    = GB_OK;
+    if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        st = GB_E_CUDA;
+    if(st == GB_OK)
+        st = alloc_state(c);
+    if(st == GB_OK)
+        st = ensure_pairs(c, cfg->pair_capacity > 0 ? cfg->pair_capacity
+                                                    : std::max<int64_t>(1 << 16, 8 * (int64_t)c->n));
+    if(st != GB_OK)
+    {
+        gb_destroy(c);
+        return fail(st);
+    }
+    if(status)
+        *status = GB_OK;
+    return c;
+}
+
+int gb_destroy(gb_ctx* c)
+{
+    if(!c)
+        return GB_E_INVALID_ARG;
+    if(c->stream)
+        cudaStreamSynchronize(c->stream);
+    void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
+                    c->d_obs_mass, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
+                    c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
+                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_count,
+                    c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
+                    c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts};
+    for(void* p : ptrs)
+        if(p)
+            cudaFree(p);
+    if(c->h_pinned)
+        cudaFreeHost(c->h_pinned);
+    if(c->stream)
+        cudaStreamDestroy(c->stream);
+    delete c;
+    return GB_OK;
+}
+
+int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* vertices,
+                        int64_t n_vertices)
+{
+    if(!c || !rbs || n_vertices < 0 || (n_vertices && !vertices))
+        return GB_E_INVALID_ARG;
+    c->rbs.assign(rbs, rbs + c->nrb);
+    c->verts.assign(vertices, vertices + 3 * n_vertices);
+    c->props.resize(c->nrb);
+    double rmax = 0.0;
+    for(int i = 0; i < c->nrb; ++i)
+    {
+        const gb_convex& cv = rbs[i].convex;
+        if(cv.type == GB_POLYHEDRON
+           && (cv.first_vertex < 0 || cv.first_vertex + cv.n_vertices > n_vertices))
+            return GB_E_INVALID_ARG;
+        if(cv.type == GB_CYLINDER || cv.type == GB_CONE)
+            return GB_E_UNSUPPORTED;
+        if(rbs[i].material < 0 || rbs[i].material >= c->nmat)
+            return GB_E_INVALID_ARG;
+        GB_TRY(gb_rigid_body_properties(&rbs[i], vertices, &c->props[i]));
+        rmax = std::max(rmax, c->props[i].circumscribed_radius); // Grains.cpp:226-231
+    }
+    // linked cell: cell = factor * 2 * max circumscribed radius (Grains.cpp:233-246)
+    double coeff = c->cfg.cell_size_factor;
+    if(coeff < 1.0)
+        coeff = 1.0;
+    c->cell = coeff * 2.0 * rmax;
+    for(int k = 0; k < 3; ++k)
+    {
+        c->lc_max[k] = c->cfg.max_coordinate[k] + (c->cfg.pad_grid ? c->cell : 0.0);
+        double t     = 1.e-10; // LinkedCell.cpp:23-28
+        t += c->lc_max[k] - c->cfg.origin[k];
+        t /= c->cell;
+        if(!(t >= 1.0) || t > 4.0e9)
+            return GB_E_INVALID_ARG;
+        c->dims[k] = (uint32_t)t;
+    }
+    const uint64_t nc = (uint64_t)c->dims[0] * c->dims[1] * c->dims[2];
+    if(nc == 0 || nc >= 0xFFFFFFF0ull)
+        return GB_E_INVALID_ARG;
+    c->ncells   = (uint32_t)nc;
+    c->key_bits = 0;
+    while(c->key_bits < 32 && (1ull << c->key_bits) < nc)
+        ++c->key_bits;
+    dfree(c->d_cstart);
+    GB_TRY(dalloc(&c->d_cstart, (size_t)nc + 1));
+    int st = c->prec == GB_MIXED ? upload_tables<float>(c) : upload_tables<double>(c);
+    if(st)
+        return st;
+    c->rb_set = true;
+    return GB_OK;
+}
+
+int gb_get_rigid_body_props(gb_ctx* c, int32_t rb, gb_rigid_body_props* out)
+{
+    if(!c || !out || rb < 0 || rb >= c->nrb || !c->rb_set)
+        return GB_E_INVALID_ARG;
+    *out = c->props[rb];
+    return GB_OK;
+}
+
+int gb_set_contact_models(gb_ctx* c, const gb_contact_model* table)
+{
+    if(!c || !table)
+        return GB_E_INVALID_ARG;
+    c->laws.assign(table, table + c->nmat * (c->nmat + 1) / 2);
+    for(auto& m : c->laws)
+        if(!(m.kn >= 0.0) || !(m.en > 0.0 && m.en <= 1.0))
+            return GB_E_INVALID_ARG;
+    int st = c->prec == GB_MIXED ? upload_laws<float>(c) : upload_laws<double>(c);
+    if(st)
+        return st;
+    c->law_set = true;
+    return GB_OK;
+}
+
+int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* transforms)
+{
+    if(!c || (c->nob && (!obst || !transforms)))
+        return GB_E_INVALID_ARG;
+    c->obs.assign(obst, obst + c->nob);
+    c->obs_tr.assign(transforms, transforms + 12 * (size_t)c->nob);
+    c->obs_props.resize(c->nob);
+    for(int i = 0; i < c->nob; ++i)
+    {
+        if(obst[i].convex.type == GB_POLYHEDRON || obst[i].convex.type == GB_CYLINDER
+           || obst[i].convex.type == GB_CONE)
+            return GB_E_UNSUPPORTED;
+        if(obst[i].material < 0 || obst[i].material >= c->nmat)
+            return GB_E_INVALID_ARG;
+        GB_TRY(gb_rigid_body_properties(&obst[i], nullptr, &c->obs_props[i]));
+    }
+    int st = c->prec == GB_MIXED ? upload_obstacles<float>(c) : upload_obstacles<double>(c);
+    if(st)
+        return st;
+    c->obs_set = true;
+    return GB_OK;
+}
+
+int gb_set_rigid_body_ids(gb_ctx* c, const uint32_t* ids)
+{
+    if(!c || !ids)
+        return GB_E_INVALID_ARG;
+    for(int i = 0; i < c->n; ++i)
+        if(ids[i] >= (uint32_t)c->nrb)
+            return GB_E_INVALID_ARG;
+    GB_CK(cudaMemcpy(c->d_rb_id, ids, c->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    c->ids_set = true;
+    return GB_OK;
+}
+
+int gb_set_transforms(gb_ctx* c, const double* t)
+{
+    if(!c || !t)
+        return GB_E_INVALID_ARG;
+    const size_t n = c->n;
+    std::vector<double> pos(3 * n);
+    for(size_t i = 0; i < n; ++i)
+        for(int k = 0; k < 3; ++k)
+            pos[k * n + i] = t[12 * i + 9 + k];
+    GB_CK(cudaMemcpy(c->d_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if(c->prec == GB_MIXED)
+    {
+        std::vector<float> q(4 * n);
+        for(size_t i = 0; i < n; ++i)
+        {
+            double qq[4];
+            basis_to_quat(t + 12 * i, qq);
+            for(int k = 0; k < 4; ++k)
+                q[k * n + i] = (float)qq[k];
+        }
+        GB_CK(cudaMemcpy(c->d_rot, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        std::vector<double> b(9 * n);
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 9; ++k)
+                b[k * n + i] = t[12 * i + k];
+        GB_CK(cudaMemcpy(c->d_rot, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    c->tr_set      = true;
+    c->links_valid = c->detect_valid = false;
+    return GB_OK;
+}
+
+static int set_soa6(gb_ctx* c, const double* kin, void* a, void* b)
+{
+    const size_t n = c->n;
+    if(c->prec == GB_MIXED)
+    {
+        std::vector<float> v(3 * n), w(3 * n);
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                v[k * n + i] = (float)kin[6 * i + k];
+                w[k * n + i] = (float)kin[6 * i + 3 + k];
+            }
+        GB_CK(cudaMemcpy(a, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+        GB_CK(cudaMemcpy(b, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        std::vector<double> v(3 * n), w(3 * n);
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                v[k * n + i] = kin[6 * i + k];
+                w[k * n + i] = kin[6 * i + 3 + k];
+            }
+        GB_CK(cudaMemcpy(a, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        GB_CK(cudaMemcpy(b, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return GB_OK;
+}
+
+static int get_soa6(gb_ctx* c, double* kin, const void* a, const void* b)
+{
+    const size_t n = c->n;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    if(c->prec == GB_MIXED)
+    {
+        std::vector<float> v(3 * n), w(3 * n);
+        GB_CK(cudaMemcpy(v.data(), a, v.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        GB_CK(cudaMemcpy(w.data(), b, w.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                kin[6 * i + k]     = v[k * n + i];
+                kin[6 * i + 3 + k] = w[k * n + i];
+            }
+    }
+    else
+    {
+        std::vector<double> v(3 * n), w(3 * n);
+        GB_CK(cudaMemcpy(v.data(), a, v.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        GB_CK(cudaMemcpy(w.data(), b, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                kin[6 * i + k]     = v[k * n + i];
+                kin[6 * i + 3 + k] = w[k * n + i];
+            }
+    }
+    return GB_OK;
+}
+
+int gb_set_velocities(gb_ctx* c, const double* kin)
+{
+    if(!c || !kin)
+        return GB_E_INVALID_ARG;
+    GB_TRY(set_soa6(c, kin, c->d_vel, c->d_omg));
+    c->vel_set = true;
+    return GB_OK;
+}
+
+int gb_get_velocities(gb_ctx* c, double* kin)
+{
+    if(!c || !kin)
+        return GB_E_INVALID_ARG;
+    return get_soa6(c, kin, c->d_vel, c->d_omg);
+}
+
+int gb_get_torces(gb_ctx* c, double* torce)
+{
+    if(!c || !torce)
+        return GB_E_INVALID_ARG;
+    return get_soa6(c, torce, c->d_frc, c->d_trq);
+}
+
+int gb_get_transforms(gb_ctx* c, double* t)
+{
+    if(!c || !t)
+        return GB_E_INVALID_ARG;
+    const size_t n = c->n;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> pos(3 * n);
+    GB_CK(cudaMemcpy(pos.data(), c->d_pos, pos.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if(c->prec == GB_MIXED)
+    {
+        std::vector<float> q(4 * n);
+        GB_CK(cudaMemcpy(q.data(), c->d_rot, q.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for(size_t i = 0; i < n; ++i)
+        {
+            const double qq[4] = {q[i], q[n + i], q[2 * n + i], q[3 * n + i]};
+            quat_to_basis(qq, t + 12 * i);
+        }
+    }
+    else
+    {
+        std::vector<double> b(9 * n);
+        GB_CK(cudaMemcpy(b.data(), c->d_rot, b.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for(size_t i = 0; i < n; ++i)
+            for(int k = 0; k < 9; ++k)
+                t[12 * i + k] = b[k * n + i];
+    }
+    for(size_t i = 0; i < n; ++i)
+        for(int k = 0; k < 3; ++k)
+            t[12 * i + 9 + k] = pos[k * n + i];
+    return GB_OK;
+}
+
+int gb_update_links(gb_ctx* c)
+{
+    GB_TRY(ready(c));
+    GB_TRY(broad_phase(c));
+    return finish(c);
+}
+
+int gb_detect_collision_and_compute_contact_forces(gb_ctx* c, int32_t* result)
+{
+    GB_TRY(ready(c));
+    GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, PHASE_DETECT, result); }));
+    c->torce_dirty = true;
+    return finish(c);
+}
+
+int gb_add_external_forces(gb_ctx* c)
+{
+    GB_TRY(ready(c));
+    GB_TRY(dispatch(c, [&](auto z) { return run_particles<decltype(z)>(c, PHASE_GRAVITY); }));
+    c->torce_dirty = true;
+    return finish(c);
+}
+
+int gb_move_particles(gb_ctx* c)
+{
+    GB_TRY(ready(c));
+    GB_TRY(dispatch(c, [&](auto z) { return run_particles<decltype(z)>(c, PHASE_MOVE); }));
+    c->torce_dirty      = false;
+    c->links_valid      = false;
+    return finish(c);
+}
+
+int gb_step(gb_ctx* c, int32_t n_steps)
+{
+    GB_TRY(ready(c));
+    if(n_steps < 0)
+        return GB_E_INVALID_ARG;
+    if(c->torce_dirty)
+    {
+        const size_t ss = store_size(c->prec);
+        GB_CK(cudaMemsetAsync(c->d_frc, 0, 3 * (size_t)c->n * ss, c->stream));
+        GB_CK(cudaMemsetAsync(c->d_trq, 0, 3 * (size_t)c->n * ss, c->stream));
+        c->torce_dirty = false;
+    }
+    GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
+    int worst = GB_OK;
+    for(int32_t s = 0; s < n_steps; ++s)
+    {
+        GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, PHASE_STEP, nullptr); }));
+        c->links_valid = false;
+    }
+    int st = finish(c);
+    if(st != GB_OK)
+        worst = st;
+    return worst;
+}
+
+int gb_synchronize(gb_ctx* c)
+{
+    if(!c)
+        return GB_E_INVALID_ARG;
+    return finish(c);
+}
+
+int gb_get_stats(gb_ctx* c, gb_stats* o)
+{
+    if(!c || !o)
+        return GB_E_INVALID_ARG;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    unsigned long long cnt[4];
+    GB_CK(cudaMemcpy(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    std::memset(o, 0, sizeof(*o));
+    o->steps_done        = c->steps_done;
+    o->candidate_pairs   = c->npairs;
+    o->obstacle_contacts = (int64_t)cnt[0];
+    o->gjk_iterations    = (int64_t)cnt[1];
+    if(c->detect_valid && c->npairs > 0)
+    {
+        std::vector<uint8_t> pc(c->npairs);
+        GB_CK(cudaMemcpy(pc.data(), c->d_pc, c->npairs, cudaMemcpyDeviceToHost));
+        int64_t k = 0;
+        for(uint8_t b : pc)
+            k += b;
+        o->contacts = k;
+    }
+    o->status_flags = c->last.status_flags;
+    o->n_cells      = (int32_t)c->ncells;
+    for(int k = 0; k < 3; ++k)
+    {
+        o->cells_per_dir[k] = (int32_t)c->dims[k];
+        o->grid_max[k]      = c->lc_max[k];
+    }
+    o->key_bits  = c->key_bits;
+    o->cell_size = c->cell;
+    return GB_OK;
+}
+
+int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t* count)
+{
+    if(!c || !count)
+        return GB_E_INVALID_ARG;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    const int64_t n = c->n;
+    auto copy_u32 = [&](const uint32_t* d, int64_t m) -> int {
+        *count = m;
+        if(out && capacity > 0)
+            GB_CK(cudaMemcpy(out, d, std::min(m, capacity) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        return GB_OK;
+    };
+    switch(kind)
+    {
+        case GB_DUMP_NEIGHBORS:
+        {
+            // the reference's 27-entry neighbour table (LinkedCell.cpp:35-72)
+            if(!c->rb_set)
+                return GB_E_NOT_READY;
+            const int64_t m = (int64_t)c->ncells * 27;
+            *count          = m;
+            if(!out)
+                return GB_OK;
+            uint32_t*      o  = (uint32_t*)out;
+            const uint32_t nx = c->dims[0], ny = c->dims[1], nz = c->dims[2];
+            int64_t        w  = 0;
+            for(uint32_t h = 0; h < c->ncells && w < capacity; ++h)
+            {
+                const int cx = h % nx, cy = (h / nx) % ny, cz = h / (nx * ny);
+                for(int k = -1; k < 2; ++k)
+                    for(int j = -1; j < 2; ++j)
+                        for(int i = -1; i < 2; ++i)
+                        {
+                            const int x = cx + i, y = cy + j, z = cz + k;
+                            const bool in = x >= 0 && x < (int)nx && y >= 0 && y < (int)ny && z >= 0
+                                            && z < (int)nz;
+                            if(w < capacity)
+                                o[w] = in ? (uint32_t)x + (uint32_t)y * nx + (uint32_t)z * nx * ny
+                                          : UINT32_MAX;
+                            ++w;
+                        }
+            }
+            return GB_OK;
+        }
+        case GB_DUMP_CELL_HASH:
+            if(!c->links_valid && !c->detect_valid)
+                return GB_E_NOT_READY;
+            return copy_u32(c->d_hash, n);
+        case GB_DUMP_SORTED_IDS:
+            if(!c->links_valid && !c->detect_valid)
+                return GB_E_NOT_READY;
+            return copy_u32(c->d_sids, n);
+        case GB_DUMP_CELL_START:
+            if(!c->links_valid && !c->detect_valid)
+                return GB_E_NOT_READY;
+            return copy_u32(c->d_cstart, (int64_t)c->ncells + 1);
+        case GB_DUMP_CANDIDATE_PAIRS:
+        case GB_DUMP_CONTACT_PAIRS:
+        case GB_DUMP_CONTACT_INFO:
+        {
+            if(!c->detect_valid)
+                return GB_E_NOT_READY;
+            if(kind == GB_DUMP_CONTACT_INFO && !c->d_info)
+                return GB_E_UNSUPPORTED;
+            const int64_t         P = c->npairs;
+            std::vector<uint32_t> a(P), b(P);
+            std::vector<uint8_t>  pc(P);
+            if(P)
+            {
+                GB_CK(cudaMemcpy(a.data(), c->d_pa, P * 4, cudaMemcpyDeviceToHost));
+                GB_CK(cudaMemcpy(b.data(), c->d_pb[c->cur], P * 4, cudaMemcpyDeviceToHost));
+                GB_CK(cudaMemcpy(pc.data(), c->d_pc, P, cudaMemcpyDeviceToHost));
+            }
+            std::vector<double> info;
+            if(kind == GB_DUMP_CONTACT_INFO && P)
+            {
+                info.resize(7 * P);
+                GB_CK(cudaMemcpy(info.data(), c->d_info, 7 * P * sizeof(double), cudaMemcpyDeviceToHost));
+            }
+            int64_t w = 0;
+            for(int64_t p = 0; p < P; ++p)
+            {
+                if(kind != GB_DUMP_CANDIDATE_PAIRS && !pc[p])
+                    continue;
+                if(kind == GB_DUMP_CONTACT_INFO)
+                {
+                    if(out && 7 * w + 7 <= capacity)
+                        std::memcpy((double*)out + 7 * w, &info[7 * p], 7 * sizeof(double));
+                }
+                else if(out && 2 * w + 2 <= capacity)
+                {
+                    ((uint32_t*)out)[2 * w]     = a[p];
+                    ((uint32_t*)out)[2 * w + 1] = b[p];
+                }
+                ++w;
+            }
+            *count = kind == GB_DUMP_CONTACT_INFO ? 7 * w : 2 * w;
+            return GB_OK;
+        }
+        default:
+            return GB_E_INVALID_ARG;
+    }
+}
+
+int gb_device_pointer(gb_ctx* c, const char* name, void** ptr)
+{
+    if(!c || !name || !ptr)
+        return GB_E_INVALID_ARG;
+    const std::string s(name);
+    const size_t      n  = c->n;
+    const size_t      ss = store_size(c->prec);
+    const char*       axes = "xyz";
+    for(int k = 0; k < 3; ++k)
+    {
+        const std::string ax(1, axes[k]);
+        if(s == "pos_" + ax)
+            return *ptr = c->d_pos + k * n, GB_OK;
+        if(s == "vel_" + ax)
+            return *ptr = (char*)c->d_vel + k * n * ss, GB_OK;
+        if(s == "omega_" + ax)
+            return *ptr = (char*)c->d_omg + k * n * ss, GB_OK;
+        if(s == "force_" + ax)
+            return *ptr = (char*)c->d_frc + k * n * ss, GB_OK;
+        if(s == "torque_" + ax)
+            return *ptr = (char*)c->d_trq + k * n * ss, GB_OK;
+    }
+    if(s == "rb_id")
+        return *ptr = c->d_rb_id, GB_OK;
+    if(s == "rotation")
+        return *ptr = c->d_rot, GB_OK;
+    return GB_E_INVALID_ARG;
+}
+
+} // extern "C"

@@ -1,0 +1,411 @@
+// gb_geom.cuh -- device rigid-body tables, support functions, OBB test and
+// GJK with Johnson's sub-algorithm.
+#pragma once
+
+#include "gb_math.cuh"
+#include "../../include/grains_b200.h"
+
+namespace gb
+{
+
+// Shape part of a rigid body, as read by the narrow phase.  k[] caches the
+// superquadric ratios and exponents that Superquadric::support recomputes
+// on every call (Superquadric.cpp:169-205); each is the same IEEE value the
+// reference computes inline.
+template <typename St>
+struct RBShape
+{
+    int32_t type;
+    int32_t nverts;
+    int64_t first_vert;
+    St      p[5];
+    St      k[8]; // b/a, c/a, c/b, 1/(n1-1), 1/(n2-1), (n1-n2)/(n2 (n1-1)), n1/n2, 1/n1
+    St      crust;
+    St      rcirc;
+    St      bb[3];
+    int32_t material;
+    int32_t pad;
+};
+
+// Inertial part, as read by the integrator (RigidBody.hh:28-37).
+template <typename St>
+struct RBInertia
+{
+    St mass;
+    St I[6];
+    St I1[6];
+    St pad;
+};
+
+template <typename St>
+struct Vert
+{
+    St x, y, z, w;
+};
+
+template <typename S>
+struct Body
+{
+    int                      type;
+    int                      nverts;
+    const Vert<store_t<S>>*  verts;
+    S                        p[5];
+    S                        k[8];
+    S                        crust, rcirc;
+    V3<S>                    bb;
+};
+
+template <typename S>
+GB_D Body<S> load_body(const RBShape<store_t<S>>* __restrict__ tab, uint32_t rb,
+                       const Vert<store_t<S>>* __restrict__ verts)
+{
+    const RBShape<store_t<S>>* r = tab + rb;
+    Body<S>                    b;
+    b.type   = __ldg(&r->type);
+    b.nverts = __ldg(&r->nverts);
+    b.verts  = verts + __ldg(&r->first_vert);
+#pragma unroll
+    for(int i = 0; i < 5; ++i)
+        b.p[i] = S(__ldg(&r->p[i]));
+#pragma unroll
+    for(int i = 0; i < 8; ++i)
+        b.k[i] = S(__ldg(&r->k[i]));
+    b.crust = S(__ldg(&r->crust));
+    b.rcirc = S(__ldg(&r->rcirc));
+    b.bb    = mk<S>(S(__ldg(&r->bb[0])), S(__ldg(&r->bb[1])), S(__ldg(&r->bb[2])));
+    return b;
+}
+
+template <typename S>
+GB_D S sgn(S x)
+{
+    // MiscMath.hh:68-72, returned as the scalar type
+    return S(double((S(0.0) < x) - (x < S(0.0))));
+}
+
+// Superquadric::support (Grains/Geometry/src/Superquadric.cpp:169-205)
+template <typename S>
+GB_D V3<S> support_sq(const Body<S>& b, const V3<S>& v)
+{
+    const S abvx = s_fabs(v.x), abvy = s_fabs(v.y), abvz = s_fabs(v.z);
+    const S signx = sgn(v.x), signy = sgn(v.y), signz = sgn(v.z);
+    const S one = S(1.0);
+    if(abvx == S(0.0))
+    {
+        if(abvy == S(0.0))
+            return mk<S>(S(0.0), S(0.0), signz * b.p[2]);
+        const S alpha = s_pow(b.k[2] * abvz / abvy, b.k[3]);
+        const S yt    = one / s_pow(one + s_pow(alpha, b.p[3]), b.k[7]);
+        return mk<S>(S(0.0), signy * b.p[1] * yt, signz * alpha * b.p[2] * yt);
+    }
+    const S alpha = s_pow(b.k[0] * abvy / abvx, b.k[4]);
+    const S temp  = one + s_pow(alpha, b.p[4]);
+    const S gamma = s_pow(temp, b.k[5]);
+    const S beta  = gamma * s_pow(b.k[1] * abvz / abvx, b.k[3]);
+    const S xt    = one / s_pow(s_pow(temp, b.k[6]) + s_pow(beta, b.p[3]), b.k[7]);
+    return mk<S>(signx * b.p[0] * xt, signy * alpha * b.p[1] * xt, signz * beta * b.p[2] * xt);
+}
+
+// NEW (no reference shape): argmax over the vertices, first index on ties.
+template <typename S>
+GB_D V3<S> support_poly(const Body<S>& b, const V3<S>& v)
+{
+    const Vert<store_t<S>>* __restrict__ pv = b.verts;
+    Vert<store_t<S>> q0 = pv[0];
+    V3<S>            best = mk<S>(S(q0.x), S(q0.y), S(q0.z));
+    S                bd   = dot(best, v);
+    for(int i = 1; i < b.nverts; ++i)
+    {
+        Vert<store_t<S>> q = pv[i];
+        V3<S>            c = mk<S>(S(q.x), S(q.y), S(q.z));
+        S                d = dot(c, v);
+        if(d > bd)
+        {
+            bd   = d;
+            best = c;
+        }
+    }
+    return best;
+}
+
+template <typename S>
+GB_D V3<S> support(const Body<S>& b, const V3<S>& v)
+{
+    switch(b.type)
+    {
+        case GB_SUPERQUADRIC:
+            return support_sq(b, v);
+        case GB_POLYHEDRON:
+            return support_poly(b, v);
+        case GB_BOX: // Box::support (Box.cpp:129-134)
+            return mk<S>(v.x < S(0.0) ? -b.p[0] : b.p[0], v.y < S(0.0) ? -b.p[1] : b.p[1],
+                         v.z < S(0.0) ? -b.p[2] : b.p[2]);
+        case GB_SPHERE: // Sphere::support = r v/|v| (Sphere.cpp:111)
+        {
+            const S n = norm(v);
+            return b.p[0] * mk<S>(v.x / n, v.y / n, v.z / n);
+        }
+        case GB_RECTANGLE: // Rectangle::support (Rectangle.cpp:115-121)
+            return mk<S>(v.x < S(0.0) ? -b.p[0] : b.p[0], v.y < S(0.0) ? -b.p[1] : b.p[1],
+                         S(0.0));
+        default:
+            return mk<S>(S(0.0), S(0.0), S(0.0));
+    }
+}
+
+// intersectOrientedBoundingBox (Grains/CollisionDetection/src/OBB.cpp:32-94):
+// `cen` is B's origin relative to A's in world axes, RA/RB the bases.
+template <typename S>
+GB_D bool obb_overlap(const V3<S>& a, const V3<S>& b, const M3<S>& RA, const M3<S>& RB,
+                      const V3<S>& d)
+{
+    const M3<S> oriT = transpose(RA);
+    const V3<S> cen  = mul(oriT, d);
+    const M3<S> ori  = mul(oriT, RB);
+    M3<S>       oa;
+#pragma unroll
+    for(int i = 0; i < 9; ++i)
+        oa.m[i] = s_fabs(ori.m[i]) + k_loweps<S>();
+    const S A[3] = {a.x, a.y, a.z}, B[3] = {b.x, b.y, b.z}, c[3] = {cen.x, cen.y, cen.z};
+#define O_(i, j) ori.m[3 * (i) + (j)]
+#define OA_(i, j) oa.m[3 * (i) + (j)]
+#pragma unroll
+    for(int i = 0; i < 3; ++i)
+        if(s_fabs(c[i]) > (A[i] + B[0] * OA_(i, 0) + B[1] * OA_(i, 1) + B[2] * OA_(i, 2)))
+            return false;
+#pragma unroll
+    for(int i = 0; i < 3; ++i)
+        if(s_fabs(c[0] * O_(0, i) + c[1] * O_(1, i) + c[2] * O_(2, i))
+           > (B[i] + A[0] * OA_(0, i) + A[1] * OA_(1, i) + A[2] * OA_(2, i)))
+            return false;
+#pragma unroll
+    for(int j = 0; j < 3; ++j)
+#pragma unroll
+        for(int i = 0; i < 3; ++i) // TESTCASE3(i, j), j outer as in the reference
+            if(s_fabs(c[(i + 2) % 3] * O_((i + 1) % 3, j) - c[(i + 1) % 3] * O_((i + 2) % 3, j))
+               > (A[(i + 1) % 3] * OA_((i + 2) % 3, j) + A[(i + 2) % 3] * OA_((i + 1) % 3, j)
+                  + B[(j + 1) % 3] * OA_(i, (j + 2) % 3) + B[(j + 2) % 3] * OA_(i, (j + 1) % 3)))
+                return false;
+#undef O_
+#undef OA_
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// GJK with Johnson's distance sub-algorithm and cached sub-determinants
+// (Grains/CollisionDetection/src/GJK_JH.cpp:9-391).  One thread per pair.
+template <typename S>
+struct JH
+{
+    S     det[16][4];
+    S     dp[4][4];
+    V3<S> y[4];
+
+    GB_D void compute_det(unsigned bits, unsigned last, unsigned last_bit, unsigned all_bits)
+    {
+        // computeDet (GJK_JH.cpp:9-63)
+        for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+            if(bits & bit)
+                dp[i][last] = dp[last][i] = dot(y[i], y[last]);
+        dp[last][last] = dot(y[last], y[last]);
+        det[last_bit][last] = S(1.0);
+        for(unsigned j = 0, sj = 1; j < 4; ++j, sj <<= 1)
+        {
+            if(bits & sj)
+            {
+                unsigned s2   = sj | last_bit;
+                det[s2][j]    = dp[last][last] - dp[last][j];
+                det[s2][last] = dp[j][j] - dp[j][last];
+                for(unsigned k = 0, sk = 1; k < j; ++k, sk <<= 1)
+                {
+                    if(bits & sk)
+                    {
+                        unsigned s3 = sk | s2;
+                        det[s3][k]  = det[s2][j] * (dp[j][j] - dp[j][k])
+                                     + det[s2][last] * (dp[last][j] - dp[last][k]);
+                        det[s3][j] = det[sk | last_bit][k] * (dp[k][k] - dp[k][j])
+                                     + det[sk | last_bit][last] * (dp[last][k] - dp[last][j]);
+                        det[s3][last] = det[sk | sj][k] * (dp[k][k] - dp[k][last])
+                                        + det[sk | sj][j] * (dp[j][k] - dp[j][last]);
+                    }
+                }
+            }
+        }
+        if(all_bits == 15)
+        {
+            det[15][0] = det[14][1] * (dp[1][1] - dp[1][0]) + det[14][2] * (dp[2][1] - dp[2][0])
+                         + det[14][3] * (dp[3][1] - dp[3][0]);
+            det[15][1] = det[13][0] * (dp[0][0] - dp[0][1]) + det[13][2] * (dp[2][0] - dp[2][1])
+                         + det[13][3] * (dp[3][0] - dp[3][1]);
+            det[15][2] = det[11][0] * (dp[0][0] - dp[0][2]) + det[11][1] * (dp[1][0] - dp[1][2])
+                         + det[11][3] * (dp[3][0] - dp[3][2]);
+            det[15][3] = det[7][0] * (dp[0][0] - dp[0][3]) + det[7][1] * (dp[1][0] - dp[1][3])
+                         + det[7][2] * (dp[2][0] - dp[2][3]);
+        }
+    }
+
+    GB_D bool valid(unsigned s, unsigned all_bits) const
+    {
+        for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+        {
+            if(all_bits & bit)
+            {
+                if(s & bit)
+                {
+                    if(det[s][i] <= k_eps<S>())
+                        return false;
+                }
+                else if(det[s | bit][i] > S(0.0))
+                    return false;
+            }
+        }
+        return true;
+    }
+
+    GB_D V3<S> compute_vector(unsigned bits) const
+    {
+        S     sum = S(0.0);
+        V3<S> v   = zero3<S>();
+        for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+            if(bits & bit)
+            {
+                sum = sum + det[bits][i];
+                v   = v + det[bits][i] * y[i];
+            }
+        return (S(1.0) / sum) * v;
+    }
+
+    GB_D bool proper(unsigned s) const
+    {
+        for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+            if((s & bit) && det[s][i] <= k_eps<S>())
+                return false;
+        return true;
+    }
+
+    GB_D bool closest(unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits,
+                      V3<S>& v)
+    {
+        compute_det(bits, last, last_bit, all_bits);
+        for(unsigned s = bits; s; --s)
+            if((s & bits) == s && valid(s | last_bit, all_bits))
+            {
+                bits = s | last_bit;
+                v    = compute_vector(bits);
+                return true;
+            }
+        if(valid(last_bit, all_bits))
+        {
+            bits = last_bit;
+            v    = y[last];
+            return true;
+        }
+        // backup procedure (GJK_JH.cpp:173-193)
+        S min_dist2 = S(INFINITY);
+        for(unsigned s = all_bits; s; --s)
+            if((s & all_bits) == s && proper(s))
+            {
+                V3<S> u     = compute_vector(s);
+                S     dist2 = norm2(u);
+                if(dist2 < min_dist2)
+                {
+                    min_dist2 = dist2;
+                    bits      = s;
+                    v         = u;
+                }
+            }
+        return false;
+    }
+
+    GB_D bool degenerate(unsigned all_bits, const V3<S>& w) const
+    {
+        for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+            if((all_bits & bit) && eq3(y[i], w))
+                return true;
+        return false;
+    }
+};
+
+template <typename S>
+struct GjkResult
+{
+    S     dist;
+    V3<S> pa, pb; // closest points in A's and B's local frames
+    int   iters;
+};
+
+// computeClosestPoints_GJK_JH (GJK_JH.cpp:310-391), in A's frame with b2a.
+template <typename S>
+GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
+{
+    unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
+    V3<S>    p[4], q[4];
+    JH<S>    jh;
+#pragma unroll
+    for(int i = 0; i < 16; ++i)
+#pragma unroll
+        for(int j = 0; j < 4; ++j)
+            jh.det[i][j] = S(0.0);
+#pragma unroll
+    for(int i = 0; i < 4; ++i)
+    {
+#pragma unroll
+        for(int j = 0; j < 4; ++j)
+            jh.dp[i][j] = S(0.0);
+        p[i] = q[i] = jh.y[i] = zero3<S>();
+    }
+    S       mu = S(0.0);
+    int     num_iterations = 0;
+    const S rel_error      = k_loweps<S>();
+    const S abs_error      = S(1.e-4) * rel_error;
+
+    V3<S> v    = support(A, zero3<S>()) - apply(b2a, support(B, zero3<S>()));
+    V3<S> w;
+    S     dist = norm(v);
+    while(bits < 15 && dist > k_higheps<S>() && num_iterations < 1000)
+    {
+        last     = 0;
+        last_bit = 1;
+        while(bits & last_bit)
+        {
+            ++last;
+            last_bit <<= 1;
+        }
+        p[last] = support(A, -v);
+        q[last] = support(B, mul_t(b2a.R, v));
+        w       = p[last] - apply(b2a, q[last]);
+        const S g = dot(v, w) / dist;
+        if(mu < g)
+            mu = g;
+        if(dist - mu <= dist * rel_error || mu < abs_error)
+            break;
+        if(jh.degenerate(all_bits, w))
+            break;
+        jh.y[last] = w;
+        all_bits   = bits | last_bit;
+        ++num_iterations;
+        if(!jh.closest(bits, last, last_bit, all_bits, v))
+            break;
+        dist = norm(v);
+    }
+    // computePoints (GJK_JH.cpp:108-130)
+    GjkResult<S> r;
+    S            sum = S(0.0);
+    r.pa             = zero3<S>();
+    r.pb             = zero3<S>();
+    for(unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+        if(bits & bit)
+        {
+            sum  = sum + jh.det[bits][i];
+            r.pa = r.pa + jh.det[bits][i] * p[i];
+            r.pb = r.pb + jh.det[bits][i] * q[i];
+        }
+    const S s = S(1.0) / sum;
+    r.pa      = s * r.pa;
+    r.pb      = s * r.pb;
+    r.dist    = dist;
+    r.iters   = num_iterations;
+    return r;
+}
+
+} // namespace gb

@@ -1,0 +1,547 @@
+// gb_step.cuh -- candidate pairs, narrow phase + contact law, and the fused
+// per-particle reduction / walls / gravity / integration kernel.
+#pragma once
+
+#include "gb_broadphase.cuh"
+#include "gb_dem.cuh"
+
+namespace gb
+{
+
+// Particle state on the device, structure of arrays.  Positions are FP64 in
+// every mode.  Orientation: in the FP64 modes the 3x3 basis of Grains'
+// Transform3 (9 arrays, row-major), updated exactly as
+// Transform3::composeLeftByRotation; in the mixed mode a unit quaternion
+// (w, x, y, z) in FP32.
+template <typename St>
+struct State
+{
+    double*   pos[3];
+    St*       rot[9]; // basis (FP64 modes) or quaternion in rot[0..3] (mixed)
+    St*       vel[3];
+    St*       omg[3];
+    St*       frc[3];
+    St*       trq[3];
+    uint32_t* rb_id;
+};
+
+template <typename S>
+struct Tables
+{
+    const RBShape<store_t<S>>*   shape;
+    const RBInertia<store_t<S>>* inertia;
+    const Vert<store_t<S>>*      verts;
+    const Law<store_t<S>>*       law; // material-pair table
+    const RBShape<store_t<S>>*   obs_shape;
+    const double*                obs_tr; // 12 per obstacle (basis, origin)
+    const double*                obs_mass;
+    int                          n_obs;
+};
+
+template <typename S>
+GB_D constexpr bool is_mixed()
+{
+    return sizeof(store_t<S>) == 4;
+}
+
+template <typename S>
+GB_D M3<S> load_rot(const State<store_t<S>>& st, uint32_t i)
+{
+    if constexpr(is_mixed<S>())
+        return quat_to_matrix<S>(S(st.rot[0][i]), S(st.rot[1][i]), S(st.rot[2][i]),
+                                 S(st.rot[3][i]));
+    else
+    {
+        M3<S> R;
+#pragma unroll
+        for(int k = 0; k < 9; ++k)
+            R.m[k] = S(st.rot[k][i]);
+        return R;
+    }
+}
+
+template <typename S>
+GB_D V3<S> load3(store_t<S>* const a[3], uint32_t i)
+{
+    return mk<S>(S(a[0][i]), S(a[1][i]), S(a[2][i]));
+}
+
+template <typename S>
+GB_D Law<S> load_law(const Law<store_t<S>>* t, int ma, int mb)
+{
+    // ContactForceModelBuilderFactory::computeHash (ContactForceModelBuilderFactory.cpp:77-83)
+    const unsigned s = ma < mb ? ma : mb, l = ma < mb ? mb : ma;
+    const Law<store_t<S>> L = t[l * (l + 1) / 2 + s];
+    Law<S>                r;
+    r.kn   = S(L.kn);
+    r.muen = S(L.muen);
+    r.etat = S(L.etat);
+    r.muc  = S(L.muc);
+    r.kr   = S(L.kr);
+    r.kt   = S(L.kt);
+    return r;
+}
+
+// ---- candidate pairs ----------------------------------------------------------
+// One thread per particle in cell-sorted order.  Enumerates the 27 neighbour
+// cells in the reference's order (k = z outer, j = y, i = x inner; the
+// neighbour table of LinkedCell.cpp:41-70) and the particles of each cell in
+// ascending id, keeping ordered pairs (A, B != A) whose bounding spheres
+// overlap: norm(xB - xA) - (rA + rB) < 0 (CollisionDetection.cpp:209-211).
+// COUNT: writes the count per particle id; FILL: writes the pair records.
+template <bool STRICT, bool FILL>
+__global__ void __launch_bounds__(kBlock)
+    k_pairs(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
+            const double4* __restrict__ spos, const uint32_t* __restrict__ cstart, uint32_t nx,
+            uint32_t ny, uint32_t nz, uint32_t* __restrict__ count,
+            const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
+            uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if(s >= n)
+        return;
+    const uint32_t a   = sids[s];
+    const uint32_t key = skeys[s];
+    const double4  pa  = spos[s];
+    const int      cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+    uint32_t       c  = 0;
+    int64_t        out = FILL ? (int64_t)offset[a] : 0;
+    for(int k = -1; k < 2; ++k)
+    {
+        const int z = cz + k;
+        if(z < 0 || z >= (int)nz)
+            continue;
+        for(int j = -1; j < 2; ++j)
+        {
+            const int y = cy + j;
+            if(y < 0 || y >= (int)ny)
+                continue;
+            const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
+            for(int i = -1; i < 2; ++i)
+            {
+                const int x = cx + i;
+                if(x < 0 || x >= (int)nx)
+                    continue;
+                const uint32_t nc = row + (uint32_t)x;
+                const uint32_t t1 = cstart[nc + 1];
+                for(uint32_t t = cstart[nc]; t < t1; ++t)
+                {
+                    if(t == (uint32_t)s)
+                        continue;
+                    const double4 pb = spos[t];
+                    bool          hit;
+                    if constexpr(STRICT)
+                    {
+                        const dstrict dx = dstrict(pb.x) - dstrict(pa.x);
+                        const dstrict dy = dstrict(pb.y) - dstrict(pa.y);
+                        const dstrict dz = dstrict(pb.z) - dstrict(pa.z);
+                        hit = s_sqrt(dx * dx + dy * dy + dz * dz) - (dstrict(pa.w) + dstrict(pb.w))
+                              < dstrict(0.0);
+                    }
+                    else
+                    {
+                        const double dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
+                        const double r  = pa.w + pb.w;
+                        hit             = dx * dx + dy * dy + dz * dz < r * r;
+                    }
+                    if(hit)
+                    {
+                        if constexpr(FILL)
+                        {
+                            if(out < cap)
+                            {
+                                pair_a[out] = a;
+                                pair_b[out] = sids[t];
+                            }
+                            else
+                                atomicOr(flags, kFlagCapacity);
+                            ++out;
+                        }
+                        else
+                            ++c;
+                    }
+                }
+            }
+        }
+    }
+    if constexpr(!FILL)
+        count[a] = c;
+}
+
+// ---- narrow phase + contact law, one thread per candidate pair ---------------
+template <typename St>
+struct PairOut
+{
+    St*      f[3];
+    St*      t[3];
+    St*      m[3];     // rolling moment (only when some kr != 0)
+    uint8_t* contact;  // 1 when overlap < 0
+    double*  info;     // optional: 7 per pair (point, vector, overlap) in world frame
+    // tangential history (history law): current step out, previous step in
+    St*             xi[3];
+    const uint32_t* prev_off;
+    const uint32_t* prev_b;
+    const St*       prev_xi[3];
+};
+
+template <typename S>
+__global__ void __launch_bounds__(128)
+    k_narrow(int64_t npairs, const uint32_t* __restrict__ pair_a,
+             const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
+             PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
+             unsigned long long* __restrict__ gjk_iters)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= npairs)
+        return;
+    const uint32_t a = pair_a[p], b = pair_b[p];
+    const uint32_t ra = st.rb_id[a], rb = st.rb_id[b];
+    const Body<S>  A = load_body<S>(tb.shape, ra, tb.verts);
+    const Body<S>  B = load_body<S>(tb.shape, rb, tb.verts);
+    const M3<S>    RA = load_rot<S>(st, a), RB = load_rot<S>(st, b);
+    const double   xa[3] = {st.pos[0][a], st.pos[1][a], st.pos[2][a]};
+    const double   xb[3] = {st.pos[0][b], st.pos[1][b], st.pos[2][b]};
+    V3<S>          oA, oB, d;
+    if constexpr(is_mixed<S>())
+    {
+        d  = mk<S>(S(xb[0] - xa[0]), S(xb[1] - xa[1]), S(xb[2] - xa[2]));
+        oA = zero3<S>();
+        oB = d;
+    }
+    else
+    {
+        oA = mk<S>(S(xa[0]), S(xa[1]), S(xa[2]));
+        oB = mk<S>(S(xb[0]), S(xb[1]), S(xb[2]));
+        d  = oB - oA;
+    }
+    int              iters = 0;
+    const Contact<S> ci    = closest_points(A, B, RA, RB, oA, oB, d, &iters);
+    const bool       hit   = ci.overlap < S(0.0);
+    Force<S>         F;
+    F.f = F.t = F.m = zero3<S>();
+    V3<S> xi_new    = zero3<S>();
+    if(hit)
+    {
+        const Law<S> L  = load_law<S>(tb.law, tb.shape[ra].material, tb.shape[rb].material);
+        const S      m1 = S(tb.inertia[ra].mass), m2 = S(tb.inertia[rb].mass);
+        const V3<S>  vA = load3<S>(st.vel, a), vB = load3<S>(st.vel, b);
+        const V3<S>  wA = load3<S>(st.omg, a), wB = load3<S>(st.omg, b);
+        // arm = contact point - A's centre
+        V3<S> arm, ptw;
+        if constexpr(is_mixed<S>())
+        {
+            arm = ci.pt;
+            ptw = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)),
+                        S(xa[2] + to_d(ci.pt.z)));
+        }
+        else
+        {
+            arm = ci.pt - oA;
+            ptw = ci.pt;
+        }
+        if(law_kind == GB_LAW_HOOKE)
+        {
+            // Kinematics::kinematicsAtPoint with the absolute contact point
+            const V3<S> rel = (vA + cross(wA, ptw)) - (vB + cross(wB, ptw));
+            F               = hooke(L, ci, rel, wA - wB, m1, m2, arm);
+        }
+        else
+        {
+            const V3<S> armB = is_mixed<S>() ? ci.pt - d : ci.pt - oB;
+            const V3<S> rel  = (vA + cross(wA, arm)) - (vB + cross(wB, armB));
+            V3<S>       xi_prev = zero3<S>();
+            for(uint32_t k = po.prev_off[a]; k < po.prev_off[a + 1]; ++k)
+                if(po.prev_b[k] == b)
+                {
+                    xi_prev = mk<S>(S(po.prev_xi[0][k]), S(po.prev_xi[1][k]), S(po.prev_xi[2][k]));
+                    break;
+                }
+            F = hooke_history(L, ci, rel, m1, m2, dt, xi_prev, xi_new, arm);
+        }
+    }
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+        const S fk[3] = {F.f.x, F.f.y, F.f.z}, tk[3] = {F.t.x, F.t.y, F.t.z};
+        po.f[k][p] = (store_t<S>)to_d(fk[k]);
+        po.t[k][p] = (store_t<S>)to_d(tk[k]);
+    }
+    if(has_kr)
+    {
+        po.m[0][p] = (store_t<S>)to_d(F.m.x);
+        po.m[1][p] = (store_t<S>)to_d(F.m.y);
+        po.m[2][p] = (store_t<S>)to_d(F.m.z);
+    }
+    if(law_kind != GB_LAW_HOOKE)
+    {
+        po.xi[0][p] = (store_t<S>)to_d(xi_new.x);
+        po.xi[1][p] = (store_t<S>)to_d(xi_new.y);
+        po.xi[2][p] = (store_t<S>)to_d(xi_new.z);
+    }
+    po.contact[p] = hit ? 1 : 0;
+    if(po.info)
+    {
+        double* o = po.info + 7 * p;
+        if constexpr(is_mixed<S>())
+        {
+            o[0] = xa[0] + to_d(ci.pt.x);
+            o[1] = xa[1] + to_d(ci.pt.y);
+            o[2] = xa[2] + to_d(ci.pt.z);
+        }
+        else
+        {
+            o[0] = to_d(ci.pt.x);
+            o[1] = to_d(ci.pt.y);
+            o[2] = to_d(ci.pt.z);
+        }
+        o[3] = to_d(ci.vec.x);
+        o[4] = to_d(ci.vec.y);
+        o[5] = to_d(ci.vec.z);
+        o[6] = to_d(ci.overlap);
+    }
+    if(iters)
+        atomicAdd(gjk_iters, (unsigned long long)iters);
+}
+
+// ---- per-particle kernel -------------------------------------------------------
+// PHASE_DETECT:  torce = sum of the particle's pair forces in enumeration
+//                order, then obstacle contacts in obstacle order
+//                (ComponentManagerCPU.cpp:356-423 then :301-351).
+// PHASE_GRAVITY: torce.force += m g (ComponentManagerCPU.cpp:448-460).
+// PHASE_MOVE:    integrate from the stored torce, then reset it
+//                (ComponentManagerCPU.cpp:465-500).
+// PHASE_STEP:    all three fused, no torce round trip.
+enum Phase
+{
+    PHASE_DETECT  = 1,
+    PHASE_GRAVITY = 2,
+    PHASE_MOVE    = 4,
+    PHASE_STEP    = 7
+};
+
+template <typename S>
+struct StepParams
+{
+    S        dt;      // time step
+    S        h;       // velocity kick of this move (dt; dt/2 on the first Verlet move)
+    V3<S>    g;       // gravity
+    int      integrator;
+    int      law_kind;
+    int      has_kr;
+    int      phases;
+};
+
+template <typename S>
+GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
+                        const double xa[3], const V3<S>& vA, const V3<S>& wA, S m1, int matA,
+                        const StepParams<S>& sp, V3<S>& F, V3<S>& T, int& nwall, int& iters)
+{
+    for(int o = 0; o < tb.n_obs; ++o)
+    {
+        const double*  ot = tb.obs_tr + 12 * o;
+        const Body<S>  O  = load_body<S>(tb.obs_shape, o, tb.verts);
+        V3<S>          oA, oO;
+        if constexpr(is_mixed<S>())
+        {
+            oA = zero3<S>();
+            oO = mk<S>(S(ot[9] - xa[0]), S(ot[10] - xa[1]), S(ot[11] - xa[2]));
+        }
+        else
+        {
+            oA = mk<S>(S(xa[0]), S(xa[1]), S(xa[2]));
+            oO = mk<S>(S(ot[9]), S(ot[10]), S(ot[11]));
+        }
+        M3<S> RO;
+#pragma unroll
+        for(int k = 0; k < 9; ++k)
+            RO.m[k] = S(ot[k]);
+        Contact<S> ci;
+        if(O.type == GB_RECTANGLE)
+            ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
+        else
+            ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+        if(!(ci.overlap < S(0.0)))
+            continue;
+        ++nwall;
+        const Law<S> L  = load_law<S>(tb.law, matA, tb.obs_shape[o].material);
+        const S      m2 = S(tb.obs_mass[o]);
+        V3<S>        arm, ptw;
+        if constexpr(is_mixed<S>())
+        {
+            arm = ci.pt;
+            ptw = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)), S(xa[2] + to_d(ci.pt.z)));
+        }
+        else
+        {
+            arm = ci.pt - oA;
+            ptw = ci.pt;
+        }
+        Force<S> f;
+        if(sp.law_kind == GB_LAW_HOOKE)
+        {
+            // obstacles have zero velocity (ComponentManagerCPU.cpp:330-340)
+            const V3<S> zero = zero3<S>();
+            const V3<S> rel  = (vA + cross(wA, ptw)) - (zero + cross(zero, ptw));
+            f                = hooke(L, ci, rel, wA - zero, m1, m2, arm);
+        }
+        else
+        {
+            V3<S> xi;
+            f = hooke_history(L, ci, vA + cross(wA, arm), m1, m2, sp.dt, zero3<S>(), xi, arm);
+        }
+        F = F + f.f;
+        T = T + f.t;
+        if(sp.has_kr)
+            T = T + f.m;
+    }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+    k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
+                PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
+                unsigned long long* __restrict__ counters, unsigned long long* __restrict__ gjk_iters)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const uint32_t            r   = st.rb_id[i];
+    const RBInertia<store_t<S>>* in = tb.inertia + r;
+    const S                   m   = S(in->mass);
+    V3<S>                     F, T;
+    V3<S>                     v = load3<S>(st.vel, i), w = load3<S>(st.omg, i);
+    int                       nc = 0, nwall = 0, iters = 0;
+    if(sp.phases & PHASE_DETECT)
+    {
+        F = zero3<S>();
+        T = zero3<S>();
+        for(uint32_t p = off[i]; p < off[i + 1]; ++p)
+        {
+            if(!po.contact[p])
+                continue;
+            ++nc;
+            F = F + mk<S>(S(po.f[0][p]), S(po.f[1][p]), S(po.f[2][p]));
+            T = T + mk<S>(S(po.t[0][p]), S(po.t[1][p]), S(po.t[2][p]));
+            if(sp.has_kr)
+                T = T + mk<S>(S(po.m[0][p]), S(po.m[1][p]), S(po.m[2][p]));
+        }
+        if(tb.n_obs)
+        {
+            const Body<S> A     = load_body<S>(tb.shape, r, tb.verts);
+            const double  xa[3] = {st.pos[0][i], st.pos[1][i], st.pos[2][i]};
+            wall_contacts(tb, A, load_rot<S>(st, i), xa, v, w, m, tb.shape[r].material, sp, F, T,
+                          nwall, iters);
+        }
+        if(contacts_out)
+            contacts_out[i] = nc;
+    }
+    else
+    {
+        F = load3<S>(st.frc, i);
+        T = load3<S>(st.trq, i);
+    }
+    if(sp.phases & PHASE_GRAVITY)
+        F = F + m * sp.g; // Torce::addForce(mass * g)
+    if(sp.phases & PHASE_MOVE)
+    {
+        // RigidBody::computeMomentum + FirstOrderExplicit::Move
+        // (RigidBody.cpp:267-307, FirstOrderExplicit.cpp:46-60) or the Verlet kick-drift
+        S I[6], I1[6];
+#pragma unroll
+        for(int k = 0; k < 6; ++k)
+        {
+            I[k]  = S(in->I[k]);
+            I1[k] = S(in->I1[k]);
+        }
+        Quat<S> q;
+        M3<S>   R;
+        if constexpr(is_mixed<S>())
+        {
+            q.w = S(st.rot[0][i]);
+            q.v = mk<S>(S(st.rot[1][i]), S(st.rot[2][i]), S(st.rot[3][i]));
+        }
+        else
+        {
+            R = load_rot<S>(st, i);
+            q = quat_from_basis(R);
+        }
+        const V3<S> acc   = mk<S>(F.x / m, F.y / m, F.z / m);
+        const V3<S> alpha = angular_acceleration(I, I1, w, T, q);
+        V3<S>       trans;
+        Quat<S>     dq;
+        if(sp.integrator == GB_FIRST_ORDER_EXPLICIT)
+        {
+            trans = sp.dt * v;
+            v     = v + sp.dt * acc;
+            dq    = quaternion_change(w, sp.dt);
+            w     = w + sp.dt * alpha;
+        }
+        else
+        {
+            v     = v + sp.h * acc;
+            w     = w + sp.h * alpha;
+            trans = sp.dt * v;
+            dq    = quaternion_change(w, sp.dt);
+        }
+        // Transform3::updateTransform (Transform3.cpp:324-329)
+#pragma unroll
+        for(int k = 0; k < 3; ++k)
+        {
+            const S tk[3] = {trans.x, trans.y, trans.z};
+            if constexpr(is_mixed<S>())
+                st.pos[k][i] = st.pos[k][i] + (double)tk[k];
+            else
+                st.pos[k][i] = to_d(S(st.pos[k][i]) + tk[k]);
+        }
+        if constexpr(is_mixed<S>())
+        {
+            Quat<S> qn = qmul(dq, q);
+            const S nq = s_sqrt(qn.w * qn.w + norm2(qn.v));
+            st.rot[0][i] = qn.w / nq;
+            st.rot[1][i] = qn.v.x / nq;
+            st.rot[2][i] = qn.v.y / nq;
+            st.rot[3][i] = qn.v.z / nq;
+        }
+        else
+        {
+            compose_left_by_rotation(R, dq);
+#pragma unroll
+            for(int k = 0; k < 9; ++k)
+                st.rot[k][i] = to_d(R.m[k]);
+        }
+        st.vel[0][i] = (store_t<S>)to_d(v.x);
+        st.vel[1][i] = (store_t<S>)to_d(v.y);
+        st.vel[2][i] = (store_t<S>)to_d(v.z);
+        st.omg[0][i] = (store_t<S>)to_d(w.x);
+        st.omg[1][i] = (store_t<S>)to_d(w.y);
+        st.omg[2][i] = (store_t<S>)to_d(w.z);
+        if(sp.phases != PHASE_STEP)
+        {
+            // Torce::reset
+#pragma unroll
+            for(int k = 0; k < 3; ++k)
+            {
+                st.frc[k][i] = store_t<S>(0);
+                st.trq[k][i] = store_t<S>(0);
+            }
+        }
+    }
+    else
+    {
+        st.frc[0][i] = (store_t<S>)to_d(F.x);
+        st.frc[1][i] = (store_t<S>)to_d(F.y);
+        st.frc[2][i] = (store_t<S>)to_d(F.z);
+        st.trq[0][i] = (store_t<S>)to_d(T.x);
+        st.trq[1][i] = (store_t<S>)to_d(T.y);
+        st.trq[2][i] = (store_t<S>)to_d(T.z);
+    }
+    if((sp.phases & PHASE_DETECT) && (nwall || iters))
+    {
+        if(nwall)
+            atomicAdd(&counters[0], (unsigned long long)nwall);
+        if(iters)
+            atomicAdd(gjk_iters, (unsigned long long)iters);
+    }
+}
+
+} // namespace gb

@@ -151,20 +151,39 @@ def superquadric_semi_axes(r_eq, ba, ca, n1, n2):
 
 
 # ---------------------------------------------------------------------------
-def config0(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000):
+def config0(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000,
+            shape="superquadric", jitter=0.15e-3, tilt=None):
     """2,000 identical superquadrics a=b=c=1 mm, n1=n2=4, on a 2.4 mm jittered
     lattice (+-0.15 mm) with random orientations, in a closed box.  The box
     is raised from 60 to 80 mm because 2,000 sites at 2.4 mm pitch do not fit
-    in 20x20x60 mm; crust = 5% of the semi-axis."""
+    in 20x20x60 mm; crust = 5% of the semi-axis.  `shape` swaps in 1 mm
+    boxes or spheres on the same lattice (parity tests without pow); `tilt`
+    (radians) replaces the uniform random orientations by small rotations."""
     rng = np.random.default_rng(seed)
     rbs = np.zeros(1, RB_DTYPE)
-    rbs[0]["type"] = abi.GB_SUPERQUADRIC
-    rbs[0]["p"] = [1e-3, 1e-3, 1e-3, 4.0, 4.0]
+    if shape == "superquadric":
+        rbs[0]["type"] = abi.GB_SUPERQUADRIC
+        rbs[0]["p"] = [1e-3, 1e-3, 1e-3, 4.0, 4.0]
+    elif shape == "box":
+        rbs[0]["type"] = abi.GB_BOX
+        rbs[0]["p"][:3] = [0.8e-3, 0.8e-3, 0.8e-3]
+    elif shape == "sphere":
+        rbs[0]["type"] = abi.GB_SPHERE
+        rbs[0]["p"][0] = 1.1e-3
+    else:
+        raise ValueError(shape)
     rbs[0]["crust"] = 5e-5
     rbs[0]["density"] = 2500.0
-    pos, _ = lattice(box, pitch, 1.6e-3, n, rng, 0.15e-3)
+    pos, _ = lattice(box, pitch, 1.6e-3, n, rng, jitter)
     tr = np.zeros((n, 12))
-    tr[:, :9] = random_rotations(rng, n)
+    if tilt is None:
+        tr[:, :9] = random_rotations(rng, n)
+    else:
+        axis = rng.normal(size=(n, 3))
+        axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+        ang = rng.uniform(0.0, tilt, n)
+        q = np.concatenate([np.cos(ang / 2)[:, None], np.sin(ang / 2)[:, None] * axis], 1)
+        tr[:, :9] = quat_to_matrix(q)
     tr[:, 9:] = pos
     walls, wtr = box_walls(box)
     cfg = dict(n_particles=n, n_rigid_bodies=1, n_obstacles=6, n_materials=2,

@@ -63,8 +63,10 @@ extern "C" {
 #define GB_MAX_POLY_VERTICES 64
 
 /* ---- run modes -------------------------------------------------------------- */
-#define GB_FP64 0  /* every kernel in double precision                         */
-#define GB_MIXED 1 /* FP32 bulk; FP64 positions, FP64 GJK polish near contact  */
+#define GB_FP64 0        /* every kernel in double precision, FMA contraction on  */
+#define GB_MIXED 1       /* FP32 bulk; FP64 positions, FP64 GJK polish near contact */
+#define GB_FP64_STRICT 2 /* FP64 in the reference's IEEE operation order (no FMA
+                            contraction): the parity mode                          */
 
 #define GB_LAW_HOOKE 0         /* HookeContactForceModel (parity)          */
 #define GB_LAW_HOOKE_HISTORY 1 /* spring-dashpot + Coulomb-capped tangential
@@ -132,7 +134,12 @@ typedef struct gb_config {
     int32_t gjk_variant; /* GB_GJK_*          */
     int32_t device;      /* CUDA device ordinal */
     int64_t pair_capacity; /* initial candidate-pair capacity, 0 = automatic */
+    int32_t flags;         /* GB_FLAG_* */
+    int32_t reserved;
 } gb_config;
+
+/* gb_config.flags */
+#define GB_FLAG_RECORD_CONTACT_INFO 1 /* keep per-pair contact info for dumps */
 
 /* Counters of the last completed step (or of the last detect call). */
 typedef struct gb_stats {
