@@ -1,0 +1,409 @@
+"""Throughput of the DEM time step on B200: particle-steps/s.
+
+Workload: the mixed-precision configuration -- 1,000,000 polydisperse
+superquadrics (equivalent radius lognormal, median 1 mm, sigma 0.25, clipped
+to 0.5-2 mm; b/a, c/a ~ U(0.5, 2); n1, n2 ~ U(2, 10)) on a jittered lattice in a
+closed 0.3 x 0.3 x 1.2 m box, dt = 1e-6 s, Hooke law kn=1e4 N/m, en=0.7,
+mu=0.5, gravity -z.  One step = one GrainsCPU::simulate loop iteration
+(collide + force, gravity, move) over all particles.
+
+  python bench.py [--gpus N --steps K --warmup W]          the engine (mixed)
+  python bench.py --impl reference [...]                   the reference CPU path
+
+Multi-GPU runs are independent replicas (one seeded packing per rank, no
+data-path collective); the device time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from grains3dgpu_b200 import abi, scenes  # noqa: E402
+
+HBM_FALLBACK_GBS = 6650.0
+METRIC = "particle-steps/s"
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+# Algorithmic bytes per phase for one step (unique bytes a phase must move;
+# N particles, C cells, P candidate pairs; S = bytes of a state scalar, 4 in
+# the mixed mode, 8 in FP64; positions are always FP64).
+def phase_bytes(n, c, p, s, quat):
+    rot = (4 if quat else 9) * s
+    shape = 16 + 18 * s + 8          # RBShape record
+    inertia = 14 * s                 # RBInertia record
+    return {
+        "hash": n * (24 + 8),
+        "sort": n * 16,
+        "cell_start": n * (4 + 4 + 24 + 4 + 8 + 32) + 4 * (c + 1),
+        "pair_count": n * (4 + 4 + 32 + 4 + 8) + 4 * (c + 1),
+        "pair_fill": n * (4 + 4 + 32 + 4) + 4 * (c + 1) + 8 * p,
+        "narrow": n * (24 + rot + 4 + shape) + p * (8 + 6 * s + 1),
+        "particle": n * (2 * (24 + rot + 6 * s) + 4 + inertia + 8) + p * (6 * s + 1),
+    }
+
+
+def clocks_sampler(out_path):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        f = open(out_path, "w")
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                 "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL), f
+    except Exception:
+        return None, None
+
+
+def clocks_summary(path, device):
+    try:
+        rows = [r.split(",") for r in open(path).read().strip().splitlines()]
+        rows = [[x.strip() for x in r] for r in rows if len(r) >= 9 and r[0].strip() == str(device)]
+    except Exception:
+        rows = []
+    if not rows:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+    mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+    reasons = set()
+    for r in rows:
+        for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                            "sw_power_cap"], r[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(name)
+    return {"sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons)}
+
+
+def make_scene(args, rank):
+    return scenes.config2(seed=2 + 1000 * rank, n=args.n)
+
+
+# ---------------------------------------------------------------------------
+def run_engine(args, scene, precision, steps, warmup, torch, rank, world, timing=True):
+    from grains3dgpu_b200 import engine
+    lib = engine.load()
+    flags = abi.GB_FLAG_PHASE_TIMING if timing else 0
+    sysm = scenes.System(lib, scene, precision=precision, device=torch.cuda.current_device(),
+                         flags=flags)
+    stream = torch.cuda.current_stream()
+    assert lib.set_stream(sysm.ctx, abi.C.c_void_p(stream.cuda_stream)) == 0
+    for _ in range(warmup):
+        sysm.step(1)
+    ms = np.zeros(abi.GB_N_PHASES)
+    lib.get_phase_times(sysm.ctx, abi.dptr(ms), None, 1)  # reset accumulators
+    launches0 = sysm.stats().kernel_launches
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        sysm.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    st = sysm.stats()
+    launches = st.kernel_launches - launches0
+    nsteps = abi.C.c_int64(0)
+    if timing:
+        lib.get_phase_times(sysm.ctx, abi.dptr(ms), abi.C.byref(nsteps), 0)
+    return sysm, elapsed, launches, ms, nsteps.value, st
+
+
+def e2e_engine(sysm, steps, torch):
+    """Same step through the public C ABI with host buffers: every step copies
+    the state in from pinned host memory and reads it back."""
+    n = sysm.n
+    tr = torch.empty((n, 12), dtype=torch.float64, pin_memory=True).numpy()
+    kin = torch.empty((n, 6), dtype=torch.float64, pin_memory=True).numpy()
+    tr[:] = sysm.transforms()
+    kin[:] = sysm.velocities()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        sysm.set_transforms(tr)
+        sysm.set_velocities(kin)
+        sysm.step(1)
+        tr[:] = sysm.transforms()
+        kin[:] = sysm.velocities()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    return e0.elapsed_time(e1) / 1e3, wall, n * 18 * 8, n * 18 * 8
+
+
+def force_error(scene, torch):
+    """Single-step force error of the mixed mode against the FP64 mode from
+    one identical state: max |F_mixed - F_fp64| over particles divided by
+    max |F_fp64|, and the same for torques."""
+    from grains3dgpu_b200 import engine
+    lib = engine.load()
+    out = {}
+    for prec in (abi.GB_MIXED, abi.GB_FP64):
+        s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device())
+        s.detect()
+        out[prec] = (s.torces(), s.stats().contacts)
+        s.close()
+    a, b = out[abi.GB_MIXED][0], out[abi.GB_FP64][0]
+    ef = np.abs(a[:, :3] - b[:, :3]).max() / max(np.abs(b[:, :3]).max(), 1e-300)
+    et = np.abs(a[:, 3:] - b[:, 3:]).max() / max(np.abs(b[:, 3:]).max(), 1e-300)
+    return {"force_rel_err": float(ef), "torque_rel_err": float(et),
+            "contacts": int(out[abi.GB_FP64][1])}
+
+
+# ---------------------------------------------------------------------------
+def full_cell_size(scene):
+    """Linked-cell size of the whole workload (2 x the largest circumscribed
+    radius), computed by the FP64 oracle's rigid-body set-up."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    s = scenes.System(pyoracle.load_oracle(), scene)
+    cell = s.stats().cell_size
+    s.close()
+    return cell
+
+
+def sample_blocks(scene, m, count):
+    """`count` disjoint blocks of about m particles each: s x s lattice columns
+    of the bottom h layers (the packing fills the lattice layer by layer), so
+    every sampled particle sees the workload's local density."""
+    cx, cy, _ = scene.lattice_counts
+    k = np.arange(scene.n)
+    ix, iy, iz = k % cx, (k // cx) % cy, k // (cx * cy)
+    per_row = int(np.ceil(np.sqrt(count)))
+    side = max(2, min(cx, cy) // per_row)                 # columns of side x side sites
+    layers = max(1, int(np.ceil(m / (side * side))))      # ... and this many layers
+    out = []
+    for b in range(count):
+        bx, by = b % per_row, b // per_row
+        sel = ((ix // side) == bx) & ((iy // side) == by) & (iz < layers)
+        out.append(np.nonzero(sel)[0])
+    return out
+
+
+def sample_scene(scene, idx, cell):
+    """The particles idx as a system of their own, with the workload's cell size."""
+    sub = scene.subset(idx)
+    probe = scenes.System(_cpu_lib()[0], sub)
+    factor = cell / probe.stats().cell_size
+    probe.close()
+    sub.config["cell_size_factor"] = factor
+    return sub
+
+
+def _cpu_lib():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if pyoracle.reference_available():
+        return pyoracle.load_reference(), "reference"
+    return pyoracle.load_oracle(), "port"
+
+
+def time_reference(scene, m, target_s, max_steps=50, cell=None):
+    lib, kind = _cpu_lib()
+    cell = cell or full_cell_size(scene)
+    sub = sample_scene(scene, sample_blocks(scene, m, 1)[0], cell)
+    m = sub.n
+    s = scenes.System(lib, sub)
+    t0 = time.perf_counter()
+    s.step(1)
+    t1 = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, target_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    s.step(steps)
+    dt = time.perf_counter() - t0
+    s.close()
+    return {"value": m * steps / dt, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"{m} particles (a lattice block of the workload, full-workload cell "
+                      f"size) x {steps} steps, {dt:.1f} s, single thread (the reference loop "
+                      f"is serial)"}
+
+
+def reference_arm(args):
+    """--impl reference: the reference's own CPU path on every host thread,
+    each thread stepping its own disjoint slab of the workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    lib, kind = _cpu_lib()
+    try:
+        nthreads = len(os.sched_getaffinity(0))
+    except Exception:
+        nthreads = os.cpu_count() or 1
+    scene = scenes.config2(seed=2, n=args.n)
+    cell = full_cell_size(scene)
+    blocks = [b for b in sample_blocks(scene, args.ref_sample, nthreads) if b.size]
+    nthreads = len(blocks)
+    systems = [scenes.System(lib, sample_scene(scene, b, cell)) for b in blocks]
+    m = int(np.mean([b.size for b in blocks]))
+    total = int(sum(b.size for b in blocks))
+
+    def run(k):
+        ths = [threading.Thread(target=s.step, args=(k,)) for s in systems]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+
+    run(args.warmup)
+    t0 = time.perf_counter()
+    run(args.steps)
+    dt = time.perf_counter() - t0
+    value = total * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "config2 sample: polydisperse superquadrics, 0.3x0.3x1.2 m box",
+                   "sample_particles_per_thread": m, "threads": nthreads},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": nthreads, "kind": kind,
+                         "sample": f"{nthreads} threads, each stepping its own lattice block of "
+                                   f"~{m} particles of the workload (full-workload cell size), "
+                                   f"{args.steps} steps"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--fp64-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-sample", type=int, default=20_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    scene = make_scene(args, rank)
+    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
+    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    sampler, fh = clocks_sampler(clk_path)
+    sysm, elapsed, launches, ms, nsteps, st = run_engine(
+        args, scene, abi.GB_MIXED, args.steps, args.warmup, torch, rank, world)
+    if sampler:
+        sampler.terminate()
+        fh.close()
+    clocks = clocks_summary(clk_path, torch.cuda.current_device())
+    t = torch.tensor([elapsed], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    t_max = float(t.item())
+    value = world * scene.n * args.steps / t_max
+
+    # per-phase roofline (phase device time from CUDA events on the launch stream)
+    hbm, hbm_kind = measured_hbm()
+    per_step = ms / max(nsteps, 1)
+    pb = phase_bytes(scene.n, st.n_cells, st.candidate_pairs, 4, True)
+    phases = {}
+    for k, name in enumerate(abi.PHASES):
+        sec = per_step[k] / 1e3
+        gbs = pb[name] / sec / 1e9 if sec > 0 else 0.0
+        phases[name] = {"ms": per_step[k], "share": per_step[k] / max(per_step.sum(), 1e-12),
+                        "algorithmic_bytes": pb[name], "achieved_gbs": gbs,
+                        "frac_of_measured_hbm": gbs / hbm}
+    top = max(phases, key=lambda k: phases[k]["ms"])
+    roofline = {"kernel": top, "bound": "hbm", "achieved": phases[top]["achieved_gbs"],
+                "peak": hbm, "unit": "GB/s", "frac": phases[top]["frac_of_measured_hbm"],
+                "traffic": TRAFFIC_PER_STEP.get(top), "peak_kind": hbm_kind}
+
+    e2e_dev, e2e_wall, h2d, d2h = e2e_engine(sysm, args.e2e_steps, torch)
+    e2e_value = world * scene.n * args.e2e_steps / max(e2e_dev, e2e_wall)
+    sysm.close()
+
+    # the all-FP64 run of the same kernels on the same workload
+    _, el64, _, ms64, n64, _ = run_engine(args, scene, abi.GB_FP64, args.fp64_steps, 3, torch,
+                                          rank, world)
+    t64 = torch.tensor([el64], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t64, op=torch.distributed.ReduceOp.MAX)
+    value64 = world * scene.n * args.fp64_steps / float(t64.item())
+    ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = time_reference(scene, args.ref_sample, args.cpu_seconds, cell=st.cell_size)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (f64 positions, f64 GJK polish near contact)",
+            "data": "synthetic (seeded jittered-lattice packing)",
+            "config": {"workload": "config2: 1,000,000 polydisperse superquadrics in a "
+                                   "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision"
+                       if scene.n == 1_000_000 else f"config2 with {scene.n} particles",
+                       "n_particles": scene.n, "precision": "mixed",
+                       "n_cells": st.n_cells, "candidate_pairs_last_step": st.candidate_pairs,
+                       "l2": "per-step working set > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline,
+            "phases_ms": {k: round(v["ms"], 4) for k, v in phases.items()},
+            "phases_hbm_frac": {k: round(v["frac_of_measured_hbm"], 4) for k, v in phases.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+                    "ms_per_step": max(e2e_dev, e2e_wall) / args.e2e_steps * 1e3},
+            "fp64": {"value": value64, "ms_per_step": float(t64.item()) / args.fp64_steps * 1e3,
+                     "steps": args.fp64_steps},
+            "mixed_over_fp64": value / value64,
+            "mixed_vs_fp64_single_step": ferr,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+# DRAM bytes per step of the dominant kernels from one ncu capture, scaled to
+# the full workload (None until captured).
+TRAFFIC_PER_STEP = {}
+
+if __name__ == "__main__":
+    sys.exit(main())

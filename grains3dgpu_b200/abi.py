@@ -25,6 +25,9 @@ GB_MAX_POLY_VERTICES = 64
 
 GB_FP64, GB_MIXED, GB_FP64_STRICT = 0, 1, 2
 GB_FLAG_RECORD_CONTACT_INFO = 1
+GB_FLAG_PHASE_TIMING = 2
+PHASES = ["hash", "sort", "cell_start", "pair_count", "pair_fill", "narrow", "particle"]
+GB_N_PHASES = len(PHASES)
 GB_LAW_HOOKE, GB_LAW_HOOKE_HISTORY = 0, 1
 GB_FIRST_ORDER_EXPLICIT, GB_VELOCITY_VERLET = 0, 1
 GB_GJK_JH, GB_GJK_SV, GB_GJK_NESTEROV = 0, 1, 2
@@ -79,7 +82,8 @@ class Stats(C.Structure):
                 ("gjk_calls", C.c_int64), ("gjk_iterations", C.c_int64),
                 ("status_flags", C.c_int32), ("n_cells", C.c_int32),
                 ("cells_per_dir", C.c_int32 * 3), ("key_bits", C.c_int32),
-                ("cell_size", C.c_double), ("grid_max", C.c_double * 3)]
+                ("cell_size", C.c_double), ("grid_max", C.c_double * 3),
+                ("kernel_launches", C.c_int64)]
 
 
 class Contact(C.Structure):
@@ -143,6 +147,8 @@ ENGINE_API = {
     "convex_hull_centroid": (C.c_int, [_D, C.c_int32, _D, _D]),
     "device_pointer": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_void_p)]),
     "synchronize": (C.c_int, [_P]),
+    "set_stream": (C.c_int, [_P, _P]),
+    "get_phase_times": (C.c_int, [_P, _D, _I64, C.c_int32]),
 }
 
 

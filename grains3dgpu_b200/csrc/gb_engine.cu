@@ -9,6 +9,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "gb_io.cuh"
 #include "gb_step.cuh"
 
 using namespace gb;
@@ -96,6 +97,11 @@ struct gb_ctx
     double*  d_obs_tr = nullptr;
     double*  d_obs_mass = nullptr;
     double*  d_rcirc64 = nullptr;
+    // FP64 shape tables: aliases of the above in the FP64 modes, separate
+    // copies in the mixed mode (read by its FP64 polish)
+    void* d_shape64 = nullptr;
+    void* d_verts64 = nullptr;
+    void* d_obs_shape64 = nullptr;
 
     // state
     double*   d_pos = nullptr; // 3n
@@ -138,10 +144,46 @@ struct gb_ctx
     bool                verlet_started = false;
     bool                links_valid = false, detect_valid = false;
     gb_stats            last{};
+
+    cudaStream_t own_stream = nullptr; // the context's stream (gb_set_stream may replace it)
+    // phase timing: two alternating event sets; a set is read once the next
+    // step's host synchronisation has passed it
+    bool        timing = false, in_step = false;
+    cudaEvent_t ev[2][GB_N_PHASES + 1];
+    int         ev_set = 0, ev_pending = -1;
+    double      phase_ms[GB_N_PHASES] = {0};
+    int64_t     phase_steps = 0;
+    int64_t     launches = 0;
+    // staging buffer for the host layouts (12 doubles per particle)
+    double* d_stage = nullptr;
 };
 
 namespace
 {
+
+// event `idx` of the current step's set (0 = step start, k+1 = end of phase k)
+void mark(gb_ctx* c, int idx)
+{
+    if(c->timing && c->in_step)
+        cudaEventRecord(c->ev[c->ev_set][idx], c->stream);
+}
+
+// adds the completed step's phase times (call only after a host sync that
+// follows that step's last event)
+void accumulate_pending(gb_ctx* c)
+{
+    if(!c->timing || c->ev_pending < 0)
+        return;
+    for(int k = 0; k < GB_N_PHASES; ++k)
+    {
+        float ms = 0.f;
+        if(cudaEventElapsedTime(&ms, c->ev[c->ev_pending][k], c->ev[c->ev_pending][k + 1])
+           == cudaSuccess)
+            c->phase_ms[k] += ms;
+    }
+    c->phase_steps++;
+    c->ev_pending = -1;
+}
 
 size_t store_size(int prec)
 {
@@ -182,9 +224,12 @@ Tables<S> tables_of(gb_ctx* c)
     t.verts     = (const Vert<St>*)c->d_verts;
     t.law       = (const Law<St>*)c->d_law;
     t.obs_shape = (const RBShape<St>*)c->d_obs_shape;
-    t.obs_tr    = c->d_obs_tr;
-    t.obs_mass  = c->d_obs_mass;
-    t.n_obs     = c->nob;
+    t.obs_tr      = c->d_obs_tr;
+    t.obs_mass    = c->d_obs_mass;
+    t.n_obs       = c->nob;
+    t.shape64     = (const RBShape<double>*)c->d_shape64;
+    t.verts64     = (const Vert<double>*)c->d_verts64;
+    t.obs_shape64 = (const RBShape<double>*)c->d_obs_shape64;
     return t;
 }
 
@@ -306,66 +351,11 @@ int upload_obstacles(gb_ctx* c)
     return GB_OK;
 }
 
-// Quaternion::setQuaternion(Matrix3) on the host, for the mixed mode's
-// quaternion state (Quaternion.cpp:125-169).
-void basis_to_quat(const double* b, double q[4])
+int ensure_stage(gb_ctx* c)
 {
-    enum { XX, XY, XZ, YX, YY, YZ, ZX, ZY, ZZ };
-    double den;
-    if(b[YY] > -b[ZZ] && b[XX] > -b[YY] && b[XX] > -b[ZZ])
-    {
-        den  = std::pow(1.0 + b[XX] + b[YY] + b[ZZ], 0.5);
-        q[0] = 0.5 * den;
-        q[1] = 0.5 * (b[ZY] - b[YZ]) / den;
-        q[2] = 0.5 * (b[XZ] - b[ZX]) / den;
-        q[3] = 0.5 * (b[YX] - b[XY]) / den;
-    }
-    else if(b[YY] < -b[ZZ] && b[XX] > b[YY] && b[XX] > b[ZZ])
-    {
-        den  = std::pow(1.0 + b[XX] - b[YY] - b[ZZ], 0.5);
-        q[0] = 0.5 * (b[ZY] - b[YZ]) / den;
-        q[1] = 0.5 * den;
-        q[2] = 0.5 * (b[XY] + b[YX]) / den;
-        q[3] = 0.5 * (b[ZX] + b[XZ]) / den;
-    }
-    else if(b[YY] > b[ZZ] && b[XX] < b[YY] && b[XX] < -b[ZZ])
-    {
-        den  = std::pow(1.0 - b[XX] + b[YY] - b[ZZ], 0.5);
-        q[0] = 0.5 * (b[XZ] - b[ZX]) / den;
-        q[1] = 0.5 * (b[XY] + b[YX]) / den;
-        q[2] = 0.5 * den;
-        q[3] = 0.5 * (b[YZ] + b[ZY]) / den;
-    }
-    else if(b[YY] < b[ZZ] && b[XX] < -b[YY] && b[XX] < b[ZZ])
-    {
-        den  = std::pow(1.0 - b[XX] - b[YY] + b[ZZ], 0.5);
-        q[0] = 0.5 * (b[YX] - b[XY]) / den;
-        q[1] = 0.5 * (b[ZX] + b[XZ]) / den;
-        q[2] = 0.5 * (b[YZ] + b[ZY]) / den;
-        q[3] = 0.5 * den;
-    }
-    else
-    {
-        q[0] = 1.0;
-        q[1] = q[2] = q[3] = 0.0;
-    }
-    const double nq = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-    for(int k = 0; k < 4; ++k)
-        q[k] /= nq;
-}
-
-void quat_to_basis(const double q[4], double* m)
-{
-    const double w = q[0], x = q[1], y = q[2], z = q[3];
-    m[0] = 1 - 2 * (y * y + z * z);
-    m[1] = 2 * (x * y - w * z);
-    m[2] = 2 * (x * z + w * y);
-    m[3] = 2 * (x * y + w * z);
-    m[4] = 1 - 2 * (x * x + z * z);
-    m[5] = 2 * (y * z - w * x);
-    m[6] = 2 * (x * z - w * y);
-    m[7] = 2 * (y * z + w * x);
-    m[8] = 1 - 2 * (x * x + y * y);
+    if(!c->d_stage)
+        GB_TRY(dalloc(&c->d_stage, 12 * (size_t)std::max(c->n, 1)));
+    return GB_OK;
 }
 
 int alloc_state(gb_ctx* c)
@@ -461,6 +451,7 @@ int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* 
     k_scan_reduce<<<nb, kBlock, 0, c->stream>>>(in, n, c->d_part);
     k_scan_partials<<<1, 1024, 0, c->stream>>>(c->d_part, nb, d_total);
     k_scan_apply<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_part);
+    c->launches += 3;
     GB_CK(cudaGetLastError());
     return GB_OK;
 }
@@ -472,11 +463,14 @@ int broad_phase(gb_ctx* c)
     const int n = c->n;
     const int nb = std::max(1, blocks(n, kBlock));
     cudaStream_t s = c->stream;
+    mark(c, 0);
     k_hash<<<nb, kBlock, 0, s>>>(n, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
                                  c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2], c->cell,
                                  c->dims[0], c->dims[1], c->dims[2], c->d_hash, c->d_iota,
                                  c->d_flags);
+    c->launches += 1;
     GB_CK(cudaGetLastError());
+    mark(c, 1);
     const uint32_t* src_k = c->d_hash;
     const uint32_t* src_i = c->d_iota;
     const int       passes = c->key_bits == 0 ? 0 : (c->key_bits + 7) / 8;
@@ -499,6 +493,7 @@ int broad_phase(gb_ctx* c)
         GB_TRY(scan_u32(c, c->d_hist, c->d_hist, (int64_t)hn, nullptr));
         k_radix_scatter<<<ntile, kBlock, 0, s>>>(src_k, src_i, c->d_k[dst], c->d_i[dst], n, shift,
                                                  mask, c->d_hist);
+        c->launches += 2;
         GB_CK(cudaGetLastError());
         src_k = c->d_k[dst];
         src_i = c->d_i[dst];
@@ -513,12 +508,15 @@ int broad_phase(gb_ctx* c)
     }
     c->d_skeys = const_cast<uint32_t*>(src_k);
     c->d_sids  = const_cast<uint32_t*>(src_i);
+    mark(c, 2);
     k_cell_start<<<blocks((int64_t)c->ncells + 1, kCellsPerBlock), kBlock, 0, s>>>(
         c->d_skeys, (uint32_t)n, c->ncells, c->d_cstart);
     k_gather_sorted<<<nb, kBlock, 0, s>>>(n, c->d_sids, c->d_pos, c->d_pos + n,
                                           c->d_pos + 2 * (size_t)n, c->d_rb_id, c->d_rcirc64,
                                           c->d_spos);
+    c->launches += 2;
     GB_CK(cudaGetLastError());
+    mark(c, 3);
     c->links_valid = true;
     return GB_OK;
 }
@@ -543,10 +541,13 @@ int build_pairs(gb_ctx* c)
                                                      c->d_cstart, c->dims[0], c->dims[1],
                                                      c->dims[2], c->d_count, nullptr, nullptr,
                                                      nullptr, 0, c->d_flags);
+    c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
+    mark(c, 4);
     GB_CK(cudaMemcpyAsync(c->h_pinned, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     GB_CK(cudaStreamSynchronize(s));
+    accumulate_pending(c); // the previous step finished before this sync
     const int64_t total = c->h_pinned[0];
     GB_TRY(ensure_pairs(c, total));
     if(strict)
@@ -558,7 +559,9 @@ int build_pairs(gb_ctx* c)
                                                     c->d_cstart, c->dims[0], c->dims[1],
                                                     c->dims[2], nullptr, off, c->d_pa,
                                                     c->d_pb[c->cur], c->cap, c->d_flags);
+    c->launches += 1;
     GB_CK(cudaGetLastError());
+    mark(c, 5);
     c->npairs = total;
     return GB_OK;
 }
@@ -591,6 +594,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
 {
     using St = store_t<S>;
     cudaStream_t s = c->stream;
+    c->in_step     = true;
     GB_TRY(broad_phase(c));
     GB_TRY(build_pairs(c));
     PairOut<St> po = pair_out<S>(c);
@@ -607,8 +611,10 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
         k_narrow<S><<<blocks(c->npairs, 128), 128, 0, s>>>(
             c->npairs, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law, c->has_kr ? 1 : 0,
             S(c->cfg.dt), c->d_counters + 1);
+        c->launches += 1;
         GB_CK(cudaGetLastError());
     }
+    mark(c, 6);
     StepParams<S> sp;
     sp.dt         = S(c->cfg.dt);
     sp.h          = S(c->cfg.integrator == GB_VELOCITY_VERLET && !c->verlet_started
@@ -621,7 +627,15 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     sp.phases     = phases;
     k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, s>>>(
         c->n, st, tb, c->d_off[c->cur], po, sp, c->d_contacts, c->d_counters, c->d_counters + 1);
+    c->launches += 1;
     GB_CK(cudaGetLastError());
+    mark(c, 7);
+    if(c->timing)
+    {
+        c->ev_pending = c->ev_set;
+        c->ev_set ^= 1;
+    }
+    c->in_step = false;
     if(phases & PHASE_MOVE)
     {
         c->verlet_started = true;
@@ -659,6 +673,7 @@ int run_particles(gb_ctx* c, int phases)
     k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, c->stream>>>(
         c->n, state_of<St>(c), tables_of<S>(c), c->d_off[c->cur], po, sp, nullptr, c->d_counters,
         c->d_counters + 1);
+    c->launches += 1;
     GB_CK(cudaGetLastError());
     if(phases & PHASE_MOVE)
     {
@@ -701,6 +716,7 @@ int finish(gb_ctx* c)
     GB_CK(cudaMemcpyAsync(&flags, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     GB_CK(cudaMemsetAsync(c->d_flags, 0, sizeof(int), c->stream));
     GB_CK(cudaStreamSynchronize(c->stream));
+    accumulate_pending(c);
     c->last.status_flags |= flags;
     if(flags & kFlagCapacity)
         return GB_E_CAPACITY;
@@ -779,8 +795,19 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
     c->nob    = cfg->n_obstacles;
     c->nmat   = cfg->n_materials;
     int st    = GB_OK;
-    if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
         st = GB_E_CUDA;
+    c->stream = c->own_stream;
+    c->timing = (cfg->flags & GB_FLAG_PHASE_TIMING) != 0;
+    if(st == GB_OK && c->timing)
+        for(int b = 0; b < 2 && st == GB_OK; ++b)
+            for(int k = 0; k <= GB_N_PHASES; ++k)
+                if(cudaEventCreate(&c->ev[b][k]) != cudaSuccess)
+                {
+                    st        = GB_E_CUDA;
+                    c->timing = false;
+                    break;
+                }
     if(st == GB_OK)
         st = alloc_state(c);
     if(st == GB_OK)
@@ -807,15 +834,56 @@ int gb_destroy(gb_ctx* c)
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
                     c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
-                    c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts};
+                    c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts,
+                    c->d_stage};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);
+    if(c->d_shape64 && c->d_shape64 != c->d_shape)
+        cudaFree(c->d_shape64);
+    if(c->d_verts64 && c->d_verts64 != c->d_verts)
+        cudaFree(c->d_verts64);
+    if(c->d_obs_shape64 && c->d_obs_shape64 != c->d_obs_shape)
+        cudaFree(c->d_obs_shape64);
     if(c->h_pinned)
         cudaFreeHost(c->h_pinned);
-    if(c->stream)
-        cudaStreamDestroy(c->stream);
+    if(c->timing)
+        for(int b = 0; b < 2; ++b)
+            for(int k = 0; k <= GB_N_PHASES; ++k)
+                cudaEventDestroy(c->ev[b][k]);
+    if(c->own_stream)
+        cudaStreamDestroy(c->own_stream);
     delete c;
+    return GB_OK;
+}
+
+int gb_set_stream(gb_ctx* c, void* cuda_stream)
+{
+    if(!c)
+        return GB_E_INVALID_ARG;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    c->stream = cuda_stream ? (cudaStream_t)cuda_stream : c->own_stream;
+    return GB_OK;
+}
+
+int gb_get_phase_times(gb_ctx* c, double* ms, int64_t* steps, int32_t reset)
+{
+    if(!c || !ms)
+        return GB_E_INVALID_ARG;
+    if(!c->timing)
+        return GB_E_NOT_READY;
+    GB_CK(cudaStreamSynchronize(c->stream));
+    accumulate_pending(c);
+    for(int k = 0; k < GB_N_PHASES; ++k)
+        ms[k] = c->phase_ms[k];
+    if(steps)
+        *steps = c->phase_steps;
+    if(reset)
+    {
+        for(int k = 0; k < GB_N_PHASES; ++k)
+            c->phase_ms[k] = 0;
+        c->phase_steps = 0;
+    }
     return GB_OK;
 }
 
@@ -865,7 +933,20 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
         ++c->key_bits;
     dfree(c->d_cstart);
     GB_TRY(dalloc(&c->d_cstart, (size_t)nc + 1));
-    int st = c->prec == GB_MIXED ? upload_tables<float>(c) : upload_tables<double>(c);
+    if(c->d_shape64 && c->d_shape64 != c->d_shape)
+    {
+        cudaFree(c->d_shape64);
+        cudaFree(c->d_verts64);
+    }
+    c->d_shape64 = c->d_verts64 = nullptr;
+    int st       = upload_tables<double>(c);
+    c->d_shape64 = c->d_shape;
+    c->d_verts64 = c->d_verts;
+    if(st == GB_OK && c->prec == GB_MIXED)
+    {
+        c->d_shape = c->d_verts = nullptr; // keep the FP64 copies, add FP32 ones
+        st                      = upload_tables<float>(c);
+    }
     if(st)
         return st;
     c->rb_set = true;
@@ -911,7 +992,16 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
             return GB_E_INVALID_ARG;
         GB_TRY(gb_rigid_body_properties(&obst[i], nullptr, &c->obs_props[i]));
     }
-    int st = c->prec == GB_MIXED ? upload_obstacles<float>(c) : upload_obstacles<double>(c);
+    if(c->d_obs_shape64 && c->d_obs_shape64 != c->d_obs_shape)
+        cudaFree(c->d_obs_shape64);
+    c->d_obs_shape64 = nullptr;
+    int st           = upload_obstacles<double>(c);
+    c->d_obs_shape64 = c->d_obs_shape;
+    if(st == GB_OK && c->prec == GB_MIXED)
+    {
+        c->d_obs_shape = nullptr;
+        st             = upload_obstacles<float>(c);
+    }
     if(st)
         return st;
     c->obs_set = true;
@@ -934,32 +1024,21 @@ int gb_set_transforms(gb_ctx* c, const double* t)
 {
     if(!c || !t)
         return GB_E_INVALID_ARG;
-    const size_t n = c->n;
-    std::vector<double> pos(3 * n);
-    for(size_t i = 0; i < n; ++i)
-        for(int k = 0; k < 3; ++k)
-            pos[k * n + i] = t[12 * i + 9 + k];
-    GB_CK(cudaMemcpy(c->d_pos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice));
+    const int n = c->n;
+    if(n == 0)
+        return c->tr_set = true, GB_OK;
+    GB_TRY(ensure_stage(c));
+    GB_CK(cudaMemcpyAsync(c->d_stage, t, 12 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice,
+                          c->stream));
     if(c->prec == GB_MIXED)
-    {
-        std::vector<float> q(4 * n);
-        for(size_t i = 0; i < n; ++i)
-        {
-            double qq[4];
-            basis_to_quat(t + 12 * i, qq);
-            for(int k = 0; k < 4; ++k)
-                q[k * n + i] = (float)qq[k];
-        }
-        GB_CK(cudaMemcpy(c->d_rot, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
+        k_set_transforms<float><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, c->d_pos, (float*)c->d_rot, 1);
     else
-    {
-        std::vector<double> b(9 * n);
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 9; ++k)
-                b[k * n + i] = t[12 * i + k];
-        GB_CK(cudaMemcpy(c->d_rot, b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice));
-    }
+        k_set_transforms<double><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, c->d_pos, (double*)c->d_rot, 0);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    GB_CK(cudaStreamSynchronize(c->stream));
     c->tr_set      = true;
     c->links_valid = c->detect_valid = false;
     return GB_OK;
@@ -967,62 +1046,41 @@ int gb_set_transforms(gb_ctx* c, const double* t)
 
 static int set_soa6(gb_ctx* c, const double* kin, void* a, void* b)
 {
-    const size_t n = c->n;
+    const int n = c->n;
+    if(n == 0)
+        return GB_OK;
+    GB_TRY(ensure_stage(c));
+    GB_CK(cudaMemcpyAsync(c->d_stage, kin, 6 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice,
+                          c->stream));
     if(c->prec == GB_MIXED)
-    {
-        std::vector<float> v(3 * n), w(3 * n);
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 3; ++k)
-            {
-                v[k * n + i] = (float)kin[6 * i + k];
-                w[k * n + i] = (float)kin[6 * i + 3 + k];
-            }
-        GB_CK(cudaMemcpy(a, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
-        GB_CK(cudaMemcpy(b, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
+        k_set_pairs3<float><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(n, c->d_stage, (float*)a,
+                                                                         (float*)b);
     else
-    {
-        std::vector<double> v(3 * n), w(3 * n);
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 3; ++k)
-            {
-                v[k * n + i] = kin[6 * i + k];
-                w[k * n + i] = kin[6 * i + 3 + k];
-            }
-        GB_CK(cudaMemcpy(a, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
-        GB_CK(cudaMemcpy(b, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
-    }
+        k_set_pairs3<double><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(n, c->d_stage,
+                                                                          (double*)a, (double*)b);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    GB_CK(cudaStreamSynchronize(c->stream));
     return GB_OK;
 }
 
 static int get_soa6(gb_ctx* c, double* kin, const void* a, const void* b)
 {
-    const size_t n = c->n;
-    GB_CK(cudaStreamSynchronize(c->stream));
+    const int n = c->n;
+    if(n == 0)
+        return GB_OK;
+    GB_TRY(ensure_stage(c));
     if(c->prec == GB_MIXED)
-    {
-        std::vector<float> v(3 * n), w(3 * n);
-        GB_CK(cudaMemcpy(v.data(), a, v.size() * sizeof(float), cudaMemcpyDeviceToHost));
-        GB_CK(cudaMemcpy(w.data(), b, w.size() * sizeof(float), cudaMemcpyDeviceToHost));
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 3; ++k)
-            {
-                kin[6 * i + k]     = v[k * n + i];
-                kin[6 * i + 3 + k] = w[k * n + i];
-            }
-    }
+        k_get_pairs3<float><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, (const float*)a, (const float*)b);
     else
-    {
-        std::vector<double> v(3 * n), w(3 * n);
-        GB_CK(cudaMemcpy(v.data(), a, v.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        GB_CK(cudaMemcpy(w.data(), b, w.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 3; ++k)
-            {
-                kin[6 * i + k]     = v[k * n + i];
-                kin[6 * i + 3 + k] = w[k * n + i];
-            }
-    }
+        k_get_pairs3<double><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, (const double*)a, (const double*)b);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    GB_CK(cudaMemcpyAsync(kin, c->d_stage, 6 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream));
+    GB_CK(cudaStreamSynchronize(c->stream));
     return GB_OK;
 }
 
@@ -1053,31 +1111,21 @@ int gb_get_transforms(gb_ctx* c, double* t)
 {
     if(!c || !t)
         return GB_E_INVALID_ARG;
-    const size_t n = c->n;
-    GB_CK(cudaStreamSynchronize(c->stream));
-    std::vector<double> pos(3 * n);
-    GB_CK(cudaMemcpy(pos.data(), c->d_pos, pos.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const int n = c->n;
+    if(n == 0)
+        return GB_OK;
+    GB_TRY(ensure_stage(c));
     if(c->prec == GB_MIXED)
-    {
-        std::vector<float> q(4 * n);
-        GB_CK(cudaMemcpy(q.data(), c->d_rot, q.size() * sizeof(float), cudaMemcpyDeviceToHost));
-        for(size_t i = 0; i < n; ++i)
-        {
-            const double qq[4] = {q[i], q[n + i], q[2 * n + i], q[3 * n + i]};
-            quat_to_basis(qq, t + 12 * i);
-        }
-    }
+        k_get_transforms<float><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, c->d_pos, (const float*)c->d_rot, 1);
     else
-    {
-        std::vector<double> b(9 * n);
-        GB_CK(cudaMemcpy(b.data(), c->d_rot, b.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        for(size_t i = 0; i < n; ++i)
-            for(int k = 0; k < 9; ++k)
-                t[12 * i + k] = b[k * n + i];
-    }
-    for(size_t i = 0; i < n; ++i)
-        for(int k = 0; k < 3; ++k)
-            t[12 * i + 9 + k] = pos[k * n + i];
+        k_get_transforms<double><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+            n, c->d_stage, c->d_pos, (const double*)c->d_rot, 0);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    GB_CK(cudaMemcpyAsync(t, c->d_stage, 12 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream));
+    GB_CK(cudaStreamSynchronize(c->stream));
     return GB_OK;
 }
 
@@ -1174,8 +1222,9 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
         o->cells_per_dir[k] = (int32_t)c->dims[k];
         o->grid_max[k]      = c->lc_max[k];
     }
-    o->key_bits  = c->key_bits;
-    o->cell_size = c->cell;
+    o->key_bits        = c->key_bits;
+    o->cell_size       = c->cell;
+    o->kernel_launches = c->launches;
     return GB_OK;
 }
 

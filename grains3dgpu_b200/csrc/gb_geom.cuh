@@ -329,14 +329,19 @@ struct JH
 template <typename S>
 struct GjkResult
 {
-    S     dist;
-    V3<S> pa, pb; // closest points in A's and B's local frames
-    int   iters;
+    S        dist;
+    S        lower;  // the optimality-gap lower bound mu on the distance
+    V3<S>    pa, pb; // closest points in A's and B's local frames
+    int      iters;
 };
 
 // computeClosestPoints_GJK_JH (GJK_JH.cpp:310-391), in A's frame with b2a.
+// `max_iter` caps the iterations (the reference's cap is 1000); the loop also
+// stops once the lower bound mu exceeds `reject_above` (the mixed mode's FP32
+// rejection test; +inf keeps the reference loop).
 template <typename S>
-GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
+GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
+                         int max_iter = 1000, S reject_above = S(INFINITY))
 {
     unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
     V3<S>    p[4], q[4];
@@ -360,9 +365,9 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
     const S abs_error      = S(1.e-4) * rel_error;
 
     V3<S> v    = support(A, zero3<S>()) - apply(b2a, support(B, zero3<S>()));
-    V3<S> w;
+    V3<S> w    = v;
     S     dist = norm(v);
-    while(bits < 15 && dist > k_higheps<S>() && num_iterations < 1000)
+    while(bits < 15 && dist > k_higheps<S>() && num_iterations < max_iter)
     {
         last     = 0;
         last_bit = 1;
@@ -377,6 +382,8 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
         const S g = dot(v, w) / dist;
         if(mu < g)
             mu = g;
+        if(mu > reject_above)
+            break;
         if(dist - mu <= dist * rel_error || mu < abs_error)
             break;
         if(jh.degenerate(all_bits, w))
@@ -404,6 +411,7 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
     r.pa      = s * r.pa;
     r.pb      = s * r.pb;
     r.dist    = dist;
+    r.lower   = mu;
     r.iters   = num_iterations;
     return r;
 }

@@ -204,17 +204,13 @@ GB_D S from_store(store_t<S> x)
     return S(x);
 }
 
-// ---- constants: Grains/Base/include/Basic.hh:103-128 (double values; the FP32
-// mode uses its own tolerances, never the reference's float ones) ------------
+// ---- constants: Grains/Base/include/Basic.hh:103-128, the double values.  The
+// FP32 mode uses the same values (they are absolute SI thresholds; the
+// reference's coarser float tolerances change the contact set) -------------
 template <typename S>
 GB_D S k_eps()
 {
     return S(1e-10);
-}
-template <>
-GB_D float k_eps<float>()
-{
-    return 1e-7f;
 }
 template <typename S>
 GB_D S k_loweps()
@@ -225,11 +221,6 @@ template <typename S>
 GB_D S k_higheps()
 {
     return S(1e-15);
-}
-template <>
-GB_D float k_higheps<float>()
-{
-    return 1e-30f;
 }
 template <typename S>
 GB_D S k_pi()

@@ -36,7 +36,94 @@ struct Tables
     const double*                obs_tr; // 12 per obstacle (basis, origin)
     const double*                obs_mass;
     int                          n_obs;
+    // FP64 copies of the shape tables (the mixed mode's polish reads these)
+    const RBShape<double>* shape64;
+    const Vert<double>*    verts64;
+    const RBShape<double>* obs_shape64;
 };
+
+// ---- mixed precision: FP32 contact detection, FP64 polish near contact ------
+// A pair whose FP32 GJK distance minus the crusts is below kPolishMargin times
+// the pair's size is re-solved in FP64, warm-started from the FP32 direction:
+// FP32 support points on mm-size grains carry ~1e-10 m of rounding, the same
+// order as a resting contact's overlap (m g / kn ~ 1e-8 m).
+constexpr float kPolishMargin = 64.0f * 1.1920929e-7f;
+
+GB_D M3<double> load_rot64(const State<float>& st, uint32_t i)
+{
+    return quat_to_matrix<double>((double)st.rot[0][i], (double)st.rot[1][i],
+                                  (double)st.rot[2][i], (double)st.rot[3][i]);
+}
+
+GB_D Contact<float> to_f(const Contact<double>& c)
+{
+    Contact<float> r;
+    r.pt      = cvt3<float>(c.pt);
+    r.vec     = cvt3<float>(c.vec);
+    r.overlap = (float)c.overlap;
+    return r;
+}
+
+// closestPointsRigidBodies for the mixed mode; points relative to A's centre
+GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& st, uint32_t a,
+                                  uint32_t b, uint32_t ra, uint32_t rb, const Body<float>& A,
+                                  const Body<float>& B, const M3<float>& RA, const M3<float>& RB,
+                                  const double xa[3], const double xb[3], int* iters)
+{
+    const V3<double> d64 = mk<double>(xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]);
+    if(A.type == GB_SPHERE && B.type == GB_SPHERE)
+    {
+        // closed form (CollisionDetection.cpp:26-48) directly in FP64
+        const double rA = tb.shape64[ra].rcirc, rB = tb.shape64[rb].rcirc;
+        const double nd = norm(d64), overlap = nd - rA - rB;
+        if(!(overlap < 0.0))
+            return no_contact<float>();
+        const V3<double> u = d64 / nd;
+        Contact<double>  c;
+        c.pt      = (rA + 0.5 * overlap) * u;
+        c.vec     = overlap * u;
+        c.overlap = overlap;
+        return to_f(c);
+    }
+    const V3<float> d = cvt3<float>(d64);
+    if(!(norm(d) - (A.rcirc + B.rcirc) < 0.0f))
+        return no_contact<float>();
+    if(!obb_overlap(A.bb, B.bb, RA, RB, d))
+        return no_contact<float>();
+    Tr<float>       b2a;
+    const M3<float> RAt = transpose(RA);
+    b2a.R               = mul(RAt, RB);
+    b2a.o               = mul(RAt, d);
+    // FP32 rejection: GJK's lower bound mu never exceeds the true distance, so a
+    // pair whose mu clears the crusts by the rounding margin is not in contact
+    const float reject = (A.crust + B.crust) + kPolishMargin * (A.rcirc + B.rcirc);
+    const GjkResult<float> g32 = gjk_jh(A, B, b2a, 32, reject);
+    *iters += g32.iters;
+    if(g32.lower > reject)
+        return no_contact<float>();
+    // every possible contact is re-solved on the FP64 path of the FP64 mode
+    const Body<double> A64 = load_body<double>(tb.shape64, ra, tb.verts64);
+    const Body<double> B64 = load_body<double>(tb.shape64, rb, tb.verts64);
+    const M3<double>   RA64 = load_rot64(st, a), RB64 = load_rot64(st, b);
+    Tr<double>         b2a64;
+    const M3<double>   RAt64 = transpose(RA64);
+    b2a64.R                  = mul(RAt64, RB64);
+    b2a64.o                  = mul(RAt64, d64);
+    const GjkResult<double> g = gjk_jh(A64, B64, b2a64);
+    *iters += g.iters;
+    const double distance = g.dist - (A64.crust + B64.crust);
+    if(distance > 0.0)
+        return no_contact<float>();
+    const V3<double> ptA = mul(RA64, g.pa);
+    const V3<double> ptB = mul(RB64, g.pb) + d64;
+    Contact<double>  c;
+    c.pt      = (ptA + ptB) / 2.0;
+    V3<double> vec = ptA - ptB;
+    vec            = round3(vec / norm(vec), 1e-10);
+    c.vec          = (-distance) * vec;
+    c.overlap      = distance;
+    return to_f(c);
+}
 
 template <typename S>
 GB_D constexpr bool is_mixed()
@@ -214,9 +301,13 @@ __global__ void __launch_bounds__(128)
         oB = mk<S>(S(xb[0]), S(xb[1]), S(xb[2]));
         d  = oB - oA;
     }
-    int              iters = 0;
-    const Contact<S> ci    = closest_points(A, B, RA, RB, oA, oB, d, &iters);
-    const bool       hit   = ci.overlap < S(0.0);
+    int        iters = 0;
+    Contact<S> ci;
+    if constexpr(is_mixed<S>())
+        ci = closest_mixed(tb, st, a, b, ra, rb, A, B, RA, RB, xa, xb, &iters);
+    else
+        ci = closest_points(A, B, RA, RB, oA, oB, d, &iters);
+    const bool hit = ci.overlap < S(0.0);
     Force<S>         F;
     F.f = F.t = F.m = zero3<S>();
     V3<S> xi_new    = zero3<S>();
@@ -334,7 +425,8 @@ struct StepParams
 template <typename S>
 GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
                         const double xa[3], const V3<S>& vA, const V3<S>& wA, S m1, int matA,
-                        const StepParams<S>& sp, V3<S>& F, V3<S>& T, int& nwall, int& iters)
+                        const StepParams<S>& sp, V3<S>& F, V3<S>& T, int& nwall, int& iters,
+                        uint32_t rbA, const Quat<double>& q64)
 {
     for(int o = 0; o < tb.n_obs; ++o)
     {
@@ -356,7 +448,28 @@ GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
         for(int k = 0; k < 9; ++k)
             RO.m[k] = S(ot[k]);
         Contact<S> ci;
-        if(O.type == GB_RECTANGLE)
+        if constexpr(is_mixed<S>())
+        {
+            // FP32 first; a contact (or a near miss within the rounding
+            // margin) is recomputed in FP64 relative to the particle centre
+            const V3<S> rn = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
+            if(O.type == GB_RECTANGLE)
+            {
+                const V3<S> rnA = s_copysign(S(1.0), dot(rn, oA - oO)) * rn;
+                const V3<S> pA  = mul(RA, support(A, mul_t(RA, -rnA)));
+                const S     sep = dot(rnA, pA - oO);
+                if(!(sep < S(1e-6)))
+                    continue;
+                const Body<double> A64 = load_body<double>(tb.shape64, rbA, tb.verts64);
+                const M3<double>   RA64 = quat_to_matrix<double>(q64.w, q64.v.x, q64.v.y, q64.v.z);
+                const V3<double>   oO64 = mk<double>(ot[9] - xa[0], ot[10] - xa[1], ot[11] - xa[2]);
+                ci = to_f(closest_rectangle(A64, RA64, zero3<double>(), oO64,
+                                            mk<double>(ot[2], ot[5], ot[8])));
+            }
+            else
+                ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+        }
+        else if(O.type == GB_RECTANGLE)
             ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
         else
             ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
@@ -429,8 +542,16 @@ __global__ void __launch_bounds__(kBlock)
         {
             const Body<S> A     = load_body<S>(tb.shape, r, tb.verts);
             const double  xa[3] = {st.pos[0][i], st.pos[1][i], st.pos[2][i]};
+            Quat<double>  q64;
+            q64.w = 1.0;
+            q64.v = zero3<double>();
+            if constexpr(is_mixed<S>())
+            {
+                q64.w = (double)st.rot[0][i];
+                q64.v = mk<double>((double)st.rot[1][i], (double)st.rot[2][i], (double)st.rot[3][i]);
+            }
             wall_contacts(tb, A, load_rot<S>(st, i), xa, v, w, m, tb.shape[r].material, sp, F, T,
-                          nwall, iters);
+                          nwall, iters, r, q64);
         }
         if(contacts_out)
             contacts_out[i] = nc;

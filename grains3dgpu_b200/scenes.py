@@ -35,6 +35,7 @@ class Scene:
     obstacle_transforms: np.ndarray  # float64 [n_obstacles, 12]
     contact_models: list     # dicts, l(l+1)/2+s indexed
     notes: str = ""
+    lattice_counts: tuple = None  # sites per axis of the jittered lattice (site k = particle k)
 
     @property
     def n(self):
@@ -268,7 +269,7 @@ def config2(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
             if cnt[0] * cnt[1] * cnt[2] >= n:
                 break
             pitch *= 0.995
-    pos, _ = lattice(box, pitch, margin, n, rng, 0.05 * pitch)
+    pos, counts = lattice(box, pitch, margin, n, rng, 0.05 * pitch)
     tr = np.zeros((n, 12))
     tr[:, :9] = random_rotations(rng, n)
     tr[:, 9:] = pos
@@ -277,7 +278,7 @@ def config2(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
                origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
     return Scene("config2", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
                  tr, np.zeros((n, 6)), walls, wtr, [law()] * 3,
-                 notes=f"lattice pitch {pitch*1e3:.3f} mm")
+                 notes=f"lattice pitch {pitch*1e3:.3f} mm", lattice_counts=tuple(counts))
 
 
 def _sq_axes_vec(r_eq, ba, ca, n1, n2):

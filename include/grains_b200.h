@@ -139,7 +139,18 @@ typedef struct gb_config {
 } gb_config;
 
 /* gb_config.flags */
-#define GB_FLAG_RECORD_CONTACT_INFO 1 /* keep per-pair contact info for dumps */
+#define GB_FLAG_RECORD_CONTACT_INFO 1 /* keep per-pair contact info for dumps   */
+#define GB_FLAG_PHASE_TIMING 2        /* CUDA-event timing of each step phase */
+
+/* Step phases timed under GB_FLAG_PHASE_TIMING (gb_get_phase_times). */
+#define GB_PHASE_HASH 0       /* cell hash per particle                       */
+#define GB_PHASE_SORT 1       /* radix sort of (cell, id)                     */
+#define GB_PHASE_CELL_START 2 /* cell-start table + sorted positions          */
+#define GB_PHASE_PAIR_COUNT 3 /* candidate count + scan                       */
+#define GB_PHASE_PAIR_FILL 4  /* candidate pair records                       */
+#define GB_PHASE_NARROW 5     /* OBB + GJK + contact law per pair             */
+#define GB_PHASE_PARTICLE 6   /* reduction + walls + gravity + integration    */
+#define GB_N_PHASES 7
 
 /* Counters of the last completed step (or of the last detect call). */
 typedef struct gb_stats {
@@ -154,7 +165,8 @@ typedef struct gb_stats {
     int32_t cells_per_dir[3];
     int32_t key_bits;
     double cell_size;
-    double grid_max[3]; /* linked-cell max corner actually used */
+    double grid_max[3];      /* linked-cell max corner actually used */
+    int64_t kernel_launches; /* kernels launched by this context so far */
 } gb_stats;
 
 /* ---- debug dump kinds -------------------------------------------------------- */
@@ -223,6 +235,13 @@ int gb_debug_dump(gb_ctx* ctx, int32_t kind, void* out, int64_t capacity,
 int gb_device_pointer(gb_ctx* ctx, const char* name, void** ptr);
 /* Synchronises the context stream and returns the device-side status flags. */
 int gb_synchronize(gb_ctx* ctx);
+/* Runs the context on the caller's CUDA stream (a cudaStream_t; NULL returns
+ * to the context's own stream).  The caller keeps ownership of the stream. */
+int gb_set_stream(gb_ctx* ctx, void* cuda_stream);
+/* Accumulated device time per phase (GB_N_PHASES doubles, milliseconds) and
+ * the number of steps they cover, when GB_FLAG_PHASE_TIMING is set; `reset`
+ * clears the accumulators after reading. */
+int gb_get_phase_times(gb_ctx* ctx, double* ms, int64_t* steps, int32_t reset);
 
 /* ---- host set-up helpers (no context needed) ------------------------------------- */
 /* Volume, mass, circumscribed radius, bounding box and inertia of a rigid

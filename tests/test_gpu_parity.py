@@ -123,3 +123,19 @@ def test_rerun_is_bitwise_deterministic(gb):
         s.step(5)
         out.append((s.transforms(), s.velocities()))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("kind", ["superquadric", "polyhedron", "box-on-walls"])
+def test_mixed_precision_single_step(gb, kind):
+    """Mixed mode (FP32 bulk, FP64 positions and GJK polish near contact)
+    against the FP64 mode from one identical state: same contact pairs, and
+    force error <= 1e-5 of the largest force."""
+    scene = make_scene(kind)
+    m = scenes.System(gb, scene, precision=abi.GB_MIXED)
+    f = scenes.System(gb, scene, precision=abi.GB_FP64)
+    m.detect()
+    f.detect()
+    assert np.array_equal(m.dump(abi.GB_DUMP_CONTACT_PAIRS), f.dump(abi.GB_DUMP_CONTACT_PAIRS))
+    a, b = m.torces(), f.torces()
+    assert np.abs(a[:, :3] - b[:, :3]).max() <= 1e-5 * np.abs(b[:, :3]).max()
+    assert np.abs(a[:, 3:] - b[:, 3:]).max() <= 1e-5 * np.abs(b[:, 3:]).max()
