@@ -243,6 +243,30 @@ int gb_set_stream(gb_ctx* ctx, void* cuda_stream);
  * clears the accumulators after reading. */
 int gb_get_phase_times(gb_ctx* ctx, double* ms, int64_t* steps, int32_t reset);
 
+/* ---- linked-cell sort without device allocation -------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory where they need the broad phase (their device memory is wholly
+ * reserved by another allocator, or their time loop must not block on a
+ * cudaMalloc): the cell hash, stable radix sort of (cell, particle id) and
+ * cell-start table of gb_update_links, with all scratch in a static device
+ * array of the library sized for at most 262,144 particles (about 6.4 MB held
+ * on every GPU that loads the library).  Nothing is allocated.
+ *   pos         device, 3*n doubles: x[n], y[n], z[n]
+ *   origin      host, the linked-cell min corner; cell_size and dims (host)
+ *               describe the grid as gb_get_stats reports it
+ *   sorted_ids  device, n uint32: particle ids sorted by (cell, id)
+ *   cell_start  device, dims[0]*dims[1]*dims[2]+1 uint32
+ *   stream      cudaStream_t (NULL: the legacy default stream)
+ * Returns GB_E_CAPACITY when n exceeds 262,144.  The first call on a device
+ * looks up the scratch's device address (one cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the scratch: calls
+ * whose work overlaps on the GPU race and must be serialised by the caller.
+ * The call synchronises `stream` to report GB_E_OUT_OF_DOMAIN /
+ * GB_E_NONFINITE like gb_update_links. */
+int gb_linked_cell_sort_static(const double* pos, int32_t n, const double origin[3],
+                               double cell_size, const int32_t dims[3], uint32_t* sorted_ids,
+                               uint32_t* cell_start, void* stream);
+
 /* ---- host set-up helpers (no context needed) ------------------------------------- */
 /* Volume, mass, circumscribed radius, bounding box and inertia of a rigid
  * body as RigidBody::RigidBody computes them; polyhedra use their convex
