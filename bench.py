@@ -91,8 +91,26 @@ def clocks_summary(path, device):
             "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons)}
 
 
+def replica_seed(rank):
+    """Each rank steps its own seeded packing (replicas; no data exchange)."""
+    return 2 + 1000 * rank
+
+
 def make_scene(args, rank):
-    return scenes.config2(seed=2 + 1000 * rank, n=args.n)
+    return scenes.config2(seed=replica_seed(rank), n=args.n)
+
+
+def aggregate(world, n_per_rank, steps, t_max):
+    """Whole-job particle-steps/s: all ranks' particle-steps over the slowest
+    rank's device time."""
+    return world * n_per_rank * steps / t_max
+
+
+def max_over_ranks(value, torch, world, device):
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
 
 
 # ---------------------------------------------------------------------------
@@ -327,11 +345,8 @@ def main():
         sampler.terminate()
         fh.close()
     clocks = clocks_summary(clk_path, torch.cuda.current_device())
-    t = torch.tensor([elapsed], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    t_max = float(t.item())
-    value = world * scene.n * args.steps / t_max
+    t_max = max_over_ranks(elapsed, torch, world, "cuda")
+    value = aggregate(world, scene.n, args.steps, t_max)
 
     # per-phase roofline (phase device time from CUDA events on the launch stream)
     hbm, hbm_kind = measured_hbm()
@@ -347,7 +362,7 @@ def main():
     top = max(phases, key=lambda k: phases[k]["ms"])
     roofline = {"kernel": top, "bound": "hbm", "achieved": phases[top]["achieved_gbs"],
                 "peak": hbm, "unit": "GB/s", "frac": phases[top]["frac_of_measured_hbm"],
-                "traffic": TRAFFIC_PER_STEP.get(top), "peak_kind": hbm_kind}
+                "traffic": traffic_bytes(top, scene.n), "peak_kind": hbm_kind}
 
     e2e_dev, e2e_wall, h2d, d2h = e2e_engine(sysm, args.e2e_steps, torch)
     e2e_value = world * scene.n * args.e2e_steps / max(e2e_dev, e2e_wall)
@@ -356,10 +371,8 @@ def main():
     # the all-FP64 run of the same kernels on the same workload
     _, el64, _, ms64, n64, _ = run_engine(args, scene, abi.GB_FP64, args.fp64_steps, 3, torch,
                                           rank, world)
-    t64 = torch.tensor([el64], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t64, op=torch.distributed.ReduceOp.MAX)
-    value64 = world * scene.n * args.fp64_steps / float(t64.item())
+    t64 = max_over_ranks(el64, torch, world, "cuda")
+    value64 = aggregate(world, scene.n, args.fp64_steps, t64)
     ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
 
     cpu = None
@@ -387,7 +400,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                     "ms_per_step": max(e2e_dev, e2e_wall) / args.e2e_steps * 1e3},
-            "fp64": {"value": value64, "ms_per_step": float(t64.item()) / args.fp64_steps * 1e3,
+            "fp64": {"value": value64, "ms_per_step": t64 / args.fp64_steps * 1e3,
                      "steps": args.fp64_steps},
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
@@ -401,9 +414,17 @@ def main():
     return 0
 
 
-# DRAM bytes per step of the dominant kernels from one ncu capture, scaled to
-# the full workload (None until captured).
-TRAFFIC_PER_STEP = {}
+# DRAM bytes (read + write) per particle of the dominant kernels, from one
+# ncu capture of this workload with 400,000 particles
+# (profiles/k_particles_k_pairs_config2_400k.md); the traffic scales with the
+# particle count, so a full launch moves this many bytes per particle.
+TRAFFIC_PER_PARTICLE = {"particle": 95.96e6 / 400_000, "pair_count": 17.15e6 / 400_000,
+                        "pair_fill": 18.75e6 / 400_000}
+
+
+def traffic_bytes(phase, n):
+    v = TRAFFIC_PER_PARTICLE.get(phase)
+    return None if v is None else v * n
 
 if __name__ == "__main__":
     sys.exit(main())
