@@ -301,17 +301,31 @@ __global__ void __launch_bounds__(kBlock) k_cell_start(const uint32_t* __restric
     }
 }
 
-// positions and bounding radii in sorted order, for contiguous neighbour reads
+// positions and bounding radii in sorted order, for contiguous neighbour
+// reads.  out32 (optional) is an FP32 copy for a conservative candidate
+// pre-test: its radius is inflated by 2^-19 (|x| + |y| + |z| + r) = 32 u (...),
+// u = 2^-24, and rounded up.  The rounding of the FP32 coordinates, of their
+// difference and of the FP32 sum of squares (FMA or not) moves |d| by less
+// than 1.01 u (|xa|_1 + |xb|_1) + 1.74 u |d| + 2.1 u |d|, so an FP32 "no
+// overlap" (|d|^2 >= (wA + wB)^2) implies |d| >= (rA + rB)(1 + 26 u) in exact
+// arithmetic, which the FP64 test also rejects.
 __global__ void k_gather_sorted(int n, const uint32_t* __restrict__ sids,
                                 const double* __restrict__ px, const double* __restrict__ py,
                                 const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
-                                const double* __restrict__ rcirc, double4* __restrict__ out)
+                                const double* __restrict__ rcirc, double4* __restrict__ out,
+                                float4* __restrict__ out32)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if(t >= n)
         return;
     const uint32_t i = sids[t];
-    out[t]           = make_double4(px[i], py[i], pz[i], rcirc[rb_id[i]]);
+    const double4  p = make_double4(px[i], py[i], pz[i], rcirc[rb_id[i]]);
+    out[t]           = p;
+    if(out32)
+    {
+        const double slack = 0x1p-19 * (fabs(p.x) + fabs(p.y) + fabs(p.z) + p.w);
+        out32[t] = make_float4((float)p.x, (float)p.y, (float)p.z, __double2float_ru(p.w + slack));
+    }
 }
 
 } // namespace gb

@@ -119,6 +119,9 @@ struct gb_ctx
     uint32_t *d_skeys = nullptr, *d_sids = nullptr; // results (alias into d_k/d_i)
     uint32_t *d_hist = nullptr, *d_part = nullptr, *d_cstart = nullptr;
     double4*  d_spos = nullptr;
+    float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
+    uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
+    bool      obs_general = false; // some obstacle is not a Rectangle
     size_t    part_cap = 0, hist_cap = 0;
 
     // pairs (double-buffered for the tangential history)
@@ -380,6 +383,8 @@ int alloc_state(gb_ctx* c)
         GB_TRY(dalloc(&c->d_off[b], n + 1));
     }
     GB_TRY(dalloc(&c->d_spos, n));
+    GB_TRY(dalloc(&c->d_spos32, n));
+    GB_TRY(dalloc(&c->d_slot, (size_t)n * kPairSlots));
     GB_TRY(dalloc(&c->d_count, n + 1));
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
@@ -513,7 +518,8 @@ int broad_phase(gb_ctx* c)
         c->d_skeys, (uint32_t)n, c->ncells, c->d_cstart);
     k_gather_sorted<<<nb, kBlock, 0, s>>>(n, c->d_sids, c->d_pos, c->d_pos + n,
                                           c->d_pos + 2 * (size_t)n, c->d_rb_id, c->d_rcirc64,
-                                          c->d_spos);
+                                          c->d_spos,
+                                          c->prec == GB_FP64_STRICT ? nullptr : c->d_spos32);
     c->launches += 2;
     GB_CK(cudaGetLastError());
     mark(c, 3);
@@ -532,15 +538,13 @@ int build_pairs(gb_ctx* c)
         c->cur ^= 1; // last step's pair list becomes the history
     uint32_t* off = c->d_off[c->cur];
     if(strict)
-        k_pairs<true, false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
-                                                    c->d_cstart, c->dims[0], c->dims[1],
-                                                    c->dims[2], c->d_count, nullptr, nullptr,
-                                                    nullptr, 0, c->d_flags);
+        k_pair_count<true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, nullptr,
+                                                 c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
+                                                 c->d_count, c->d_slot);
     else
-        k_pairs<false, false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
-                                                     c->d_cstart, c->dims[0], c->dims[1],
-                                                     c->dims[2], c->d_count, nullptr, nullptr,
-                                                     nullptr, 0, c->d_flags);
+        k_pair_count<false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
+                                                  c->d_spos32, c->d_cstart, c->dims[0],
+                                                  c->dims[1], c->dims[2], c->d_count, c->d_slot);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
@@ -551,14 +555,15 @@ int build_pairs(gb_ctx* c)
     const int64_t total = c->h_pinned[0];
     GB_TRY(ensure_pairs(c, total));
     if(strict)
-        k_pairs<true, true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, c->d_cstart,
-                                                   c->dims[0], c->dims[1], c->dims[2], nullptr, off,
-                                                   c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags);
+        k_pair_fill<true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, nullptr,
+                                                c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
+                                                c->d_count, c->d_slot, off, c->d_pa,
+                                                c->d_pb[c->cur], c->cap, c->d_flags);
     else
-        k_pairs<false, true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
-                                                    c->d_cstart, c->dims[0], c->dims[1],
-                                                    c->dims[2], nullptr, off, c->d_pa,
-                                                    c->d_pb[c->cur], c->cap, c->d_flags);
+        k_pair_fill<false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
+                                                 c->d_spos32, c->d_cstart, c->dims[0], c->dims[1],
+                                                 c->dims[2], c->d_count, c->d_slot, off, c->d_pa,
+                                                 c->d_pb[c->cur], c->cap, c->d_flags);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 5);
@@ -587,6 +592,23 @@ PairOut<store_t<S>> pair_out(gb_ctx* c)
     for(int k = 0; k < 3; ++k)
         po.prev_xi[k] = c->d_xi[prev] ? (const St*)c->d_xi[prev] + k * cap : nullptr;
     return po;
+}
+
+// k_particles without the general-obstacle GJK unless some obstacle needs it
+template <typename S>
+void launch_particles(gb_ctx* c, const State<store_t<S>>& st, const Tables<S>& tb,
+                      const PairOut<store_t<S>>& po, const StepParams<S>& sp, int* contacts_out)
+{
+    const int nb = std::max(1, blocks(c->n, kBlock));
+    if(c->obs_general)
+        k_particles<S, true><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po, sp,
+                                                            contacts_out, c->d_counters,
+                                                            c->d_counters + 1);
+    else
+        k_particles<S, false><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po,
+                                                             sp, contacts_out, c->d_counters,
+                                                             c->d_counters + 1);
+    c->launches += 1;
 }
 
 template <typename S>
@@ -625,9 +647,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     sp.law_kind   = c->cfg.contact_law;
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
-    k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, s>>>(
-        c->n, st, tb, c->d_off[c->cur], po, sp, c->d_contacts, c->d_counters, c->d_counters + 1);
-    c->launches += 1;
+    launch_particles<S>(c, st, tb, po, sp, c->d_contacts);
     GB_CK(cudaGetLastError());
     mark(c, 7);
     if(c->timing)
@@ -670,10 +690,7 @@ int run_particles(gb_ctx* c, int phases)
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
     PairOut<St> po = pair_out<S>(c);
-    k_particles<S><<<std::max(1, blocks(c->n, kBlock)), kBlock, 0, c->stream>>>(
-        c->n, state_of<St>(c), tables_of<S>(c), c->d_off[c->cur], po, sp, nullptr, c->d_counters,
-        c->d_counters + 1);
-    c->launches += 1;
+    launch_particles<S>(c, state_of<St>(c), tables_of<S>(c), po, sp, nullptr);
     GB_CK(cudaGetLastError());
     if(phases & PHASE_MOVE)
     {
@@ -832,7 +849,7 @@ int gb_destroy(gb_ctx* c)
     void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
                     c->d_obs_mass, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
-                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_count,
+                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_spos32, c->d_slot, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts,
                     c->d_stage};
@@ -981,6 +998,9 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
     if(!c || (c->nob && (!obst || !transforms)))
         return GB_E_INVALID_ARG;
     c->obs.assign(obst, obst + c->nob);
+    c->obs_general = false;
+    for(int i = 0; i < c->nob; ++i)
+        c->obs_general = c->obs_general || obst[i].convex.type != GB_RECTANGLE;
     c->obs_tr.assign(transforms, transforms + 12 * (size_t)c->nob);
     c->obs_props.resize(c->nob);
     for(int i = 0; i < c->nob; ++i)

@@ -43,10 +43,12 @@ struct Tables
 };
 
 // ---- mixed precision: FP32 contact detection, FP64 polish near contact ------
-// A pair whose FP32 GJK distance minus the crusts is below kPolishMargin times
-// the pair's size is re-solved in FP64, warm-started from the FP32 direction:
-// FP32 support points on mm-size grains carry ~1e-10 m of rounding, the same
-// order as a resting contact's overlap (m g / kn ~ 1e-8 m).
+// FP32 GJK serves only as a certified rejection: its lower bound never exceeds
+// the true distance, so a pair whose bound clears the crusts by kPolishMargin
+// times the pair's size has no contact.  Every other pair is re-solved from
+// scratch by the FP64 GJK of the FP64 mode: FP32 support points on mm-size
+// grains carry ~1e-10 m of rounding, the order of a resting contact's overlap
+// (m g / kn ~ 1e-8 m), so contact points and overlaps come from FP64.
 constexpr float kPolishMargin = 64.0f * 1.1920929e-7f;
 
 GB_D M3<double> load_rot64(const State<float>& st, uint32_t i)
@@ -175,24 +177,29 @@ GB_D Law<S> load_law(const Law<store_t<S>>* t, int ma, int mb)
 // neighbour table of LinkedCell.cpp:41-70) and the particles of each cell in
 // ascending id, keeping ordered pairs (A, B != A) whose bounding spheres
 // overlap: norm(xB - xA) - (rA + rB) < 0 (CollisionDetection.cpp:209-211).
-// COUNT: writes the count per particle id; FILL: writes the pair records.
-template <bool STRICT, bool FILL>
-__global__ void __launch_bounds__(kBlock)
-    k_pairs(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
-            const double4* __restrict__ spos, const uint32_t* __restrict__ cstart, uint32_t nx,
-            uint32_t ny, uint32_t nz, uint32_t* __restrict__ count,
-            const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
-            uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
+// The three cells x-1, x, x+1 of one (y, z) row have consecutive keys, so
+// their particles are one contiguous range of the sorted order: the walk is
+// nine ranges, visiting the candidates in the same order as the 27 cells.
+// Outside STRICT a conservative FP32 test on spos32 (k_gather_sorted inflates
+// its radii by a bound on the FP32 rounding, so an FP32 rejection implies an
+// FP64 rejection) skips most non-candidates before the FP64 test: the
+// candidate set is the FP64 test's.
+constexpr int kPairSlots = 16; // candidates kept per particle by the count pass
+
+template <bool STRICT, typename Hit>
+GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
+                             const double4* __restrict__ spos,
+                             const float4* __restrict__ spos32,
+                             const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny,
+                             uint32_t nz, Hit&& hit)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if(s >= n)
-        return;
-    const uint32_t a   = sids[s];
     const uint32_t key = skeys[s];
     const double4  pa  = spos[s];
-    const int      cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
-    uint32_t       c  = 0;
-    int64_t        out = FILL ? (int64_t)offset[a] : 0;
+    float4         pa32;
+    if constexpr(!STRICT)
+        pa32 = spos32[s];
+    const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+    const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < (int)nx ? cx + 1 : cx;
     for(int k = -1; k < 2; ++k)
     {
         const int z = cz + k;
@@ -204,55 +211,103 @@ __global__ void __launch_bounds__(kBlock)
             if(y < 0 || y >= (int)ny)
                 continue;
             const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
-            for(int i = -1; i < 2; ++i)
+            const uint32_t t1  = cstart[row + (uint32_t)x1 + 1];
+            for(uint32_t t = cstart[row + (uint32_t)x0]; t < t1; ++t)
             {
-                const int x = cx + i;
-                if(x < 0 || x >= (int)nx)
+                if(t == (uint32_t)s)
                     continue;
-                const uint32_t nc = row + (uint32_t)x;
-                const uint32_t t1 = cstart[nc + 1];
-                for(uint32_t t = cstart[nc]; t < t1; ++t)
+                if constexpr(!STRICT)
                 {
-                    if(t == (uint32_t)s)
+                    const float4 q  = spos32[t];
+                    const float  fx = q.x - pa32.x, fy = q.y - pa32.y, fz = q.z - pa32.z;
+                    const float  fr = pa32.w + q.w;
+                    if(fx * fx + fy * fy + fz * fz >= fr * fr)
                         continue;
-                    const double4 pb = spos[t];
-                    bool          hit;
-                    if constexpr(STRICT)
-                    {
-                        const dstrict dx = dstrict(pb.x) - dstrict(pa.x);
-                        const dstrict dy = dstrict(pb.y) - dstrict(pa.y);
-                        const dstrict dz = dstrict(pb.z) - dstrict(pa.z);
-                        hit = s_sqrt(dx * dx + dy * dy + dz * dz) - (dstrict(pa.w) + dstrict(pb.w))
-                              < dstrict(0.0);
-                    }
-                    else
-                    {
-                        const double dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
-                        const double r  = pa.w + pb.w;
-                        hit             = dx * dx + dy * dy + dz * dz < r * r;
-                    }
-                    if(hit)
-                    {
-                        if constexpr(FILL)
-                        {
-                            if(out < cap)
-                            {
-                                pair_a[out] = a;
-                                pair_b[out] = sids[t];
-                            }
-                            else
-                                atomicOr(flags, kFlagCapacity);
-                            ++out;
-                        }
-                        else
-                            ++c;
-                    }
                 }
+                const double4 pb = spos[t];
+                bool          h;
+                if constexpr(STRICT)
+                {
+                    const dstrict dx = dstrict(pb.x) - dstrict(pa.x);
+                    const dstrict dy = dstrict(pb.y) - dstrict(pa.y);
+                    const dstrict dz = dstrict(pb.z) - dstrict(pa.z);
+                    h = s_sqrt(dx * dx + dy * dy + dz * dz) - (dstrict(pa.w) + dstrict(pb.w))
+                        < dstrict(0.0);
+                }
+                else
+                {
+                    const double dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
+                    const double r  = pa.w + pb.w;
+                    h               = dx * dx + dy * dy + dz * dz < r * r;
+                }
+                if(h)
+                    hit(t);
             }
         }
     }
-    if constexpr(!FILL)
-        count[a] = c;
+}
+
+// Count pass: the number of candidates of each particle (by id) and the first
+// kPairSlots of them (sorted positions t, in enumeration order) in slot[s].
+template <bool STRICT>
+__global__ void __launch_bounds__(kBlock)
+    k_pair_count(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
+                 const double4* __restrict__ spos, const float4* __restrict__ spos32,
+                 const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
+                 uint32_t* __restrict__ count, uint32_t* __restrict__ slot)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if(s >= n)
+        return;
+    uint32_t  c    = 0;
+    uint32_t* mine = slot + (size_t)s * kPairSlots;
+    for_each_candidate<STRICT>(s, skeys, spos, spos32, cstart, nx, ny, nz, [&](uint32_t t) {
+        if(c < kPairSlots)
+            mine[c] = t;
+        ++c;
+    });
+    count[sids[s]] = c;
+}
+
+// Fill pass: the pair records of particle a at offset[a], copied from its
+// slots, or enumerated again when it had more than kPairSlots candidates.
+template <bool STRICT>
+__global__ void __launch_bounds__(kBlock)
+    k_pair_fill(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
+                const double4* __restrict__ spos, const float4* __restrict__ spos32,
+                const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
+                const uint32_t* __restrict__ count, const uint32_t* __restrict__ slot,
+                const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
+                uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if(s >= n)
+        return;
+    const uint32_t a = sids[s];
+    const uint32_t c = count[a];
+    if(c == 0)
+        return;
+    int64_t out = offset[a];
+    if(out + c > cap)
+    {
+        atomicOr(flags, kFlagCapacity);
+        return;
+    }
+    if(c <= kPairSlots)
+    {
+        const uint32_t* mine = slot + (size_t)s * kPairSlots;
+        for(uint32_t k = 0; k < c; ++k)
+        {
+            pair_a[out + k] = a;
+            pair_b[out + k] = sids[mine[k]];
+        }
+        return;
+    }
+    for_each_candidate<STRICT>(s, skeys, spos, spos32, cstart, nx, ny, nz, [&](uint32_t t) {
+        pair_a[out] = a;
+        pair_b[out] = sids[t];
+        ++out;
+    });
 }
 
 // ---- narrow phase + contact law, one thread per candidate pair ---------------
@@ -422,7 +477,7 @@ struct StepParams
     int      phases;
 };
 
-template <typename S>
+template <typename S, bool GEN>
 GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
                         const double xa[3], const V3<S>& vA, const V3<S>& wA, S m1, int matA,
                         const StepParams<S>& sp, V3<S>& F, V3<S>& T, int& nwall, int& iters,
@@ -448,6 +503,24 @@ GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
         for(int k = 0; k < 9; ++k)
             RO.m[k] = S(ot[k]);
         Contact<S> ci;
+        if(O.type == GB_RECTANGLE)
+        {
+            // A lies in its bounding box (half extents A.bb), so its support
+            // point towards the plane is at most bb . |RA^T n| from its centre:
+            // a centre farther than that from the plane (plus a bound on the
+            // rounding of both sides) has no contact with it, and the support
+            // evaluation is skipped.  The same wall is rejected by the full
+            // computation, so the contact set is unchanged.
+            const V3<S> rn  = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
+            const V3<S> nb  = mul_t(RA, rn);
+            const S     dc  = s_fabs(dot(rn, oA - oO));
+            const S     hb  = A.bb.x * s_fabs(nb.x) + A.bb.y * s_fabs(nb.y) + A.bb.z * s_fabs(nb.z);
+            const S     mag = s_fabs(oA.x) + s_fabs(oA.y) + s_fabs(oA.z) + s_fabs(oO.x)
+                          + s_fabs(oO.y) + s_fabs(oO.z) + hb;
+            const S slack = is_mixed<S>() ? S(1e-6) + S(1e-6) * mag : S(1e-12) * (S(1.0) + mag);
+            if(dc - hb > slack)
+                continue;
+        }
         if constexpr(is_mixed<S>())
         {
             // FP32 first; a contact (or a near miss within the rounding
@@ -466,13 +539,17 @@ GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
                 ci = to_f(closest_rectangle(A64, RA64, zero3<double>(), oO64,
                                             mk<double>(ot[2], ot[5], ot[8])));
             }
-            else
+            else if constexpr(GEN)
                 ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+            else
+                ci = no_contact<S>();
         }
         else if(O.type == GB_RECTANGLE)
             ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
-        else
+        else if constexpr(GEN)
             ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+        else
+            ci = no_contact<S>();
         if(!(ci.overlap < S(0.0)))
             continue;
         ++nwall;
@@ -509,8 +586,15 @@ GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
     }
 }
 
-template <typename S>
-__global__ void __launch_bounds__(kBlock)
+// GEN: some obstacle is not a Rectangle and needs the full GJK.  Without it
+// the rare FP64 wall recomputation alone sets the register count; the launch
+// bound keeps GB_PARTICLES_MIN_BLOCKS 256-thread blocks resident per SM and
+// lets the rare paths spill instead.
+#ifndef GB_PARTICLES_MIN_BLOCKS
+#define GB_PARTICLES_MIN_BLOCKS 3
+#endif
+template <typename S, bool GEN>
+__global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
                 unsigned long long* __restrict__ counters, unsigned long long* __restrict__ gjk_iters)
@@ -550,7 +634,7 @@ __global__ void __launch_bounds__(kBlock)
                 q64.w = (double)st.rot[0][i];
                 q64.v = mk<double>((double)st.rot[1][i], (double)st.rot[2][i], (double)st.rot[3][i]);
             }
-            wall_contacts(tb, A, load_rot<S>(st, i), xa, v, w, m, tb.shape[r].material, sp, F, T,
+            wall_contacts<S, GEN>(tb, A, load_rot<S>(st, i), xa, v, w, m, tb.shape[r].material, sp, F, T,
                           nwall, iters, r, q64);
         }
         if(contacts_out)

@@ -338,6 +338,10 @@ class System:
         self._check(lib.set_rigid_bodies(
             self.ctx, rbs.ctypes.data_as(abi.C.POINTER(abi.RigidBodyDesc)),
             abi.dptr(verts) if verts.size else None, verts.shape[0]), "set_rigid_bodies")
+        need = self.cfg.n_materials * (self.cfg.n_materials + 1) // 2
+        if len(scene.contact_models) != need:
+            raise ValueError(f"{len(scene.contact_models)} contact laws for "
+                             f"{self.cfg.n_materials} materials (need {need})")
         cms = abi.contact_model_array(scene.contact_models)
         self._check(lib.set_contact_models(self.ctx, cms), "set_contact_models")
         if self.cfg.n_obstacles:

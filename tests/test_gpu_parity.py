@@ -129,7 +129,7 @@ def test_rerun_is_bitwise_deterministic(gb):
 def test_mixed_precision_single_step(gb, kind):
     """Mixed mode (FP32 bulk, FP64 positions and GJK polish near contact)
     against the FP64 mode from one identical state: same contact pairs, and
-    force error <= 1e-5 of the largest force (the north-star bound)."""
+    force error <= 1e-5 of the largest force."""
     scene = make_scene(kind)
     m = scenes.System(gb, scene, precision=abi.GB_MIXED)
     f = scenes.System(gb, scene, precision=abi.GB_FP64)
