@@ -18,6 +18,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -97,7 +98,7 @@ def replica_seed(rank):
 
 
 def make_scene(args, rank):
-    return scenes.config2(seed=replica_seed(rank), n=args.n)
+    return scenes.polydisperse_superquadrics(seed=replica_seed(rank), n=args.n)
 
 
 def aggregate(world, n_per_rank, steps, t_max):
@@ -270,7 +271,7 @@ def reference_arm(args):
         nthreads = len(os.sched_getaffinity(0))
     except Exception:
         nthreads = os.cpu_count() or 1
-    scene = scenes.config2(seed=2, n=args.n)
+    scene = scenes.polydisperse_superquadrics(seed=2, n=args.n)
     cell = full_cell_size(scene)
     blocks = [b for b in sample_blocks(scene, args.ref_sample, nthreads) if b.size]
     nthreads = len(blocks)
@@ -295,7 +296,7 @@ def reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": "config2 sample: polydisperse superquadrics, 0.3x0.3x1.2 m box",
+        "config": {"workload": "sample of 1,000,000 polydisperse superquadrics in a 0.3x0.3x1.2 m box",
                    "sample_particles_per_thread": m, "threads": nthreads},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": nthreads, "kind": kind,
                          "sample": f"{nthreads} threads, each stepping its own lattice block of "
@@ -336,8 +337,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     scene = make_scene(args, rank)
-    clk_path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")
-    os.makedirs(os.path.dirname(clk_path), exist_ok=True)
+    fd, clk_path = tempfile.mkstemp(prefix=f"gb_clocks_rank{rank}_", suffix=".csv")
+    os.close(fd)
     sampler, fh = clocks_sampler(clk_path)
     sysm, elapsed, launches, ms, nsteps, st = run_engine(
         args, scene, abi.GB_MIXED, args.steps, args.warmup, torch, rank, world)
@@ -345,6 +346,7 @@ def main():
         sampler.terminate()
         fh.close()
     clocks = clocks_summary(clk_path, torch.cuda.current_device())
+    os.unlink(clk_path)
     t_max = max_over_ranks(elapsed, torch, world, "cuda")
     value = aggregate(world, scene.n, args.steps, t_max)
 
@@ -386,9 +388,8 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (f64 positions, f64 GJK polish near contact)",
             "data": "synthetic (seeded jittered-lattice packing)",
-            "config": {"workload": "config2: 1,000,000 polydisperse superquadrics in a "
-                                   "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision"
-                       if scene.n == 1_000_000 else f"config2 with {scene.n} particles",
+            "config": {"workload": f"{scene.n:,} polydisperse superquadrics in a "
+                                   "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision",
                        "n_particles": scene.n, "precision": "mixed",
                        "n_cells": st.n_cells, "candidate_pairs_last_step": st.candidate_pairs,
                        "l2": "per-step working set > 126 MB L2, no flush",
@@ -416,7 +417,7 @@ def main():
 
 # DRAM bytes (read + write) per particle of the dominant kernels, from one
 # ncu capture of this workload with 400,000 particles
-# (profiles/k_particles_k_pairs_config2_400k.md); the traffic scales with the
+# (profiles/k_particles_k_pairs_superquadrics_400k.md); the traffic scales with the
 # particle count, so a full launch moves this many bytes per particle.
 TRAFFIC_PER_PARTICLE = {"particle": 95.96e6 / 400_000, "pair_count": 17.15e6 / 400_000,
                         "pair_fill": 18.75e6 / 400_000}

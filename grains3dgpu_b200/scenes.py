@@ -152,7 +152,7 @@ def superquadric_semi_axes(r_eq, ba, ca, n1, n2):
 
 
 # ---------------------------------------------------------------------------
-def config0(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000,
+def superquadric_column(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000,
             shape="superquadric", jitter=0.15e-3, tilt=None):
     """2,000 identical superquadrics a=b=c=1 mm, n1=n2=4, on a 2.4 mm jittered
     lattice (+-0.15 mm) with random orientations, in a closed box.  The box
@@ -189,7 +189,7 @@ def config0(seed=0, n=2000, box=(0.020, 0.020, 0.080), pitch=2.4e-3, steps=20000
     walls, wtr = box_walls(box)
     cfg = dict(n_particles=n, n_rigid_bodies=1, n_obstacles=6, n_materials=2,
                origin=(0, 0, 0), max_coordinate=box, dt=2e-6, gravity=(0, 0, -9.81))
-    return Scene("config0", cfg, rbs, np.zeros((0, 3)), np.zeros(n, np.uint32), tr,
+    return Scene("superquadric_column", cfg, rbs, np.zeros((0, 3)), np.zeros(n, np.uint32), tr,
                  np.zeros((n, 6)), walls, wtr, [law()] * 3,
                  notes=f"box raised to {box[2]*1e3:.0f} mm; {steps} steps nominal")
 
@@ -209,7 +209,7 @@ def ellipsoid_points(rng, axes, k):
     return np.array(out[:k])
 
 
-def config1(seed=1, n=200_000, box=(0.100, 0.100, 0.400), pitch=2.6e-3,
+def polyhedra_box(seed=1, n=200_000, box=(0.100, 0.100, 0.400), pitch=2.6e-3,
             hull_centroid=None):
     """Convex polyhedra: each the hull of 8-32 points uniform on an ellipsoid
     of semi-axes 1 mm x U(0.6,1.4) x U(0.6,1.4) mm, re-centred on the hull
@@ -239,11 +239,11 @@ def config1(seed=1, n=200_000, box=(0.100, 0.100, 0.400), pitch=2.6e-3,
     walls, wtr = box_walls(box)
     cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
                origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
-    return Scene("config1", cfg, rbs, verts, np.arange(n, dtype=np.uint32), tr,
+    return Scene("polyhedra_box", cfg, rbs, verts, np.arange(n, dtype=np.uint32), tr,
                  np.zeros((n, 6)), walls, wtr, [law()] * 3)
 
 
-def config2(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
+def polydisperse_superquadrics(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
     """Polydisperse superquadrics: r_eq lognormal (median 1 mm, sigma 0.25)
     clipped to [0.5, 2] mm, b/a and c/a ~ U(0.5, 2), n1, n2 ~ U(2, 10), on the
     densest jittered cubic lattice that holds n sites in the box."""
@@ -276,7 +276,7 @@ def config2(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=None):
     walls, wtr = box_walls(box)
     cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
                origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
-    return Scene("config2", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
+    return Scene("polydisperse_superquadrics", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
                  tr, np.zeros((n, 6)), walls, wtr, [law()] * 3,
                  notes=f"lattice pitch {pitch*1e3:.3f} mm", lattice_counts=tuple(counts))
 
@@ -290,7 +290,7 @@ def _sq_axes_vec(r_eq, ba, ca, n1, n2):
     return (v / (unit * ba * ca)) ** (1.0 / 3.0)
 
 
-def config3(seed=3, n=10_000, column_height=None):
+def superquadric_column_on_plate(seed=3, n=10_000, column_height=None):
     """Superquadrics with n1, n2 ~ U(2, 8) and semi-axes ~ U(0.8, 1.2) mm in a
     column resting on a plate (its bottom layer within crust range of the
     plate, so contacts exist within the 2,000-step window); initial
@@ -316,7 +316,7 @@ def config3(seed=3, n=10_000, column_height=None):
     walls, wtr = box_walls(box)
     cfg = dict(n_particles=n, n_rigid_bodies=n, n_obstacles=6, n_materials=2,
                origin=(0, 0, 0), max_coordinate=box, dt=2e-6, gravity=(0, 0, -9.81))
-    return Scene("config3", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
+    return Scene("superquadric_column_on_plate", cfg, rbs, np.zeros((0, 3)), np.arange(n, dtype=np.uint32),
                  tr, vel, walls, wtr, [law()] * 3)
 
 

@@ -157,9 +157,9 @@ def main():
     rng = np.random.default_rng(20261203)
     functions(R, rng)
     hooke_cases(R, rng)
-    system(R, "superquadric", scenes.config0(n=400, pitch=2.05e-3,
+    system(R, "superquadric", scenes.superquadric_column(n=400, pitch=2.05e-3,
                                              box=(0.012, 0.012, 0.036)), 20)
-    s = scenes.config0(n=400, pitch=2.05e-3, box=(0.012, 0.012, 0.036), shape="sphere")
+    s = scenes.superquadric_column(n=400, pitch=2.05e-3, box=(0.012, 0.012, 0.036), shape="sphere")
     system(R, "sphere", s, 20)
     print("fixtures written to", HERE)
 

@@ -148,7 +148,7 @@ def test_polyhedron_hull_engine_vs_oracle(oracle):
 
 
 def test_scene_generators_are_seeded():
-    a, b = scenes.config2(n=2000), scenes.config2(n=2000)
+    a, b = scenes.polydisperse_superquadrics(n=2000), scenes.polydisperse_superquadrics(n=2000)
     assert np.array_equal(a.transforms, b.transforms) and np.array_equal(a.rbs, b.rbs)
-    c = scenes.config2(n=2000, seed=5)
+    c = scenes.polydisperse_superquadrics(n=2000, seed=5)
     assert not np.array_equal(a.transforms, c.transforms)

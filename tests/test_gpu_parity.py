@@ -31,17 +31,17 @@ def hull_centroid(v):
 
 def make_scene(kind):
     if kind == "superquadric":
-        return scenes.config0(n=1500, pitch=2.05e-3)
+        return scenes.superquadric_column(n=1500, pitch=2.05e-3)
     if kind == "sphere":
-        return scenes.config0(n=1500, pitch=2.05e-3, shape="sphere")
+        return scenes.superquadric_column(n=1500, pitch=2.05e-3, shape="sphere")
     if kind == "box-on-walls":
         # boxes touch each other only through the walls in the reference: its
         # OBB pre-filter is the exact box, so box-box pairs never reach a contact
-        s = scenes.config0(n=1500, pitch=2.05e-3, shape="box", tilt=0.3)
+        s = scenes.superquadric_column(n=1500, pitch=2.05e-3, shape="box", tilt=0.3)
         s.transforms[:, 9:] -= 1.6e-3 - 0.79e-3
         return s
     if kind == "polyhedron":
-        return scenes.config1(n=1200, box=(0.030, 0.030, 0.030), pitch=1.9e-3,
+        return scenes.polyhedra_box(n=1200, box=(0.030, 0.030, 0.030), pitch=1.9e-3,
                               hull_centroid=hull_centroid)
     raise ValueError(kind)
 

@@ -97,7 +97,7 @@ def test_hooke_vs_golden(oracle):
 @pytest.mark.parametrize("name,shape", [("superquadric", "superquadric"), ("sphere", "sphere")])
 def test_system_vs_golden(oracle, name, shape):
     g = load("system_" + name)
-    scene = scenes.config0(n=400, pitch=2.05e-3, box=(0.012, 0.012, 0.036), shape=shape)
+    scene = scenes.superquadric_column(n=400, pitch=2.05e-3, box=(0.012, 0.012, 0.036), shape=shape)
     s = scenes.System(oracle, scene)
     p = abi.RigidBodyProps()
     v = g["props"][0]
@@ -151,7 +151,7 @@ def test_functions_bit_exact_vs_reference(oracle, reference):
 
 
 def test_system_bit_exact_vs_reference(oracle, reference):
-    scene = scenes.config0(n=600, pitch=2.05e-3, box=(0.014, 0.014, 0.040))
+    scene = scenes.superquadric_column(n=600, pitch=2.05e-3, box=(0.014, 0.014, 0.040))
     o = scenes.System(oracle, scene)
     r = scenes.System(reference, scene)
     p = r.rb_props(0)

@@ -24,7 +24,7 @@ def _rank(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=__import__("datetime").timedelta(seconds=60))
-    scene = scenes.config2(seed=bench.replica_seed(rank), n=3000)
+    scene = scenes.polydisperse_superquadrics(seed=bench.replica_seed(rank), n=3000)
     s = scenes.System(pyoracle.load_oracle(), scene)
     t0 = time.perf_counter()
     s.step(2)

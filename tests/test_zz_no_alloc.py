@@ -30,7 +30,7 @@ def static_sort_fn():
 def test_static_sort_matches_update_links(gb):
     import torch
     fn = static_sort_fn()
-    scene = scenes.config0(n=1500, pitch=2.05e-3)
+    scene = scenes.superquadric_column(n=1500, pitch=2.05e-3)
     s = scenes.System(gb, scene, precision=abi.GB_FP64)
     assert gb.update_links(s.ctx) == abi.GB_OK
     ref_ids = s.dump(abi.GB_DUMP_SORTED_IDS)
