@@ -112,6 +112,7 @@ SYSTEM_API = {
     "get_transforms": (C.c_int, [_P, _D]),
     "get_velocities": (C.c_int, [_P, _D]),
     "get_torces": (C.c_int, [_P, _D]),
+    "set_torces": (C.c_int, [_P, _D]),
     "update_links": (C.c_int, [_P]),
     "detect_collision_and_compute_contact_forces": (C.c_int, [_P, _I32]),
     "add_external_forces": (C.c_int, [_P]),

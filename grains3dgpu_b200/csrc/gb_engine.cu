@@ -647,6 +647,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     sp.law_kind   = c->cfg.contact_law;
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
+    sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
     launch_particles<S>(c, st, tb, po, sp, c->d_contacts);
     GB_CK(cudaGetLastError());
     mark(c, 7);
@@ -689,6 +690,7 @@ int run_particles(gb_ctx* c, int phases)
     sp.law_kind   = c->cfg.contact_law;
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
+    sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
     PairOut<St> po = pair_out<S>(c);
     launch_particles<S>(c, state_of<St>(c), tables_of<S>(c), po, sp, nullptr);
     GB_CK(cudaGetLastError());
@@ -1127,6 +1129,15 @@ int gb_get_torces(gb_ctx* c, double* torce)
     return get_soa6(c, torce, c->d_frc, c->d_trq);
 }
 
+int gb_set_torces(gb_ctx* c, const double* torce)
+{
+    if(!c || !torce)
+        return GB_E_INVALID_ARG;
+    GB_TRY(set_soa6(c, torce, c->d_frc, c->d_trq));
+    c->torce_dirty = true;
+    return GB_OK;
+}
+
 int gb_get_transforms(gb_ctx* c, double* t)
 {
     if(!c || !t)
@@ -1187,19 +1198,14 @@ int gb_step(gb_ctx* c, int32_t n_steps)
     GB_TRY(ready(c));
     if(n_steps < 0)
         return GB_E_INVALID_ARG;
-    if(c->torce_dirty)
-    {
-        const size_t ss = store_size(c->prec);
-        GB_CK(cudaMemsetAsync(c->d_frc, 0, 3 * (size_t)c->n * ss, c->stream));
-        GB_CK(cudaMemsetAsync(c->d_trq, 0, 3 * (size_t)c->n * ss, c->stream));
-        c->torce_dirty = false;
-    }
     GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
     int worst = GB_OK;
     for(int32_t s = 0; s < n_steps; ++s)
     {
+        // the first step adds to a torce left by separate calls, then resets it
         GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, PHASE_STEP, nullptr); }));
         c->links_valid = false;
+        c->torce_dirty = false;
     }
     int st = finish(c);
     if(st != GB_OK)

@@ -475,6 +475,7 @@ struct StepParams
     int      law_kind;
     int      has_kr;
     int      phases;
+    int      accumulate; // PHASE_DETECT adds to the stored torce instead of to zero
 };
 
 template <typename S, bool GEN>
@@ -610,8 +611,18 @@ __global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
     int                       nc = 0, nwall = 0, iters = 0;
     if(sp.phases & PHASE_DETECT)
     {
-        F = zero3<S>();
-        T = zero3<S>();
+        // Torce::addForce onto the torce accumulated since the last move
+        // (zero unless set_torces, add_external_forces or a detect came first)
+        if(sp.accumulate)
+        {
+            F = load3<S>(st.frc, i);
+            T = load3<S>(st.trq, i);
+        }
+        else
+        {
+            F = zero3<S>();
+            T = zero3<S>();
+        }
         for(uint32_t p = off[i]; p < off[i + 1]; ++p)
         {
             if(!po.contact[p])
@@ -720,7 +731,7 @@ __global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
         st.omg[0][i] = (store_t<S>)to_d(w.x);
         st.omg[1][i] = (store_t<S>)to_d(w.y);
         st.omg[2][i] = (store_t<S>)to_d(w.z);
-        if(sp.phases != PHASE_STEP)
+        if(sp.phases != PHASE_STEP || sp.accumulate)
         {
             // Torce::reset
 #pragma unroll

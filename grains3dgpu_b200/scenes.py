@@ -386,6 +386,10 @@ class System:
         self._check(self.lib.get_torces(self.ctx, abi.dptr(out)), "get_torces")
         return out
 
+    def set_torces(self, t):
+        self._check(self.lib.set_torces(self.ctx, abi.dptr(np.ascontiguousarray(t, np.float64))),
+                    "set_torces")
+
     def rb_props(self, i):
         p = abi.RigidBodyProps()
         self._check(self.lib.get_rigid_body_props(self.ctx, i, abi.C.byref(p)), "get_rigid_body_props")

@@ -205,6 +205,10 @@ int gb_get_transforms(gb_ctx* ctx, double* transforms);
 int gb_get_velocities(gb_ctx* ctx, double* kin);
 /* Torce per particle: force(3) torque(3), accumulated since the last move. */
 int gb_get_torces(gb_ctx* ctx, double* torce);
+/* ComponentManager::setTorce (ComponentManager.hh:93): replaces the
+ * accumulated torces; the next detect and add_external_forces add to them and
+ * the next move consumes and resets them, as in ComponentManagerCPU. */
+int gb_set_torces(gb_ctx* ctx, const double* torce);
 
 /* ---- the time step: the ComponentManager hot-path calls ---------------------- */
 /* ComponentManager::updateLinks (ComponentManagerCPU.cpp:278-296). */

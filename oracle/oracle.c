@@ -1705,6 +1705,15 @@ int or_get_torces(or_ctx* c, double* t)
     return GB_OK;
 }
 
+/* ComponentManagerCPU::setTorce (ComponentManagerCPU.cpp, m_torce = t). */
+int or_set_torces(or_ctx* c, const double* t)
+{
+    if(!c || !t)
+        return GB_E_INVALID_ARG;
+    memcpy(c->torce, t, (size_t)c->n * 6 * sizeof(double));
+    return GB_OK;
+}
+
 int or_update_links(or_ctx* c)
 {
     /* ComponentManagerCPU::updateLinks (ComponentManagerCPU.cpp:278-296): cell

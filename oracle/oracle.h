@@ -79,6 +79,7 @@ int or_set_velocities(or_ctx* ctx, const double* kin);
 int or_get_transforms(or_ctx* ctx, double* transforms);
 int or_get_velocities(or_ctx* ctx, double* kin);
 int or_get_torces(or_ctx* ctx, double* torce);
+int or_set_torces(or_ctx* ctx, const double* torce);
 int or_update_links(or_ctx* ctx);
 int or_detect_collision_and_compute_contact_forces(or_ctx* ctx, int32_t* result);
 int or_add_external_forces(or_ctx* ctx);

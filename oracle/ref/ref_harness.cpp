@@ -444,6 +444,16 @@ int ref_get_torces(ref_ctx* c, double* t)
     return GB_OK;
 }
 
+int ref_set_torces(ref_ctx* c, const double* t)
+{
+    std::vector<Torce<T>> v(c->cfg.n_particles);
+    for(size_t i = 0; i < v.size(); ++i)
+        v[i] = Torce<T>(Vector3<T>(t[6 * i + 3], t[6 * i + 4], t[6 * i + 5]),
+                        Vector3<T>(t[6 * i], t[6 * i + 1], t[6 * i + 2]));
+    c->cm->setTorce(v);
+    return GB_OK;
+}
+
 int ref_update_links(ref_ctx* c)
 {
     LinkedCell<T>* lcp = c->lc;

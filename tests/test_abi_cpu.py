@@ -78,6 +78,20 @@ def test_create_without_device_fails_cleanly():
     assert not ctx and st.value == abi.GB_E_NO_DEVICE
 
 
+def test_component_manager_adapter_fails_cleanly_without_device():
+    """ComponentManagerB200 (C++ adapter over the C ABI) turns the engine's
+    status into an exception, which the drop-in driver reports as JSON."""
+    import json
+    import torch
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "oracle", "_ref", "adapter_drive")
+    if torch.cuda.is_available() or not os.path.exists(exe):
+        pytest.skip("needs the built driver and no GPU")
+    out = subprocess.run([exe, "1"], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 2
+    assert "no usable CUDA device" in json.loads(out.stdout.strip())["error"]
+
+
 def test_invalid_config_is_rejected():
     lib = engine.load()
     st = C.c_int32(0)

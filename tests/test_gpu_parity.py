@@ -102,6 +102,36 @@ def test_trajectory_fp64(gb, oracle, precision):
     assert rel_err(g.velocities(), o.velocities()) < 1e-7
 
 
+@pytest.mark.parametrize("precision", [abi.GB_FP64_STRICT, abi.GB_MIXED])
+def test_torce_accumulation(gb, oracle, precision):
+    """set_torces, two detects and gravity add onto one torce; the move (and
+    a fused step after separate calls) consumes and resets it."""
+    scene = make_scene("sphere")
+    g, o = pair(gb, oracle, scene, precision=precision)
+    t0 = np.random.default_rng(3).normal(size=(scene.n, 6)) * 1e-4
+    for s in (g, o):
+        s.set_torces(t0)
+        s.detect()
+        s.detect()
+        s.add_external_forces()
+    if precision == abi.GB_FP64_STRICT:
+        assert np.array_equal(g.torces(), o.torces())
+    else:
+        assert np.abs(g.torces() - o.torces()).max() <= 1e-5 * np.abs(o.torces()).max()
+    for s in (g, o):
+        s.set_torces(t0)
+        s.step(2)
+    assert not g.torces().any()
+    d = np.abs(g.transforms() - o.transforms())
+    if precision == abi.GB_FP64_STRICT:
+        assert d.max() < 1e-12
+        assert rel_err(g.velocities(), o.velocities()) < 1e-12
+    else:
+        # FP32 quaternion: basis entries to ~1e-7, FP64 centres
+        assert d[:, 9:].max() < 1e-9 and d[:, :9].max() < 1e-6
+        assert rel_err(g.velocities(), o.velocities()) < 1e-4
+
+
 def test_separate_calls_equal_fused_step(gb):
     scene = make_scene("superquadric")
     a = scenes.System(gb, scene, precision=abi.GB_FP64_STRICT)

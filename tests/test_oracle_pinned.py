@@ -163,6 +163,29 @@ def test_system_bit_exact_vs_reference(oracle, reference):
     assert np.array_equal(o.velocities(), r.velocities())
 
 
+def test_torce_accumulation_vs_reference(oracle, reference):
+    """setTorce, two detects and gravity accumulate onto one torce, which the
+    move consumes (ComponentManagerCPU: addForce onto m_torce, reset in
+    moveParticles)."""
+    scene = scenes.superquadric_column(n=400, pitch=2.05e-3, box=(0.012, 0.012, 0.036),
+                                       shape="sphere")
+    o = scenes.System(oracle, scene)
+    r = scenes.System(reference, scene)
+    oracle.set_rigid_body_props(o.ctx, 0, C.byref(r.rb_props(0)))
+    t0 = np.random.default_rng(3).normal(size=(scene.n, 6)) * 1e-4
+    for s in (o, r):
+        s.set_torces(t0)
+        s.detect()
+        s.detect()
+        s.add_external_forces()
+    assert np.array_equal(o.torces(), r.torces())
+    for s in (o, r):
+        s.move()
+    assert np.array_equal(o.torces(), r.torces()) and not o.torces().any()
+    assert np.array_equal(o.transforms(), r.transforms())
+    assert np.array_equal(o.velocities(), r.velocities())
+
+
 def test_engine_host_properties_match_reference(reference):
     """The engine computes rigid-body properties on the host with the
     reference's formulas and std::beta: bit-identical."""
