@@ -150,23 +150,24 @@ def run_engine(args, scene, precision, steps, warmup, torch, rank, world, timing
 
 def e2e_engine(sysm, steps, torch):
     """Same step through the public C ABI with host buffers: every step copies
-    the state in from pinned host memory and reads it back."""
+    the state (transforms and velocities, Grains' host layout) in from pinned
+    host memory and reads it back into the same buffers."""
     n = sysm.n
+    lib, ctx = sysm.lib, sysm.ctx
     tr = torch.empty((n, 12), dtype=torch.float64, pin_memory=True).numpy()
     kin = torch.empty((n, 6), dtype=torch.float64, pin_memory=True).numpy()
     tr[:] = sysm.transforms()
     kin[:] = sysm.velocities()
+    ptr, pkin = abi.dptr(tr), abi.dptr(kin)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
     for _ in range(steps):
-        sysm.set_transforms(tr)
-        sysm.set_velocities(kin)
-        sysm.step(1)
-        tr[:] = sysm.transforms()
-        kin[:] = sysm.velocities()
+        assert lib.set_transforms(ctx, ptr) == 0 and lib.set_velocities(ctx, pkin) == 0
+        assert lib.step(ctx, 1) in (abi.GB_OK, abi.GB_E_OUT_OF_DOMAIN)
+        assert lib.get_transforms(ctx, ptr) == 0 and lib.get_velocities(ctx, pkin) == 0
     e1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -417,10 +418,10 @@ def main():
 
 # DRAM bytes (read + write) per particle of the dominant kernels, from one
 # ncu capture of this workload with 400,000 particles
-# (profiles/k_particles_k_pairs_superquadrics_400k.md); the traffic scales with the
-# particle count, so a full launch moves this many bytes per particle.
-TRAFFIC_PER_PARTICLE = {"particle": 95.96e6 / 400_000, "pair_count": 17.15e6 / 400_000,
-                        "pair_fill": 18.75e6 / 400_000}
+# (profiles/k_pair_count_k_particles_superquadrics_400k.md); the traffic scales
+# with the particle count, so a full launch moves this many bytes per particle.
+TRAFFIC_PER_PARTICLE = {"particle": (89.93e6 + 16.81e6) / 400_000,
+                        "pair_count": (23.55e6 + 0.0003e6) / 400_000}
 
 
 def traffic_bytes(phase, n):
