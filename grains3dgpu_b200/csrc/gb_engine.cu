@@ -121,7 +121,7 @@ struct gb_ctx
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
-    bool      obs_general = false; // some obstacle is not a Rectangle
+    uint32_t* d_obsmask = nullptr; // obstacle candidates per sorted particle
     size_t    part_cap = 0, hist_cap = 0;
 
     // pairs (double-buffered for the tangential history)
@@ -385,6 +385,7 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_spos, n));
     GB_TRY(dalloc(&c->d_spos32, n));
     GB_TRY(dalloc(&c->d_slot, (size_t)n * kPairSlots));
+    GB_TRY(dalloc(&c->d_obsmask, n));
     GB_TRY(dalloc(&c->d_count, n + 1));
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
@@ -519,7 +520,7 @@ int broad_phase(gb_ctx* c)
     k_gather_sorted<<<nb, kBlock, 0, s>>>(n, c->d_sids, c->d_pos, c->d_pos + n,
                                           c->d_pos + 2 * (size_t)n, c->d_rb_id, c->d_rcirc64,
                                           c->d_spos,
-                                          c->prec == GB_FP64_STRICT ? nullptr : c->d_spos32);
+                                          c->prec == GB_MIXED ? c->d_spos32 : nullptr);
     c->launches += 2;
     GB_CK(cudaGetLastError());
     mark(c, 3);
@@ -527,24 +528,23 @@ int broad_phase(gb_ctx* c)
     return GB_OK;
 }
 
-// candidate pairs: count -> scan -> (read total, grow) -> fill
+// candidate pairs (particles, then obstacles): count -> scan -> (read total,
+// grow) -> fill
+template <typename S>
 int build_pairs(gb_ctx* c)
 {
+    using St = store_t<S>;
     const int    n = c->n;
     const int    nb = std::max(1, blocks(n, kBlock));
     cudaStream_t s = c->stream;
-    const bool   strict = c->prec == GB_FP64_STRICT;
     if(c->cfg.contact_law == GB_LAW_HOOKE_HISTORY)
         c->cur ^= 1; // last step's pair list becomes the history
-    uint32_t* off = c->d_off[c->cur];
-    if(strict)
-        k_pair_count<true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, nullptr,
-                                                 c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
-                                                 c->d_count, c->d_slot);
-    else
-        k_pair_count<false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
-                                                  c->d_spos32, c->d_cstart, c->dims[0],
-                                                  c->dims[1], c->dims[2], c->d_count, c->d_slot);
+    uint32_t*       off    = c->d_off[c->cur];
+    const float4*   spos32 = c->prec == GB_MIXED ? c->d_spos32 : nullptr;
+    k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
+                                          c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                                          c->d_slot, c->d_obsmask, state_of<St>(c),
+                                          tables_of<S>(c));
     c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
@@ -554,16 +554,10 @@ int build_pairs(gb_ctx* c)
     accumulate_pending(c); // the previous step finished before this sync
     const int64_t total = c->h_pinned[0];
     GB_TRY(ensure_pairs(c, total));
-    if(strict)
-        k_pair_fill<true><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, nullptr,
-                                                c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
-                                                c->d_count, c->d_slot, off, c->d_pa,
-                                                c->d_pb[c->cur], c->cap, c->d_flags);
-    else
-        k_pair_fill<false><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos,
-                                                 c->d_spos32, c->d_cstart, c->dims[0], c->dims[1],
-                                                 c->dims[2], c->d_count, c->d_slot, off, c->d_pa,
-                                                 c->d_pb[c->cur], c->cap, c->d_flags);
+    k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
+                                         c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                                         c->d_slot, c->d_obsmask, c->nob, off, c->d_pa,
+                                         c->d_pb[c->cur], c->cap, c->d_flags);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 5);
@@ -594,20 +588,13 @@ PairOut<store_t<S>> pair_out(gb_ctx* c)
     return po;
 }
 
-// k_particles without the general-obstacle GJK unless some obstacle needs it
 template <typename S>
 void launch_particles(gb_ctx* c, const State<store_t<S>>& st, const Tables<S>& tb,
                       const PairOut<store_t<S>>& po, const StepParams<S>& sp, int* contacts_out)
 {
     const int nb = std::max(1, blocks(c->n, kBlock));
-    if(c->obs_general)
-        k_particles<S, true><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po, sp,
-                                                            contacts_out, c->d_counters,
-                                                            c->d_counters + 1);
-    else
-        k_particles<S, false><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po,
-                                                             sp, contacts_out, c->d_counters,
-                                                             c->d_counters + 1);
+    k_particles<S><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po, sp,
+                                                 contacts_out);
     c->launches += 1;
 }
 
@@ -618,7 +605,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     cudaStream_t s = c->stream;
     c->in_step     = true;
     GB_TRY(broad_phase(c));
-    GB_TRY(build_pairs(c));
+    GB_TRY(build_pairs<S>(c));
     PairOut<St> po = pair_out<S>(c);
     const bool hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
     if(hist && !c->have_prev)
@@ -632,7 +619,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     {
         k_narrow<S><<<blocks(c->npairs, 128), 128, 0, s>>>(
             c->npairs, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law, c->has_kr ? 1 : 0,
-            S(c->cfg.dt), c->d_counters + 1);
+            S(c->cfg.dt), c->d_counters);
         c->launches += 1;
         GB_CK(cudaGetLastError());
     }
@@ -851,7 +838,7 @@ int gb_destroy(gb_ctx* c)
     void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
                     c->d_obs_mass, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
-                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_spos32, c->d_slot, c->d_count,
+                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_spos32, c->d_slot, c->d_obsmask, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts,
                     c->d_stage};
@@ -1000,9 +987,6 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
     if(!c || (c->nob && (!obst || !transforms)))
         return GB_E_INVALID_ARG;
     c->obs.assign(obst, obst + c->nob);
-    c->obs_general = false;
-    for(int i = 0; i < c->nob; ++i)
-        c->obs_general = c->obs_general || obst[i].convex.type != GB_RECTANGLE;
     c->obs_tr.assign(transforms, transforms + 12 * (size_t)c->nob);
     c->obs_props.resize(c->nob);
     for(int i = 0; i < c->nob; ++i)
@@ -1234,12 +1218,20 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
     o->gjk_iterations    = (int64_t)cnt[1];
     if(c->detect_valid && c->npairs > 0)
     {
-        std::vector<uint8_t> pc(c->npairs);
+        // particle pairs only: obstacle candidates share the list
+        std::vector<uint8_t>  pc(c->npairs);
+        std::vector<uint32_t> pb(c->npairs);
         GB_CK(cudaMemcpy(pc.data(), c->d_pc, c->npairs, cudaMemcpyDeviceToHost));
-        int64_t k = 0;
-        for(uint8_t b : pc)
-            k += b;
-        o->contacts = k;
+        GB_CK(cudaMemcpy(pb.data(), c->d_pb[c->cur], c->npairs * sizeof(uint32_t),
+                         cudaMemcpyDeviceToHost));
+        int64_t k = 0, obs = 0;
+        for(int64_t p = 0; p < c->npairs; ++p)
+        {
+            k += pc[p] == kContactParticle;
+            obs += (pb[p] & kObstacleBit) != 0;
+        }
+        o->contacts        = k;
+        o->candidate_pairs = c->npairs - obs;
     }
     o->status_flags = c->last.status_flags;
     o->n_cells      = (int32_t)c->ncells;
@@ -1336,6 +1328,8 @@ int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
             int64_t w = 0;
             for(int64_t p = 0; p < P; ++p)
             {
+                if(b[p] & kObstacleBit) // particle-obstacle records share the list
+                    continue;
                 if(kind != GB_DUMP_CANDIDATE_PAIRS && !pc[p])
                     continue;
                 if(kind == GB_DUMP_CONTACT_INFO)

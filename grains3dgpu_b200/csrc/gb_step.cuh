@@ -180,13 +180,89 @@ GB_D Law<S> load_law(const Law<store_t<S>>* t, int ma, int mb)
 // The three cells x-1, x, x+1 of one (y, z) row have consecutive keys, so
 // their particles are one contiguous range of the sorted order: the walk is
 // nine ranges, visiting the candidates in the same order as the 27 cells.
-// Outside STRICT a conservative FP32 test on spos32 (k_gather_sorted inflates
-// its radii by a bound on the FP32 rounding, so an FP32 rejection implies an
-// FP64 rejection) skips most non-candidates before the FP64 test: the
-// candidate set is the FP64 test's.
+// PRE32 (the mixed mode): a conservative FP32 test on spos32 (k_gather_sorted
+// inflates its radii by a bound on the FP32 rounding, so an FP32 rejection
+// implies an FP64 rejection) skips most non-candidates before the FP64 test:
+// the candidate set is the FP64 test's.  The FP64 modes test in FP64 only.
 constexpr int kPairSlots = 16; // candidates kept per particle by the count pass
 
-template <bool STRICT, typename Hit>
+// Particle-obstacle pairs (ComponentManagerCPU.cpp:301-351) share the pair
+// list: after the particle pairs of A come A's obstacle candidates in obstacle
+// order, as b = kObstacleBit | o, so that the segmented sum adds the obstacle
+// forces after the particle forces, in the reference's order.
+constexpr uint32_t kObstacleBit     = 0x80000000u;
+constexpr uint8_t  kContactParticle = 1; // contact flags of a pair record
+constexpr uint8_t  kContactObstacle = 2;
+constexpr int      kMaskObstacles   = 32; // obstacles beyond these are always candidates
+
+// Frame of obstacle o for particle A at xa: A's centre oA and the obstacle's
+// origin oO (relative to xa in the mixed mode, absolute in the FP64 modes).
+template <typename S>
+GB_D void obstacle_frame(const Tables<S>& tb, int o, const double xa[3], V3<S>& oA, V3<S>& oO,
+                         M3<S>& RO)
+{
+    const double* ot = tb.obs_tr + 12 * o;
+    if constexpr(is_mixed<S>())
+    {
+        oA = zero3<S>();
+        oO = mk<S>(S(ot[9] - xa[0]), S(ot[10] - xa[1]), S(ot[11] - xa[2]));
+    }
+    else
+    {
+        oA = mk<S>(S(xa[0]), S(xa[1]), S(xa[2]));
+        oO = mk<S>(S(ot[9]), S(ot[10]), S(ot[11]));
+    }
+#pragma unroll
+    for(int k = 0; k < 9; ++k)
+        RO.m[k] = S(ot[k]);
+}
+
+// Obstacles that particle a may touch, bit o for obstacle o < kMaskObstacles.
+// A lies in its bounding box (half extents bb), so its support point towards
+// a Rectangle's plane is at most bb . |RA^T n| from its centre: a centre
+// farther than that from the plane (plus a bound on the rounding of both
+// sides) cannot touch it, and the full test of closest_rectangle would reject
+// it too.  Other obstacle types are always candidates.
+template <typename S>
+GB_D uint32_t obstacle_mask(const State<store_t<S>>& st, const Tables<S>& tb, uint32_t a)
+{
+    if(tb.n_obs == 0)
+        return 0u;
+    const uint32_t r     = st.rb_id[a];
+    const V3<S>    bb    = mk<S>(S(tb.shape[r].bb[0]), S(tb.shape[r].bb[1]), S(tb.shape[r].bb[2]));
+    const M3<S>    RA    = load_rot<S>(st, a);
+    const double   xa[3] = {st.pos[0][a], st.pos[1][a], st.pos[2][a]};
+    uint32_t       mask  = 0u;
+    const int      nm    = tb.n_obs < kMaskObstacles ? tb.n_obs : kMaskObstacles;
+    for(int o = 0; o < nm; ++o)
+    {
+        bool cand = true;
+        if(tb.obs_shape[o].type == GB_RECTANGLE)
+        {
+            V3<S> oA, oO;
+            M3<S> RO;
+            obstacle_frame(tb, o, xa, oA, oO, RO);
+            const V3<S> rn  = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
+            const V3<S> nb  = mul_t(RA, rn);
+            const S     dc  = s_fabs(dot(rn, oA - oO));
+            const S     hb  = bb.x * s_fabs(nb.x) + bb.y * s_fabs(nb.y) + bb.z * s_fabs(nb.z);
+            const S     mag = s_fabs(oA.x) + s_fabs(oA.y) + s_fabs(oA.z) + s_fabs(oO.x)
+                          + s_fabs(oO.y) + s_fabs(oO.z) + hb;
+            const S slack = is_mixed<S>() ? S(1e-6) + S(1e-6) * mag : S(1e-12) * (S(1.0) + mag);
+            cand          = !(dc - hb > slack);
+        }
+        if(cand)
+            mask |= 1u << o;
+    }
+    return mask;
+}
+
+GB_D int obstacle_candidates(uint32_t mask, int n_obs)
+{
+    return __popc(mask) + (n_obs > kMaskObstacles ? n_obs - kMaskObstacles : 0);
+}
+
+template <bool STRICT, bool PRE32, typename Hit>
 GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
                              const double4* __restrict__ spos,
                              const float4* __restrict__ spos32,
@@ -196,7 +272,7 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
     const uint32_t key = skeys[s];
     const double4  pa  = spos[s];
     float4         pa32;
-    if constexpr(!STRICT)
+    if constexpr(PRE32)
         pa32 = spos32[s];
     const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
     const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < (int)nx ? cx + 1 : cx;
@@ -216,7 +292,7 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
             {
                 if(t == (uint32_t)s)
                     continue;
-                if constexpr(!STRICT)
+                if constexpr(PRE32)
                 {
                     const float4 q  = spos32[t];
                     const float  fx = q.x - pa32.x, fy = q.y - pa32.y, fz = q.z - pa32.z;
@@ -249,34 +325,51 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
 
 // Count pass: the number of candidates of each particle (by id) and the first
 // kPairSlots of them (sorted positions t, in enumeration order) in slot[s].
-template <bool STRICT>
+template <typename S>
+GB_D constexpr bool is_strict()
+{
+    return std::is_same<S, dstrict>::value;
+}
+
+// Count pass: per particle (by id) the number of candidates -- particles,
+// then obstacles -- with the first kPairSlots particle candidates (sorted
+// positions t, in enumeration order) in slot[s] and the obstacle mask in
+// obsmask[s].
+template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_count(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
-                 uint32_t* __restrict__ count, uint32_t* __restrict__ slot)
+                 uint32_t* __restrict__ count, uint32_t* __restrict__ slot,
+                 uint32_t* __restrict__ obsmask, State<store_t<S>> st, Tables<S> tb)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= n)
         return;
     uint32_t  c    = 0;
     uint32_t* mine = slot + (size_t)s * kPairSlots;
-    for_each_candidate<STRICT>(s, skeys, spos, spos32, cstart, nx, ny, nz, [&](uint32_t t) {
-        if(c < kPairSlots)
-            mine[c] = t;
-        ++c;
-    });
-    count[sids[s]] = c;
+    for_each_candidate<is_strict<S>(), is_mixed<S>()>(s, skeys, spos, spos32, cstart, nx, ny, nz,
+                                                      [&](uint32_t t) {
+                                                          if(c < kPairSlots)
+                                                              mine[c] = t;
+                                                          ++c;
+                                                      });
+    const uint32_t a    = sids[s];
+    const uint32_t mask = obstacle_mask<S>(st, tb, a);
+    obsmask[s]          = mask;
+    count[a]            = c + (uint32_t)obstacle_candidates(mask, tb.n_obs);
 }
 
-// Fill pass: the pair records of particle a at offset[a], copied from its
-// slots, or enumerated again when it had more than kPairSlots candidates.
-template <bool STRICT>
+// Fill pass: the pair records of particle a at offset[a] -- its particle
+// candidates copied from the slots (or enumerated again when there were more
+// than kPairSlots), then its obstacle candidates.
+template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_fill(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                 const double4* __restrict__ spos, const float4* __restrict__ spos32,
                 const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
                 const uint32_t* __restrict__ count, const uint32_t* __restrict__ slot,
+                const uint32_t* __restrict__ obsmask, int n_obs,
                 const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
 {
@@ -293,21 +386,32 @@ __global__ void __launch_bounds__(kBlock)
         atomicOr(flags, kFlagCapacity);
         return;
     }
-    if(c <= kPairSlots)
+    const uint32_t mask = obsmask[s];
+    const uint32_t cp   = c - (uint32_t)obstacle_candidates(mask, n_obs);
+    if(cp <= kPairSlots)
     {
         const uint32_t* mine = slot + (size_t)s * kPairSlots;
-        for(uint32_t k = 0; k < c; ++k)
+        for(uint32_t k = 0; k < cp; ++k)
         {
             pair_a[out + k] = a;
             pair_b[out + k] = sids[mine[k]];
         }
-        return;
+        out += cp;
     }
-    for_each_candidate<STRICT>(s, skeys, spos, spos32, cstart, nx, ny, nz, [&](uint32_t t) {
-        pair_a[out] = a;
-        pair_b[out] = sids[t];
-        ++out;
-    });
+    else
+        for_each_candidate<is_strict<S>(), is_mixed<S>()>(s, skeys, spos, spos32, cstart, nx, ny,
+                                                          nz, [&](uint32_t t) {
+                                                              pair_a[out] = a;
+                                                              pair_b[out] = sids[t];
+                                                              ++out;
+                                                          });
+    for(int o = 0; o < n_obs; ++o)
+        if(o >= kMaskObstacles || ((mask >> o) & 1u))
+        {
+            pair_a[out] = a;
+            pair_b[out] = kObstacleBit | (uint32_t)o;
+            ++out;
+        }
 }
 
 // ---- narrow phase + contact law, one thread per candidate pair ---------------
@@ -317,7 +421,7 @@ struct PairOut
     St*      f[3];
     St*      t[3];
     St*      m[3];     // rolling moment (only when some kr != 0)
-    uint8_t* contact;  // 1 when overlap < 0
+    uint8_t* contact;  // kContactParticle / kContactObstacle when overlap < 0, else 0
     double*  info;     // optional: 7 per pair (point, vector, overlap) in world frame
     // tangential history (history law): current step out, previous step in
     St*             xi[3];
@@ -326,17 +430,160 @@ struct PairOut
     const St*       prev_xi[3];
 };
 
+// the outputs of pair p: force, torque, rolling moment, spring, contact flag,
+// and (when recorded) the contact point in world frame, vector and overlap
+template <typename S>
+GB_D void store_pair(const PairOut<store_t<S>>& po, int64_t p, const Force<S>& F,
+                     const V3<S>& xi_new, uint8_t flag, int law_kind, int has_kr,
+                     const Contact<S>& ci, const double xa[3])
+{
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+        const S fk[3] = {F.f.x, F.f.y, F.f.z}, tk[3] = {F.t.x, F.t.y, F.t.z};
+        po.f[k][p] = (store_t<S>)to_d(fk[k]);
+        po.t[k][p] = (store_t<S>)to_d(tk[k]);
+    }
+    if(has_kr)
+    {
+        po.m[0][p] = (store_t<S>)to_d(F.m.x);
+        po.m[1][p] = (store_t<S>)to_d(F.m.y);
+        po.m[2][p] = (store_t<S>)to_d(F.m.z);
+    }
+    if(law_kind != GB_LAW_HOOKE)
+    {
+        po.xi[0][p] = (store_t<S>)to_d(xi_new.x);
+        po.xi[1][p] = (store_t<S>)to_d(xi_new.y);
+        po.xi[2][p] = (store_t<S>)to_d(xi_new.z);
+    }
+    po.contact[p] = flag;
+    if(po.info)
+    {
+        double* o = po.info + 7 * p;
+        if constexpr(is_mixed<S>())
+        {
+            o[0] = xa[0] + to_d(ci.pt.x);
+            o[1] = xa[1] + to_d(ci.pt.y);
+            o[2] = xa[2] + to_d(ci.pt.z);
+        }
+        else
+        {
+            o[0] = to_d(ci.pt.x);
+            o[1] = to_d(ci.pt.y);
+            o[2] = to_d(ci.pt.z);
+        }
+        o[3] = to_d(ci.vec.x);
+        o[4] = to_d(ci.vec.y);
+        o[5] = to_d(ci.vec.z);
+        o[6] = to_d(ci.overlap);
+    }
+}
+
+// Pair p of particle a with obstacle o: closestPointsRigidBodies against the
+// obstacle and the contact law with the obstacle at rest
+// (ComponentManagerCPU.cpp:301-351).  The history law starts a fresh spring
+// for obstacle contacts every step.  Kept out of line: it is rare and would
+// otherwise set the register count of the particle-pair path.
+template <typename S>
+__device__ __noinline__ void narrow_obstacle(int64_t p, uint32_t a, int o,
+                                             const State<store_t<S>>& st, const Tables<S>& tb,
+                                             const PairOut<store_t<S>>& po, int law_kind,
+                                             int has_kr, S dt, unsigned long long* counters)
+{
+    const uint32_t ra    = st.rb_id[a];
+    const Body<S>  A     = load_body<S>(tb.shape, ra, tb.verts);
+    const M3<S>    RA    = load_rot<S>(st, a);
+    const double   xa[3] = {st.pos[0][a], st.pos[1][a], st.pos[2][a]};
+    const double*  ot    = tb.obs_tr + 12 * o;
+    const Body<S>  O     = load_body<S>(tb.obs_shape, o, tb.verts);
+    V3<S>          oA, oO;
+    M3<S>          RO;
+    obstacle_frame(tb, o, xa, oA, oO, RO);
+    int        iters = 0;
+    Contact<S> ci    = no_contact<S>();
+    if constexpr(is_mixed<S>())
+    {
+        if(O.type == GB_RECTANGLE)
+        {
+            // FP32 first; a contact (or a near miss within the rounding
+            // margin) is recomputed in FP64 relative to the particle centre
+            const V3<S> rn  = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
+            const V3<S> rnA = s_copysign(S(1.0), dot(rn, oA - oO)) * rn;
+            const V3<S> pA  = mul(RA, support(A, mul_t(RA, -rnA)));
+            const S     sep = dot(rnA, pA - oO);
+            if(sep < S(1e-6))
+            {
+                const Body<double> A64  = load_body<double>(tb.shape64, ra, tb.verts64);
+                const M3<double>   RA64 = load_rot64(st, a);
+                const V3<double>   oO64 = mk<double>(ot[9] - xa[0], ot[10] - xa[1], ot[11] - xa[2]);
+                ci = to_f(closest_rectangle(A64, RA64, zero3<double>(), oO64,
+                                            mk<double>(ot[2], ot[5], ot[8])));
+            }
+        }
+        else
+            ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+    }
+    else if(O.type == GB_RECTANGLE)
+        ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
+    else
+        ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+    const bool hit = ci.overlap < S(0.0);
+    Force<S>   F;
+    F.f = F.t = F.m = zero3<S>();
+    if(hit)
+    {
+        const Law<S> L  = load_law<S>(tb.law, tb.shape[ra].material, tb.obs_shape[o].material);
+        const S      m1 = S(tb.inertia[ra].mass);
+        const S      m2 = S(tb.obs_mass[o]);
+        const V3<S>  vA = load3<S>(st.vel, a), wA = load3<S>(st.omg, a);
+        V3<S>        arm, ptw;
+        if constexpr(is_mixed<S>())
+        {
+            arm = ci.pt;
+            ptw = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)), S(xa[2] + to_d(ci.pt.z)));
+        }
+        else
+        {
+            arm = ci.pt - oA;
+            ptw = ci.pt;
+        }
+        if(law_kind == GB_LAW_HOOKE)
+        {
+            // obstacles have zero velocity (ComponentManagerCPU.cpp:330-340)
+            const V3<S> zero = zero3<S>();
+            const V3<S> rel  = (vA + cross(wA, ptw)) - (zero + cross(zero, ptw));
+            F                = hooke(L, ci, rel, wA - zero, m1, m2, arm);
+        }
+        else
+        {
+            V3<S> xi;
+            F = hooke_history(L, ci, vA + cross(wA, arm), m1, m2, dt, zero3<S>(), xi, arm);
+        }
+        atomicAdd(&counters[0], 1ull);
+    }
+    store_pair<S>(po, p, F, zero3<S>(), hit ? kContactObstacle : uint8_t(0), law_kind, has_kr, ci,
+                  xa);
+    if(iters)
+        atomicAdd(&counters[1], (unsigned long long)iters);
+}
+
 template <typename S>
 __global__ void __launch_bounds__(128)
     k_narrow(int64_t npairs, const uint32_t* __restrict__ pair_a,
              const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
              PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
-             unsigned long long* __restrict__ gjk_iters)
+             unsigned long long* __restrict__ counters)
 {
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if(p >= npairs)
         return;
     const uint32_t a = pair_a[p], b = pair_b[p];
+    if(b & kObstacleBit)
+    {
+        narrow_obstacle<S>(p, a, (int)(b & ~kObstacleBit), st, tb, po, law_kind, has_kr, dt,
+                           counters);
+        return;
+    }
     const uint32_t ra = st.rb_id[a], rb = st.rb_id[b];
     const Body<S>  A = load_body<S>(tb.shape, ra, tb.verts);
     const Body<S>  B = load_body<S>(tb.shape, rb, tb.verts);
@@ -405,48 +652,9 @@ __global__ void __launch_bounds__(128)
             F = hooke_history(L, ci, rel, m1, m2, dt, xi_prev, xi_new, arm);
         }
     }
-#pragma unroll
-    for(int k = 0; k < 3; ++k)
-    {
-        const S fk[3] = {F.f.x, F.f.y, F.f.z}, tk[3] = {F.t.x, F.t.y, F.t.z};
-        po.f[k][p] = (store_t<S>)to_d(fk[k]);
-        po.t[k][p] = (store_t<S>)to_d(tk[k]);
-    }
-    if(has_kr)
-    {
-        po.m[0][p] = (store_t<S>)to_d(F.m.x);
-        po.m[1][p] = (store_t<S>)to_d(F.m.y);
-        po.m[2][p] = (store_t<S>)to_d(F.m.z);
-    }
-    if(law_kind != GB_LAW_HOOKE)
-    {
-        po.xi[0][p] = (store_t<S>)to_d(xi_new.x);
-        po.xi[1][p] = (store_t<S>)to_d(xi_new.y);
-        po.xi[2][p] = (store_t<S>)to_d(xi_new.z);
-    }
-    po.contact[p] = hit ? 1 : 0;
-    if(po.info)
-    {
-        double* o = po.info + 7 * p;
-        if constexpr(is_mixed<S>())
-        {
-            o[0] = xa[0] + to_d(ci.pt.x);
-            o[1] = xa[1] + to_d(ci.pt.y);
-            o[2] = xa[2] + to_d(ci.pt.z);
-        }
-        else
-        {
-            o[0] = to_d(ci.pt.x);
-            o[1] = to_d(ci.pt.y);
-            o[2] = to_d(ci.pt.z);
-        }
-        o[3] = to_d(ci.vec.x);
-        o[4] = to_d(ci.vec.y);
-        o[5] = to_d(ci.vec.z);
-        o[6] = to_d(ci.overlap);
-    }
+    store_pair<S>(po, p, F, xi_new, hit ? kContactParticle : uint8_t(0), law_kind, has_kr, ci, xa);
     if(iters)
-        atomicAdd(gjk_iters, (unsigned long long)iters);
+        atomicAdd(&counters[1], (unsigned long long)iters);
 }
 
 // ---- per-particle kernel -------------------------------------------------------
@@ -478,127 +686,13 @@ struct StepParams
     int      accumulate; // PHASE_DETECT adds to the stored torce instead of to zero
 };
 
-template <typename S, bool GEN>
-GB_D void wall_contacts(const Tables<S>& tb, const Body<S>& A, const M3<S>& RA,
-                        const double xa[3], const V3<S>& vA, const V3<S>& wA, S m1, int matA,
-                        const StepParams<S>& sp, V3<S>& F, V3<S>& T, int& nwall, int& iters,
-                        uint32_t rbA, const Quat<double>& q64)
-{
-    for(int o = 0; o < tb.n_obs; ++o)
-    {
-        const double*  ot = tb.obs_tr + 12 * o;
-        const Body<S>  O  = load_body<S>(tb.obs_shape, o, tb.verts);
-        V3<S>          oA, oO;
-        if constexpr(is_mixed<S>())
-        {
-            oA = zero3<S>();
-            oO = mk<S>(S(ot[9] - xa[0]), S(ot[10] - xa[1]), S(ot[11] - xa[2]));
-        }
-        else
-        {
-            oA = mk<S>(S(xa[0]), S(xa[1]), S(xa[2]));
-            oO = mk<S>(S(ot[9]), S(ot[10]), S(ot[11]));
-        }
-        M3<S> RO;
-#pragma unroll
-        for(int k = 0; k < 9; ++k)
-            RO.m[k] = S(ot[k]);
-        Contact<S> ci;
-        if(O.type == GB_RECTANGLE)
-        {
-            // A lies in its bounding box (half extents A.bb), so its support
-            // point towards the plane is at most bb . |RA^T n| from its centre:
-            // a centre farther than that from the plane (plus a bound on the
-            // rounding of both sides) has no contact with it, and the support
-            // evaluation is skipped.  The same wall is rejected by the full
-            // computation, so the contact set is unchanged.
-            const V3<S> rn  = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
-            const V3<S> nb  = mul_t(RA, rn);
-            const S     dc  = s_fabs(dot(rn, oA - oO));
-            const S     hb  = A.bb.x * s_fabs(nb.x) + A.bb.y * s_fabs(nb.y) + A.bb.z * s_fabs(nb.z);
-            const S     mag = s_fabs(oA.x) + s_fabs(oA.y) + s_fabs(oA.z) + s_fabs(oO.x)
-                          + s_fabs(oO.y) + s_fabs(oO.z) + hb;
-            const S slack = is_mixed<S>() ? S(1e-6) + S(1e-6) * mag : S(1e-12) * (S(1.0) + mag);
-            if(dc - hb > slack)
-                continue;
-        }
-        if constexpr(is_mixed<S>())
-        {
-            // FP32 first; a contact (or a near miss within the rounding
-            // margin) is recomputed in FP64 relative to the particle centre
-            const V3<S> rn = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
-            if(O.type == GB_RECTANGLE)
-            {
-                const V3<S> rnA = s_copysign(S(1.0), dot(rn, oA - oO)) * rn;
-                const V3<S> pA  = mul(RA, support(A, mul_t(RA, -rnA)));
-                const S     sep = dot(rnA, pA - oO);
-                if(!(sep < S(1e-6)))
-                    continue;
-                const Body<double> A64 = load_body<double>(tb.shape64, rbA, tb.verts64);
-                const M3<double>   RA64 = quat_to_matrix<double>(q64.w, q64.v.x, q64.v.y, q64.v.z);
-                const V3<double>   oO64 = mk<double>(ot[9] - xa[0], ot[10] - xa[1], ot[11] - xa[2]);
-                ci = to_f(closest_rectangle(A64, RA64, zero3<double>(), oO64,
-                                            mk<double>(ot[2], ot[5], ot[8])));
-            }
-            else if constexpr(GEN)
-                ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
-            else
-                ci = no_contact<S>();
-        }
-        else if(O.type == GB_RECTANGLE)
-            ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
-        else if constexpr(GEN)
-            ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
-        else
-            ci = no_contact<S>();
-        if(!(ci.overlap < S(0.0)))
-            continue;
-        ++nwall;
-        const Law<S> L  = load_law<S>(tb.law, matA, tb.obs_shape[o].material);
-        const S      m2 = S(tb.obs_mass[o]);
-        V3<S>        arm, ptw;
-        if constexpr(is_mixed<S>())
-        {
-            arm = ci.pt;
-            ptw = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)), S(xa[2] + to_d(ci.pt.z)));
-        }
-        else
-        {
-            arm = ci.pt - oA;
-            ptw = ci.pt;
-        }
-        Force<S> f;
-        if(sp.law_kind == GB_LAW_HOOKE)
-        {
-            // obstacles have zero velocity (ComponentManagerCPU.cpp:330-340)
-            const V3<S> zero = zero3<S>();
-            const V3<S> rel  = (vA + cross(wA, ptw)) - (zero + cross(zero, ptw));
-            f                = hooke(L, ci, rel, wA - zero, m1, m2, arm);
-        }
-        else
-        {
-            V3<S> xi;
-            f = hooke_history(L, ci, vA + cross(wA, arm), m1, m2, sp.dt, zero3<S>(), xi, arm);
-        }
-        F = F + f.f;
-        T = T + f.t;
-        if(sp.has_kr)
-            T = T + f.m;
-    }
-}
-
-// GEN: some obstacle is not a Rectangle and needs the full GJK.  Without it
-// the rare FP64 wall recomputation alone sets the register count; the launch
-// bound keeps GB_PARTICLES_MIN_BLOCKS 256-thread blocks resident per SM and
-// lets the rare paths spill instead.
-#ifndef GB_PARTICLES_MIN_BLOCKS
-#define GB_PARTICLES_MIN_BLOCKS 3
-#endif
-template <typename S, bool GEN>
-__global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
+// ---- per-particle kernel: segmented sum, gravity, integration -----------------
+// A streaming kernel: four 256-thread blocks per SM keep enough loads in
+// flight (the mixed instantiation fits 64 registers without spilling).
+template <typename S>
+__global__ void __launch_bounds__(kBlock, 4)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
-                PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
-                unsigned long long* __restrict__ counters, unsigned long long* __restrict__ gjk_iters)
+                PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n)
@@ -608,7 +702,7 @@ __global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
     const S                   m   = S(in->mass);
     V3<S>                     F, T;
     V3<S>                     v = load3<S>(st.vel, i), w = load3<S>(st.omg, i);
-    int                       nc = 0, nwall = 0, iters = 0;
+    int                       nc = 0;
     if(sp.phases & PHASE_DETECT)
     {
         // Torce::addForce onto the torce accumulated since the last move
@@ -623,30 +717,17 @@ __global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
             F = zero3<S>();
             T = zero3<S>();
         }
+        // the particle's pairs, then its obstacle pairs, in list order
         for(uint32_t p = off[i]; p < off[i + 1]; ++p)
         {
-            if(!po.contact[p])
+            const uint8_t hit = po.contact[p];
+            if(!hit)
                 continue;
-            ++nc;
+            nc += hit == kContactParticle;
             F = F + mk<S>(S(po.f[0][p]), S(po.f[1][p]), S(po.f[2][p]));
             T = T + mk<S>(S(po.t[0][p]), S(po.t[1][p]), S(po.t[2][p]));
             if(sp.has_kr)
                 T = T + mk<S>(S(po.m[0][p]), S(po.m[1][p]), S(po.m[2][p]));
-        }
-        if(tb.n_obs)
-        {
-            const Body<S> A     = load_body<S>(tb.shape, r, tb.verts);
-            const double  xa[3] = {st.pos[0][i], st.pos[1][i], st.pos[2][i]};
-            Quat<double>  q64;
-            q64.w = 1.0;
-            q64.v = zero3<double>();
-            if constexpr(is_mixed<S>())
-            {
-                q64.w = (double)st.rot[0][i];
-                q64.v = mk<double>((double)st.rot[1][i], (double)st.rot[2][i], (double)st.rot[3][i]);
-            }
-            wall_contacts<S, GEN>(tb, A, load_rot<S>(st, i), xa, v, w, m, tb.shape[r].material, sp, F, T,
-                          nwall, iters, r, q64);
         }
         if(contacts_out)
             contacts_out[i] = nc;
@@ -750,13 +831,6 @@ __global__ void __launch_bounds__(kBlock, GB_PARTICLES_MIN_BLOCKS)
         st.trq[0][i] = (store_t<S>)to_d(T.x);
         st.trq[1][i] = (store_t<S>)to_d(T.y);
         st.trq[2][i] = (store_t<S>)to_d(T.z);
-    }
-    if((sp.phases & PHASE_DETECT) && (nwall || iters))
-    {
-        if(nwall)
-            atomicAdd(&counters[0], (unsigned long long)nwall);
-        if(iters)
-            atomicAdd(gjk_iters, (unsigned long long)iters);
     }
 }
 
