@@ -19,6 +19,7 @@ constexpr int kWarps = kBlock / 32;
 constexpr int kFlagOutOfDomain = 1 << 5;
 constexpr int kFlagNonFinite   = 1 << 6;
 constexpr int kFlagCapacity    = 1 << 8;
+constexpr int kFlagCellCrowded = 1 << 9; // a cell too full for the counting sort's rank pass
 
 // ---- cell hash: LinkedCell::computeCellId / computeLinearCellHash
 //      (Grains/Component/src/LinkedCell.cpp:117-159): floor((p - min)/extent)
@@ -59,6 +60,133 @@ __global__ void k_hash(int n, const double* __restrict__ px, const double* __res
     ids[i]  = (uint32_t)i;
     if(bad)
         atomicOr(flags, bad);
+}
+
+// ---- counting sort by cell --------------------------------------------------
+// The sort the linked cell needs is by cell key with ascending particle id
+// inside a cell (the order in which ComponentManagerCPU::updateLinks appends
+// particles to its cell lists, ComponentManagerCPU.cpp:278-296).  With the
+// cell count as the number of buckets, the exclusive scan of the per-cell
+// counts is the cell-start table itself:
+//   k_hash_count:    key per particle and count[key] += 1 (atomics)
+//   scan:            cstart = exclusive scan of count (C + 1 entries)
+//   k_cell_scatter:  each particle into a free slot of its cell (any order)
+//   k_cell_rank:     each particle's rank among its cell's ids puts it in
+//                    ascending-id order, and writes the sorted key, id and
+//                    positions (the gather of the pair search) in one pass.
+// The rank pass costs O(m^2) per cell of m particles; cells of more than
+// kRankMaxCell particles flag kFlagCellCrowded and the caller sorts with the
+// radix kernels below instead.
+constexpr uint32_t kRankMaxCell = 512;
+
+__global__ void k_hash_count(int n, const double* __restrict__ px, const double* __restrict__ py,
+                             const double* __restrict__ pz, double mnx, double mny, double mnz,
+                             double cell, uint32_t nx, uint32_t ny, uint32_t nz,
+                             uint32_t* __restrict__ keys, uint32_t* __restrict__ count,
+                             int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const double   p[3]   = {px[i], py[i], pz[i]};
+    const double   mn[3]  = {mnx, mny, mnz};
+    const uint32_t dim[3] = {nx, ny, nz};
+    uint32_t       c[3];
+    int            bad = 0;
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+        const double f = floor(__ddiv_rn(__dsub_rn(p[k], mn[k]), cell));
+        if(!(f >= 0.0))
+        {
+            c[k] = 0;
+            bad |= (f != f) ? kFlagNonFinite : kFlagOutOfDomain;
+        }
+        else if(f >= (double)dim[k])
+        {
+            c[k] = dim[k] - 1;
+            bad |= kFlagOutOfDomain;
+        }
+        else
+            c[k] = (uint32_t)f;
+    }
+    const uint32_t key = (c[2] * ny + c[1]) * nx + c[0];
+    keys[i]            = key;
+    atomicAdd(&count[key], 1u);
+    if(bad)
+        atomicOr(flags, bad);
+}
+
+// count[] holds the per-cell counts again after the scan; each particle takes
+// one of its cell's slots by decrementing it
+__global__ void k_cell_scatter(int n, const uint32_t* __restrict__ keys,
+                               const uint32_t* __restrict__ cstart, uint32_t* __restrict__ count,
+                               uint32_t* __restrict__ unordered)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const uint32_t key  = keys[i];
+    const uint32_t slot = cstart[key] + atomicSub(&count[key], 1u) - 1u;
+    unordered[slot]     = (uint32_t)i;
+}
+
+// Particle e's entry at sorted position s: position and bounding radius
+// (double4) and, when out32 is given, an FP32 copy for a conservative
+// candidate pre-test: its radius is inflated by 2^-19 (|x| + |y| + |z| + r) =
+// 32 u (...), u = 2^-24, and rounded up.  The rounding of the FP32 coordinates,
+// of their difference and of the FP32 sum of squares (FMA or not) moves |d| by
+// less than 1.01 u (|xa|_1 + |xb|_1) + 1.74 u |d| + 2.1 u |d|, so an FP32 "no
+// overlap" (|d|^2 >= (wA + wB)^2) implies |d| >= (rA + rB)(1 + 26 u) in exact
+// arithmetic, which the FP64 test also rejects.
+__device__ __forceinline__ void put_sorted(uint32_t s, uint32_t e, const double* __restrict__ px,
+                                           const double* __restrict__ py,
+                                           const double* __restrict__ pz,
+                                           const uint32_t* __restrict__ rb_id,
+                                           const double* __restrict__ rcirc,
+                                           double4* __restrict__ out, float4* __restrict__ out32)
+{
+    const double4 p = make_double4(px[e], py[e], pz[e], rcirc[rb_id[e]]);
+    out[s]          = p;
+    if(out32)
+    {
+        const double slack = 0x1p-19 * (fabs(p.x) + fabs(p.y) + fabs(p.z) + p.w);
+        out32[s] = make_float4((float)p.x, (float)p.y, (float)p.z, __double2float_ru(p.w + slack));
+    }
+}
+
+// slot t of the unordered cell lists -> its place in ascending-id order, with
+// the sorted key and the sorted positions (put_sorted)
+__global__ void k_cell_rank(int n, const uint32_t* __restrict__ unordered,
+                            const uint32_t* __restrict__ keys, const uint32_t* __restrict__ cstart,
+                            uint32_t* __restrict__ skeys, uint32_t* __restrict__ sids,
+                            const double* __restrict__ px, const double* __restrict__ py,
+                            const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
+                            const double* __restrict__ rcirc, double4* __restrict__ out,
+                            float4* __restrict__ out32, int* __restrict__ flags)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= n)
+        return;
+    const uint32_t e   = unordered[t];
+    const uint32_t key = keys[e];
+    const uint32_t lo = cstart[key], hi = cstart[key + 1];
+    if(hi - lo > kRankMaxCell)
+    {
+        // keep a valid permutation (the caller redoes the sort)
+        skeys[t] = key;
+        sids[t]  = e;
+        put_sorted((uint32_t)t, e, px, py, pz, rb_id, rcirc, out, out32);
+        atomicOr(flags, kFlagCellCrowded);
+        return;
+    }
+    uint32_t rank = 0;
+    for(uint32_t u = lo; u < hi; ++u)
+        rank += unordered[u] < e;
+    const uint32_t s = lo + rank;
+    skeys[s]         = key;
+    sids[s]          = e;
+    put_sorted(s, e, px, py, pz, rb_id, rcirc, out, out32);
 }
 
 // ---- radix sort, pass 1: per-block digit histograms, digit-major layout
@@ -301,14 +429,8 @@ __global__ void __launch_bounds__(kBlock) k_cell_start(const uint32_t* __restric
     }
 }
 
-// positions and bounding radii in sorted order, for contiguous neighbour
-// reads.  out32 (optional) is an FP32 copy for a conservative candidate
-// pre-test: its radius is inflated by 2^-19 (|x| + |y| + |z| + r) = 32 u (...),
-// u = 2^-24, and rounded up.  The rounding of the FP32 coordinates, of their
-// difference and of the FP32 sum of squares (FMA or not) moves |d| by less
-// than 1.01 u (|xa|_1 + |xb|_1) + 1.74 u |d| + 2.1 u |d|, so an FP32 "no
-// overlap" (|d|^2 >= (wA + wB)^2) implies |d| >= (rA + rB)(1 + 26 u) in exact
-// arithmetic, which the FP64 test also rejects.
+// positions and bounding radii in sorted order (put_sorted), for contiguous
+// neighbour reads, after the radix sort
 __global__ void k_gather_sorted(int n, const uint32_t* __restrict__ sids,
                                 const double* __restrict__ px, const double* __restrict__ py,
                                 const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
@@ -318,14 +440,7 @@ __global__ void k_gather_sorted(int n, const uint32_t* __restrict__ sids,
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if(t >= n)
         return;
-    const uint32_t i = sids[t];
-    const double4  p = make_double4(px[i], py[i], pz[i], rcirc[rb_id[i]]);
-    out[t]           = p;
-    if(out32)
-    {
-        const double slack = 0x1p-19 * (fabs(p.x) + fabs(p.y) + fabs(p.z) + p.w);
-        out32[t] = make_float4((float)p.x, (float)p.y, (float)p.z, __double2float_ru(p.w + slack));
-    }
+    put_sorted((uint32_t)t, sids[t], px, py, pz, rb_id, rcirc, out, out32);
 }
 
 } // namespace gb

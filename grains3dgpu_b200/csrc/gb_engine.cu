@@ -118,6 +118,8 @@ struct gb_ctx
              *d_i[2] = {nullptr, nullptr};
     uint32_t *d_skeys = nullptr, *d_sids = nullptr; // results (alias into d_k/d_i)
     uint32_t *d_hist = nullptr, *d_part = nullptr, *d_cstart = nullptr;
+    uint32_t* d_ccount   = nullptr; // per-cell counts of the counting sort (C + 1)
+    bool      radix_sort = false;   // a crowded cell was seen: sort with the radix kernels
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
@@ -142,7 +144,7 @@ struct gb_ctx
     int*                d_flags = nullptr;
     unsigned long long* d_counters = nullptr; // [0] wall contacts [1] gjk iterations [2] contacts
     int*                d_contacts = nullptr;  // per-particle contact count of the last detect
-    uint32_t*           h_pinned = nullptr;    // pair total
+    uint32_t*           h_pinned = nullptr;    // [0] pair total [1] flags [2] flags to restore
     int64_t             steps_done = 0;
     bool                verlet_started = false;
     bool                links_valid = false, detect_valid = false;
@@ -464,7 +466,10 @@ int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* 
 
 // hash -> stable radix sort of (cell, id) -> cell-start table -> sorted
 // positions (ComponentManager::updateLinks)
-int broad_phase(gb_ctx* c)
+// Stable LSD radix sort of (cell key, id), then the cell-start search and the
+// gather of sorted positions: the fallback for cells too full for the
+// counting sort's rank pass.
+int broad_phase_radix(gb_ctx* c)
 {
     const int n = c->n;
     const int nb = std::max(1, blocks(n, kBlock));
@@ -528,6 +533,57 @@ int broad_phase(gb_ctx* c)
     return GB_OK;
 }
 
+// Counting sort by cell (gb_broadphase.cuh): the cell counts' scan is the
+// cell-start table and the rank pass writes the sorted positions.
+int broad_phase_counting(gb_ctx* c)
+{
+    const int    n  = c->n;
+    const int    nb = std::max(1, blocks(n, kBlock));
+    cudaStream_t s  = c->stream;
+    mark(c, 0);
+    GB_CK(cudaMemsetAsync(c->d_ccount, 0, ((size_t)c->ncells + 1) * sizeof(uint32_t), s));
+    k_hash_count<<<nb, kBlock, 0, s>>>(n, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
+                                       c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2],
+                                       c->cell, c->dims[0], c->dims[1], c->dims[2], c->d_hash,
+                                       c->d_ccount, c->d_flags);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    mark(c, 1);
+    GB_TRY(scan_u32(c, c->d_ccount, c->d_cstart, (int64_t)c->ncells + 1, nullptr));
+    k_cell_scatter<<<nb, kBlock, 0, s>>>(n, c->d_hash, c->d_cstart, c->d_ccount, c->d_i[0]);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    mark(c, 2);
+    c->d_skeys = c->d_k[1];
+    c->d_sids  = c->d_i[1];
+    k_cell_rank<<<nb, kBlock, 0, s>>>(n, c->d_i[0], c->d_hash, c->d_cstart, c->d_skeys, c->d_sids,
+                                      c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
+                                      c->d_rb_id, c->d_rcirc64, c->d_spos,
+                                      c->prec == GB_MIXED ? c->d_spos32 : nullptr, c->d_flags);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    mark(c, 3);
+    c->links_valid = true;
+    return GB_OK;
+}
+
+int broad_phase(gb_ctx* c)
+{
+    return c->radix_sort ? broad_phase_radix(c) : broad_phase_counting(c);
+}
+
+// after a kFlagCellCrowded report: clear that flag and redo the broad phase
+// with the radix sort (kept for the rest of the context's life)
+int redo_with_radix(gb_ctx* c)
+{
+    const int keep = (int)c->h_pinned[1] & ~kFlagCellCrowded;
+    std::memcpy(c->h_pinned + 2, &keep, sizeof(int));
+    GB_CK(cudaMemcpyAsync(c->d_flags, c->h_pinned + 2, sizeof(int), cudaMemcpyHostToDevice,
+                          c->stream));
+    c->radix_sort = true;
+    return broad_phase(c);
+}
+
 // candidate pairs (particles, then obstacles): count -> scan -> (read total,
 // grow) -> fill
 template <typename S>
@@ -541,17 +597,26 @@ int build_pairs(gb_ctx* c)
         c->cur ^= 1; // last step's pair list becomes the history
     uint32_t*       off    = c->d_off[c->cur];
     const float4*   spos32 = c->prec == GB_MIXED ? c->d_spos32 : nullptr;
-    k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
-                                          c->dims[0], c->dims[1], c->dims[2], c->d_count,
-                                          c->d_slot, c->d_obsmask, state_of<St>(c),
-                                          tables_of<S>(c));
-    c->launches += 1;
-    GB_CK(cudaGetLastError());
-    GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
-    mark(c, 4);
-    GB_CK(cudaMemcpyAsync(c->h_pinned, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    GB_CK(cudaStreamSynchronize(s));
-    accumulate_pending(c); // the previous step finished before this sync
+    for(;;)
+    {
+        k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32,
+                                              c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
+                                              c->d_count, c->d_slot, c->d_obsmask,
+                                              state_of<St>(c), tables_of<S>(c));
+        c->launches += 1;
+        GB_CK(cudaGetLastError());
+        GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
+        mark(c, 4);
+        GB_CK(cudaMemcpyAsync(c->h_pinned, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaMemcpyAsync(c->h_pinned + 1, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaStreamSynchronize(s));
+        accumulate_pending(c); // the previous step finished before this sync
+        if(!(c->h_pinned[1] & kFlagCellCrowded))
+            break;
+        // a cell too full for the counting sort: sort this context with the
+        // radix kernels from now on and redo the broad phase and the count
+        GB_TRY(redo_with_radix(c));
+    }
     const int64_t total = c->h_pinned[0];
     GB_TRY(ensure_pairs(c, total));
     k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
@@ -838,7 +903,7 @@ int gb_destroy(gb_ctx* c)
     void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
                     c->d_obs_mass, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
-                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_spos, c->d_spos32, c->d_slot, c->d_obsmask, c->d_count,
+                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_ccount, c->d_spos, c->d_spos32, c->d_slot, c->d_obsmask, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts,
                     c->d_stage};
@@ -939,6 +1004,8 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
         ++c->key_bits;
     dfree(c->d_cstart);
     GB_TRY(dalloc(&c->d_cstart, (size_t)nc + 1));
+    dfree(c->d_ccount);
+    GB_TRY(dalloc(&c->d_ccount, (size_t)nc + 1));
     if(c->d_shape64 && c->d_shape64 != c->d_shape)
     {
         cudaFree(c->d_shape64);
@@ -1148,6 +1215,14 @@ int gb_update_links(gb_ctx* c)
 {
     GB_TRY(ready(c));
     GB_TRY(broad_phase(c));
+    if(!c->radix_sort)
+    {
+        GB_CK(cudaMemcpyAsync(c->h_pinned + 1, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+        GB_CK(cudaStreamSynchronize(c->stream));
+        if(c->h_pinned[1] & kFlagCellCrowded)
+            GB_TRY(redo_with_radix(c));
+    }
     return finish(c);
 }
 

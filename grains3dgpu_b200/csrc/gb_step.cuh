@@ -688,9 +688,10 @@ struct StepParams
 
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
 // A streaming kernel: four 256-thread blocks per SM keep enough loads in
-// flight (the mixed instantiation fits 64 registers without spilling).
+// flight (the mixed instantiation fits 64 registers without spilling; the
+// FP64 ones need about 100 and get two blocks).
 template <typename S>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out)
 {

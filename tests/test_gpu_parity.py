@@ -102,6 +102,52 @@ def test_trajectory_fp64(gb, oracle, precision):
     assert rel_err(g.velocities(), o.velocities()) < 1e-7
 
 
+def crowded_cell_scene():
+    """One 5 mm sphere sets a 10 mm cell; 600 spheres of 0.13 mm radius on a
+    0.25 mm lattice all sit in the first cell, more than the counting sort's
+    rank pass takes, so the engine falls back to its radix sort."""
+    rng = np.random.default_rng(5)
+    n_small = 600
+    rbs = np.zeros(2, scenes.RB_DTYPE)
+    for k, r in enumerate((0.13e-3, 5e-3)):
+        rbs[k]["type"] = abi.GB_SPHERE
+        rbs[k]["p"][0] = r
+        rbs[k]["crust"] = 0.05 * r
+        rbs[k]["density"] = 2500.0
+    ix = np.arange(n_small)
+    pos = np.stack([1e-3 + (ix % 10) * 0.25e-3, 1e-3 + (ix // 10 % 10) * 0.25e-3,
+                    1e-3 + (ix // 100) * 0.25e-3], 1)
+    pos += rng.uniform(-2e-5, 2e-5, pos.shape)
+    pos = np.concatenate([pos, [[0.02, 0.02, 0.02]]])
+    n = n_small + 1
+    tr = np.zeros((n, 12))
+    tr[:, :9] = scenes.random_rotations(rng, n)
+    tr[:, 9:] = pos
+    box = (0.04, 0.04, 0.04)
+    walls, wtr = scenes.box_walls(box)
+    cfg = dict(n_particles=n, n_rigid_bodies=2, n_obstacles=6, n_materials=2, origin=(0, 0, 0),
+               max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
+    ids = np.zeros(n, np.uint32)
+    ids[-1] = 1
+    return scenes.Scene("crowded-cell", cfg, rbs, np.zeros((0, 3)), ids, tr, np.zeros((n, 6)),
+                        walls, wtr, [scenes.law()] * 3)
+
+
+@pytest.mark.parametrize("precision", [abi.GB_FP64_STRICT, abi.GB_MIXED])
+def test_crowded_cell_falls_back_to_radix_sort(gb, oracle, precision):
+    scene = crowded_cell_scene()
+    g, o = pair(gb, oracle, scene, precision=precision)
+    for s in (g, o):
+        s.detect()
+    assert np.diff(o.dump(abi.GB_DUMP_CELL_START)).max() > 512
+    for kind_ in BROAD_DUMPS + [abi.GB_DUMP_CONTACT_PAIRS]:
+        assert np.array_equal(g.dump(kind_), o.dump(kind_)), f"dump {kind_} differs"
+    assert g.stats().contacts == o.stats().contacts > 0
+    g.step(3)
+    o.step(3)
+    assert np.abs(g.transforms()[:, 9:] - o.transforms()[:, 9:]).max() < 1e-9
+
+
 @pytest.mark.parametrize("precision", [abi.GB_FP64_STRICT, abi.GB_MIXED])
 def test_torce_accumulation(gb, oracle, precision):
     """set_torces, two detects and gravity add onto one torce; the move (and
