@@ -20,6 +20,14 @@ constexpr int kFlagOutOfDomain = 1 << 5;
 constexpr int kFlagNonFinite   = 1 << 6;
 constexpr int kFlagCapacity    = 1 << 8;
 constexpr int kFlagCellCrowded = 1 << 9; // a cell too full for the counting sort's rank pass
+// Either one aborts the step: the kernels that write pair lists or state
+// return at entry once it is set, and the host replays the step.
+constexpr int kFlagAbort = kFlagCapacity | kFlagCellCrowded;
+
+__device__ __forceinline__ bool step_aborted(const int* flags)
+{
+    return flags && (*(volatile const int*)flags & kFlagAbort);
+}
 
 // ---- cell hash: LinkedCell::computeCellId / computeLinearCellHash
 //      (Grains/Component/src/LinkedCell.cpp:117-159): floor((p - min)/extent)
@@ -163,7 +171,8 @@ __global__ void k_cell_rank(int n, const uint32_t* __restrict__ unordered,
                             const double* __restrict__ px, const double* __restrict__ py,
                             const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
                             const double* __restrict__ rcirc, double4* __restrict__ out,
-                            float4* __restrict__ out32, int* __restrict__ flags)
+                            float4* __restrict__ out32, uint32_t* __restrict__ sorted_of,
+                            int* __restrict__ flags)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if(t >= n)
@@ -171,21 +180,19 @@ __global__ void k_cell_rank(int n, const uint32_t* __restrict__ unordered,
     const uint32_t e   = unordered[t];
     const uint32_t key = keys[e];
     const uint32_t lo = cstart[key], hi = cstart[key + 1];
+    uint32_t       s  = (uint32_t)t;
     if(hi - lo > kRankMaxCell)
+        atomicOr(flags, kFlagCellCrowded); // keep a valid permutation; the caller redoes the sort
+    else
     {
-        // keep a valid permutation (the caller redoes the sort)
-        skeys[t] = key;
-        sids[t]  = e;
-        put_sorted((uint32_t)t, e, px, py, pz, rb_id, rcirc, out, out32);
-        atomicOr(flags, kFlagCellCrowded);
-        return;
+        uint32_t rank = 0;
+        for(uint32_t u = lo; u < hi; ++u)
+            rank += unordered[u] < e;
+        s = lo + rank;
     }
-    uint32_t rank = 0;
-    for(uint32_t u = lo; u < hi; ++u)
-        rank += unordered[u] < e;
-    const uint32_t s = lo + rank;
-    skeys[s]         = key;
-    sids[s]          = e;
+    skeys[s]     = key;
+    sids[s]      = e;
+    sorted_of[e] = s;
     put_sorted(s, e, px, py, pz, rb_id, rcirc, out, out32);
 }
 
@@ -339,9 +346,14 @@ __global__ void __launch_bounds__(kBlock) k_scan_reduce(const uint32_t* __restri
 }
 
 // single block: exclusive scan of the per-tile partial sums, in chunks
+// abort_flags (optional): a scan whose output belongs to an aborted step
+// (step_aborted) leaves its output untouched
 __global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* __restrict__ partial, int m,
-                                                        uint32_t* __restrict__ grand_total)
+                                                        uint32_t* __restrict__ grand_total,
+                                                        const int* abort_flags = nullptr)
 {
+    if(step_aborted(abort_flags))
+        return;
     uint32_t carry = 0;
     for(int c = 0; c < m; c += 1024)
     {
@@ -359,8 +371,11 @@ __global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* __restrict__ p
 
 __global__ void __launch_bounds__(kBlock) k_scan_apply(const uint32_t* __restrict__ in,
                                                        uint32_t* __restrict__ out, int64_t n,
-                                                       const uint32_t* __restrict__ partial)
+                                                       const uint32_t* __restrict__ partial,
+                                                       const int* abort_flags = nullptr)
 {
+    if(step_aborted(abort_flags))
+        return;
     const int64_t base = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
     uint32_t      v[kItems];
     uint32_t      s = 0;
@@ -435,12 +450,14 @@ __global__ void k_gather_sorted(int n, const uint32_t* __restrict__ sids,
                                 const double* __restrict__ px, const double* __restrict__ py,
                                 const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
                                 const double* __restrict__ rcirc, double4* __restrict__ out,
-                                float4* __restrict__ out32)
+                                float4* __restrict__ out32, uint32_t* __restrict__ sorted_of)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if(t >= n)
         return;
-    put_sorted((uint32_t)t, sids[t], px, py, pz, rb_id, rcirc, out, out32);
+    const uint32_t e = sids[t];
+    sorted_of[e]     = (uint32_t)t;
+    put_sorted((uint32_t)t, e, px, py, pz, rb_id, rcirc, out, out32);
 }
 
 } // namespace gb

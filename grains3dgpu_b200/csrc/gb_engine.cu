@@ -96,6 +96,8 @@ struct gb_ctx
     void*    d_obs_shape = nullptr;
     double*  d_obs_tr = nullptr;
     double*  d_obs_mass = nullptr;
+    double4* d_obs_plane = nullptr; // Rectangle planes: normal, normal . origin
+    uint32_t obs_rect    = 0u;      // bit o: obstacle o (< 32) is a Rectangle
     double*  d_rcirc64 = nullptr;
     // FP64 shape tables: aliases of the above in the FP64 modes, separate
     // copies in the mixed mode (read by its FP64 polish)
@@ -123,7 +125,9 @@ struct gb_ctx
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
-    uint32_t* d_obsmask = nullptr; // obstacle candidates per sorted particle
+    uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
+    uint32_t* d_obsmask_id = nullptr; // the same per particle id, from the last move
+    bool      mask_valid   = false;   // d_obsmask_id matches the current poses
     size_t    part_cap = 0, hist_cap = 0;
 
     // pairs (double-buffered for the tangential history)
@@ -136,8 +140,10 @@ struct gb_ctx
     double*   d_info = nullptr;
     void*     d_xi[2] = {nullptr, nullptr}; // 3 * cap each
     int64_t   cap = 0;
+    int64_t   cap_hint = 0; // capacity the next step allocates up front (grows after an overflow)
     int       cur = 0;
-    int64_t   npairs = 0, prev_npairs = 0;
+    int64_t   npairs = 0; // of the last detect (read back after it)
+    int       sms    = 148; // multiprocessors of the context's device
     bool      have_prev = false;
 
     // counters and flags
@@ -153,9 +159,11 @@ struct gb_ctx
     cudaStream_t own_stream = nullptr; // the context's stream (gb_set_stream may replace it)
     // phase timing: two alternating event sets; a set is read once the next
     // step's host synchronisation has passed it
-    bool        timing = false, in_step = false;
-    cudaEvent_t ev[2][GB_N_PHASES + 1];
-    int         ev_set = 0, ev_pending = -1;
+    bool                 timing = false, in_step = false;
+    static constexpr int kEvRing = 16; // steps whose phase events are kept until a sync
+    cudaEvent_t          ev[kEvRing][GB_N_PHASES + 1];
+    int                  ev_next = 0, ev_npending = 0;
+    unsigned int*        d_done  = nullptr; // k_particles launches that completed (not aborted)
     double      phase_ms[GB_N_PHASES] = {0};
     int64_t     phase_steps = 0;
     int64_t     launches = 0;
@@ -170,24 +178,37 @@ namespace
 void mark(gb_ctx* c, int idx)
 {
     if(c->timing && c->in_step)
-        cudaEventRecord(c->ev[c->ev_set][idx], c->stream);
+        cudaEventRecord(c->ev[c->ev_next][idx], c->stream);
 }
 
-// adds the completed step's phase times (call only after a host sync that
-// follows that step's last event)
+// the current step's event set is complete: move to the next one
+void close_event_set(gb_ctx* c)
+{
+    if(!c->timing)
+        return;
+    c->ev_next = (c->ev_next + 1) % gb_ctx::kEvRing;
+    c->ev_npending++;
+}
+
+// adds the phase times of the steps recorded since the last call (at most
+// the last kEvRing of them; call only after a host sync that follows them)
 void accumulate_pending(gb_ctx* c)
 {
-    if(!c->timing || c->ev_pending < 0)
+    if(!c->timing || c->ev_npending == 0)
         return;
-    for(int k = 0; k < GB_N_PHASES; ++k)
+    const int m = std::min(c->ev_npending, gb_ctx::kEvRing);
+    for(int j = 0; j < m; ++j)
     {
-        float ms = 0.f;
-        if(cudaEventElapsedTime(&ms, c->ev[c->ev_pending][k], c->ev[c->ev_pending][k + 1])
-           == cudaSuccess)
-            c->phase_ms[k] += ms;
+        const int set = (c->ev_next - m + j + gb_ctx::kEvRing) % gb_ctx::kEvRing;
+        for(int k = 0; k < GB_N_PHASES; ++k)
+        {
+            float ms = 0.f;
+            if(cudaEventElapsedTime(&ms, c->ev[set][k], c->ev[set][k + 1]) == cudaSuccess)
+                c->phase_ms[k] += ms;
+        }
+        c->phase_steps++;
     }
-    c->phase_steps++;
-    c->ev_pending = -1;
+    c->ev_npending = 0;
 }
 
 size_t store_size(int prec)
@@ -231,6 +252,8 @@ Tables<S> tables_of(gb_ctx* c)
     t.obs_shape = (const RBShape<St>*)c->d_obs_shape;
     t.obs_tr      = c->d_obs_tr;
     t.obs_mass    = c->d_obs_mass;
+    t.obs_plane   = c->d_obs_plane;
+    t.obs_rect    = c->obs_rect;
     t.n_obs       = c->nob;
     t.shape64     = (const RBShape<double>*)c->d_shape64;
     t.verts64     = (const Vert<double>*)c->d_verts64;
@@ -353,6 +376,20 @@ int upload_obstacles(gb_ctx* c)
         GB_CK(cudaMemcpy(c->d_obs_tr, c->obs_tr.data(), c->obs_tr.size() * sizeof(double),
                          cudaMemcpyHostToDevice));
     GB_CK(cudaMemcpy(c->d_obs_mass, mass.data(), mass.size() * sizeof(double), cudaMemcpyHostToDevice));
+    // planes of the Rectangle obstacles (normal = the frame's z axis, n . origin)
+    std::vector<double4> plane(std::max(c->nob, 1), make_double4(0, 0, 0, 0));
+    c->obs_rect = 0u;
+    for(int i = 0; i < c->nob; ++i)
+    {
+        const double* t = c->obs_tr.data() + 12 * i;
+        plane[i]        = make_double4(t[2], t[5], t[8], t[2] * t[9] + t[5] * t[10] + t[8] * t[11]);
+        if(i < kMaskObstacles && c->obs[i].convex.type == GB_RECTANGLE)
+            c->obs_rect |= 1u << i;
+    }
+    dfree(c->d_obs_plane);
+    GB_TRY(dalloc(&c->d_obs_plane, plane.size()));
+    GB_CK(cudaMemcpy(c->d_obs_plane, plane.data(), plane.size() * sizeof(double4),
+                     cudaMemcpyHostToDevice));
     return GB_OK;
 }
 
@@ -387,7 +424,8 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_spos, n));
     GB_TRY(dalloc(&c->d_spos32, n));
     GB_TRY(dalloc(&c->d_slot, (size_t)n * kPairSlots));
-    GB_TRY(dalloc(&c->d_obsmask, n));
+    GB_TRY(dalloc(&c->d_sorted_of, n));
+    GB_TRY(dalloc(&c->d_obsmask_id, n));
     GB_TRY(dalloc(&c->d_count, n + 1));
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
@@ -396,6 +434,8 @@ int alloc_state(gb_ctx* c)
     GB_CK(cudaMemset(c->d_counters, 0, 4 * sizeof(unsigned long long)));
     GB_CK(cudaMemset(c->d_contacts, 0, std::max<size_t>(1, n) * sizeof(int)));
     GB_CK(cudaMallocHost((void**)&c->h_pinned, 4 * sizeof(uint32_t)));
+    GB_TRY(dalloc(&c->d_done, 1));
+    GB_CK(cudaMemset(c->d_done, 0, sizeof(unsigned int)));
     return GB_OK;
 }
 
@@ -403,7 +443,8 @@ int ensure_pairs(gb_ctx* c, int64_t need)
 {
     if(need <= c->cap)
         return GB_OK;
-    int64_t ncap = std::max<int64_t>(need + need / 2, 1024);
+    int64_t ncap = c->cap == 0 ? std::max<int64_t>(need, 1024)
+                               : std::max<int64_t>(need + need / 2, 1024);
     const size_t ss = store_size(c->prec);
     const bool   hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
     // the previous step's history buffers must survive the growth
@@ -415,16 +456,18 @@ int ensure_pairs(gb_ctx* c, int64_t need)
         if(hist)
             GB_CK(cudaMalloc(&nxi[b], 3 * ncap * ss));
     }
+    // (the previous step's pair count is on the device: copy the whole old
+    // capacity)
     const int prev = 1 - c->cur;
-    if(c->have_prev && c->prev_npairs > 0)
+    if(c->have_prev && c->cap > 0)
     {
-        GB_CK(cudaMemcpy(npb[prev], c->d_pb[prev], c->prev_npairs * sizeof(uint32_t),
+        GB_CK(cudaMemcpy(npb[prev], c->d_pb[prev], c->cap * sizeof(uint32_t),
                          cudaMemcpyDeviceToDevice));
         if(hist)
             for(int k = 0; k < 3; ++k)
                 GB_CK(cudaMemcpy((char*)nxi[prev] + k * ncap * ss,
-                                 (char*)c->d_xi[prev] + k * c->cap * ss,
-                                 c->prev_npairs * ss, cudaMemcpyDeviceToDevice));
+                                 (char*)c->d_xi[prev] + k * c->cap * ss, c->cap * ss,
+                                 cudaMemcpyDeviceToDevice));
     }
     for(int b = 0; b < 2; ++b)
     {
@@ -447,7 +490,10 @@ int ensure_pairs(gb_ctx* c, int64_t need)
 }
 
 // exclusive scan of n uint32 (in place allowed); *d_total (device) gets the sum
-int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total)
+// exclusive scan of n values; with abort_flags, an aborted step's scan writes
+// nothing
+int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total,
+             const int* abort_flags = nullptr)
 {
     const int nb = std::max(1, blocks(n, kTile));
     if((size_t)nb > c->part_cap)
@@ -457,8 +503,8 @@ int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* 
         c->part_cap = nb;
     }
     k_scan_reduce<<<nb, kBlock, 0, c->stream>>>(in, n, c->d_part);
-    k_scan_partials<<<1, 1024, 0, c->stream>>>(c->d_part, nb, d_total);
-    k_scan_apply<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_part);
+    k_scan_partials<<<1, 1024, 0, c->stream>>>(c->d_part, nb, d_total, abort_flags);
+    k_scan_apply<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_part, abort_flags);
     c->launches += 3;
     GB_CK(cudaGetLastError());
     return GB_OK;
@@ -525,7 +571,8 @@ int broad_phase_radix(gb_ctx* c)
     k_gather_sorted<<<nb, kBlock, 0, s>>>(n, c->d_sids, c->d_pos, c->d_pos + n,
                                           c->d_pos + 2 * (size_t)n, c->d_rb_id, c->d_rcirc64,
                                           c->d_spos,
-                                          c->prec == GB_MIXED ? c->d_spos32 : nullptr);
+                                          c->prec == GB_MIXED ? c->d_spos32 : nullptr,
+                                          c->d_sorted_of);
     c->launches += 2;
     GB_CK(cudaGetLastError());
     mark(c, 3);
@@ -559,7 +606,8 @@ int broad_phase_counting(gb_ctx* c)
     k_cell_rank<<<nb, kBlock, 0, s>>>(n, c->d_i[0], c->d_hash, c->d_cstart, c->d_skeys, c->d_sids,
                                       c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
                                       c->d_rb_id, c->d_rcirc64, c->d_spos,
-                                      c->prec == GB_MIXED ? c->d_spos32 : nullptr, c->d_flags);
+                                      c->prec == GB_MIXED ? c->d_spos32 : nullptr,
+                                      c->d_sorted_of, c->d_flags);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 3);
@@ -584,8 +632,9 @@ int redo_with_radix(gb_ctx* c)
     return broad_phase(c);
 }
 
-// candidate pairs (particles, then obstacles): count -> scan -> (read total,
-// grow) -> fill
+// candidate pairs (particles, then obstacles): count -> scan -> fill, with no
+// host round trip: the total stays on the device (off[n]); a total beyond the
+// capacity aborts the step (kFlagCapacity) and the host replays it larger
 template <typename S>
 int build_pairs(gb_ctx* c)
 {
@@ -595,38 +644,31 @@ int build_pairs(gb_ctx* c)
     cudaStream_t s = c->stream;
     if(c->cfg.contact_law == GB_LAW_HOOKE_HISTORY)
         c->cur ^= 1; // last step's pair list becomes the history
+    GB_TRY(ensure_pairs(c, c->cap_hint));
     uint32_t*       off    = c->d_off[c->cur];
     const float4*   spos32 = c->prec == GB_MIXED ? c->d_spos32 : nullptr;
-    for(;;)
+    if(c->nob && !c->mask_valid)
     {
-        k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32,
-                                              c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
-                                              c->d_count, c->d_slot, c->d_obsmask,
-                                              state_of<St>(c), tables_of<S>(c));
+        k_obstacle_mask<S><<<nb, kBlock, 0, s>>>(n, state_of<St>(c), tables_of<S>(c),
+                                                 c->d_obsmask_id);
         c->launches += 1;
         GB_CK(cudaGetLastError());
-        GB_TRY(scan_u32(c, c->d_count, off, n, off + n));
-        mark(c, 4);
-        GB_CK(cudaMemcpyAsync(c->h_pinned, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        GB_CK(cudaMemcpyAsync(c->h_pinned + 1, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s));
-        GB_CK(cudaStreamSynchronize(s));
-        accumulate_pending(c); // the previous step finished before this sync
-        if(!(c->h_pinned[1] & kFlagCellCrowded))
-            break;
-        // a cell too full for the counting sort: sort this context with the
-        // radix kernels from now on and redo the broad phase and the count
-        GB_TRY(redo_with_radix(c));
+        c->mask_valid = true;
     }
-    const int64_t total = c->h_pinned[0];
-    GB_TRY(ensure_pairs(c, total));
-    k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
-                                         c->dims[0], c->dims[1], c->dims[2], c->d_count,
-                                         c->d_slot, c->d_obsmask, c->nob, off, c->d_pa,
-                                         c->d_pb[c->cur], c->cap, c->d_flags);
+    k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
+                                          c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                                          c->d_slot, c->d_obsmask_id, c->nob);
+    c->launches += 1;
+    GB_CK(cudaGetLastError());
+    GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));
+    mark(c, 4);
+    k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_sorted_of, c->d_spos,
+                                         spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
+                                         c->d_count, c->d_slot, c->d_obsmask_id, c->nob, off,
+                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 5);
-    c->npairs = total;
     return GB_OK;
 }
 
@@ -657,14 +699,19 @@ template <typename S>
 void launch_particles(gb_ctx* c, const State<store_t<S>>& st, const Tables<S>& tb,
                       const PairOut<store_t<S>>& po, const StepParams<S>& sp, int* contacts_out)
 {
-    const int nb = std::max(1, blocks(c->n, kBlock));
+    const int  nb   = std::max(1, blocks(c->n, kBlock));
+    const bool move = (sp.phases & PHASE_MOVE) != 0;
     k_particles<S><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po, sp,
-                                                 contacts_out);
+                                                 contacts_out,
+                                                 move && c->nob ? c->d_obsmask_id : nullptr,
+                                                 c->d_flags, c->d_done);
     c->launches += 1;
+    if(move)
+        c->mask_valid = c->nob > 0;
 }
 
 template <typename S>
-int run_detect(gb_ctx* c, int phases, int32_t* result)
+int run_detect(gb_ctx* c, int phases)
 {
     using St = store_t<S>;
     cudaStream_t s = c->stream;
@@ -680,12 +727,30 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     }
     const State<St> st = state_of<St>(c);
     const Tables<S> tb = tables_of<S>(c);
-    if(c->npairs > 0)
     {
-        k_narrow<S><<<blocks(c->npairs, 128), 128, 0, s>>>(
-            c->npairs, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law, c->has_kr ? 1 : 0,
-            S(c->cfg.dt), c->d_counters);
+        // grid-stride over the device-side total (off[n]) with a grid of
+        // 8 blocks per SM (at most what the capacity needs)
+        const uint32_t* total = c->d_off[c->cur] + c->n;
+        const int       grid  = (int)std::max<int64_t>(
+            1, std::min<int64_t>(blocks(c->cap, 128), (int64_t)8 * c->sms));
+        const int kr = c->has_kr ? 1 : 0;
+        k_narrow<S><<<grid, 128, 0, s>>>(total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po,
+                                         c->cfg.contact_law, kr, S(c->cfg.dt), c->d_counters);
         c->launches += 1;
+        if(c->nob)
+        {
+            const bool all_rect = c->nob <= kMaskObstacles
+                                  && c->obs_rect == ((c->nob == 32) ? ~0u : ((1u << c->nob) - 1u));
+            if(all_rect)
+                k_narrow_obstacles<S, false><<<grid, 128, 0, s>>>(
+                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law,
+                    kr, S(c->cfg.dt), c->d_counters);
+            else
+                k_narrow_obstacles<S, true><<<grid, 128, 0, s>>>(
+                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law,
+                    kr, S(c->cfg.dt), c->d_counters);
+            c->launches += 1;
+        }
         GB_CK(cudaGetLastError());
     }
     mark(c, 6);
@@ -703,11 +768,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
     launch_particles<S>(c, st, tb, po, sp, c->d_contacts);
     GB_CK(cudaGetLastError());
     mark(c, 7);
-    if(c->timing)
-    {
-        c->ev_pending = c->ev_set;
-        c->ev_set ^= 1;
-    }
+    close_event_set(c);
     c->in_step = false;
     if(phases & PHASE_MOVE)
     {
@@ -715,16 +776,7 @@ int run_detect(gb_ctx* c, int phases, int32_t* result)
         c->steps_done++;
     }
     c->detect_valid = true;
-    c->prev_npairs  = c->npairs;
     c->have_prev    = hist;
-    if(result)
-    {
-        std::vector<int> cnt(c->n);
-        GB_CK(cudaMemcpyAsync(cnt.data(), c->d_contacts, c->n * sizeof(int), cudaMemcpyDeviceToHost, s));
-        GB_CK(cudaStreamSynchronize(s));
-        for(int i = 0; i < c->n; ++i)
-            result[i] += cnt[i];
-    }
     return GB_OK;
 }
 
@@ -791,6 +843,119 @@ int finish(gb_ctx* c)
     c->last.status_flags |= flags;
     if(flags & kFlagCapacity)
         return GB_E_CAPACITY;
+    if(flags & kFlagNonFinite)
+        return GB_E_NONFINITE;
+    if(flags & kFlagOutOfDomain)
+        return GB_E_OUT_OF_DOMAIN;
+    return GB_OK;
+}
+
+// the host-side bookkeeping of one step, kept to replay aborted steps
+struct StepSnap
+{
+    int     cur;
+    bool    have_prev, verlet_started, torce_dirty, mask_valid, detect_valid, links_valid;
+    int64_t steps_done;
+};
+
+StepSnap snap(const gb_ctx* c)
+{
+    return {c->cur,         c->have_prev,    c->verlet_started, c->torce_dirty,
+            c->mask_valid,  c->detect_valid, c->links_valid,    c->steps_done};
+}
+
+void restore(gb_ctx* c, const StepSnap& s)
+{
+    c->cur            = s.cur;
+    c->have_prev      = s.have_prev;
+    c->verlet_started = s.verlet_started;
+    c->torce_dirty    = s.torce_dirty;
+    c->mask_valid     = s.mask_valid;
+    c->detect_valid   = s.detect_valid;
+    c->links_valid    = s.links_valid;
+    c->steps_done     = s.steps_done;
+}
+
+// Launches n_steps detects (PHASE_DETECT) or fused steps (PHASE_STEP) with no
+// host synchronisation between them, then reads the device status once.  A
+// step that aborted -- more candidate pairs than the capacity, or a cell too
+// full for the counting sort -- left the state untouched, and so did every
+// step launched after it (they return at entry): the host grows the capacity
+// or switches to the radix sort, restores its bookkeeping to the aborted step
+// and launches the remaining steps again.
+int run_steps(gb_ctx* c, int32_t n_steps, int phases, int32_t* result)
+{
+    cudaStream_t s    = c->stream;
+    const bool   hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
+    int32_t      done = 0;
+    for(int attempt = 0; done < n_steps; ++attempt)
+    {
+        if(attempt > 16)
+            return GB_E_CAPACITY;
+        std::vector<StepSnap> snaps;
+        GB_CK(cudaMemsetAsync(c->d_done, 0, sizeof(unsigned int), s));
+        for(int32_t k = done; k < n_steps; ++k)
+        {
+            snaps.push_back(snap(c));
+            GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, phases); }));
+            if(phases & PHASE_MOVE)
+            {
+                // the first step adds to a torce left by separate calls, then resets it
+                c->links_valid = false;
+                c->torce_dirty = false;
+            }
+            else
+                c->torce_dirty = true;
+        }
+        // one synchronisation: status flags, completed launches and the last
+        // step's pair count together
+        GB_CK(cudaMemcpyAsync(c->h_pinned + 1, c->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaMemcpyAsync(c->h_pinned + 2, c->d_done, sizeof(unsigned int),
+                              cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaMemcpyAsync(c->h_pinned + 3, c->d_off[c->cur] + c->n, sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, s));
+        GB_CK(cudaStreamSynchronize(s));
+        const int      flags = (int)c->h_pinned[1];
+        const uint32_t ok    = c->h_pinned[2];
+        if(!(flags & kFlagAbort))
+        {
+            accumulate_pending(c);
+            c->npairs = c->h_pinned[3];
+            done      = n_steps;
+            break;
+        }
+        if(ok >= snaps.size())
+            return GB_E_CUDA; // an abort flag with every launch completed: inconsistent
+        c->ev_npending = 0;   // the aborted launches' phase times mean nothing
+        restore(c, snaps[ok]);
+        if(flags & kFlagCellCrowded)
+            c->radix_sort = true;
+        if(flags & kFlagCapacity)
+        {
+            // the aborted step's own pair total is in its offsets buffer (the
+            // steps after it skipped their scans)
+            const int cur_k = hist ? (c->cur ^ 1) : c->cur;
+            GB_CK(cudaMemcpy(c->h_pinned + 3, c->d_off[cur_k] + c->n, sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost));
+            const int64_t need = c->h_pinned[3];
+            c->cap_hint        = std::max<int64_t>(2 * c->cap, need + need / 4);
+        }
+        const int keep = flags & ~kFlagAbort;
+        std::memcpy(c->h_pinned + 1, &keep, sizeof(int));
+        GB_CK(cudaMemcpy(c->d_flags, c->h_pinned + 1, sizeof(int), cudaMemcpyHostToDevice));
+        done += (int32_t)ok;
+    }
+    if(result)
+    {
+        std::vector<int> cnt(c->n);
+        GB_CK(cudaMemcpy(cnt.data(), c->d_contacts, c->n * sizeof(int), cudaMemcpyDeviceToHost));
+        for(int i = 0; i < c->n; ++i)
+            result[i] += cnt[i];
+    }
+    // the status (finish() without another synchronisation)
+    const int flags = n_steps > 0 ? (int)c->h_pinned[1] : 0;
+    GB_CK(cudaMemsetAsync(c->d_flags, 0, sizeof(int), s));
+    c->last.status_flags |= flags;
     if(flags & kFlagNonFinite)
         return GB_E_NONFINITE;
     if(flags & kFlagOutOfDomain)
@@ -866,12 +1031,16 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
     c->nob    = cfg->n_obstacles;
     c->nmat   = cfg->n_materials;
     int st    = GB_OK;
+    int sms   = 0;
+    if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) == cudaSuccess
+       && sms > 0)
+        c->sms = sms;
     if(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
         st = GB_E_CUDA;
     c->stream = c->own_stream;
     c->timing = (cfg->flags & GB_FLAG_PHASE_TIMING) != 0;
     if(st == GB_OK && c->timing)
-        for(int b = 0; b < 2 && st == GB_OK; ++b)
+        for(int b = 0; b < gb_ctx::kEvRing && st == GB_OK; ++b)
             for(int k = 0; k <= GB_N_PHASES; ++k)
                 if(cudaEventCreate(&c->ev[b][k]) != cudaSuccess)
                 {
@@ -884,6 +1053,7 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
     if(st == GB_OK)
         st = ensure_pairs(c, cfg->pair_capacity > 0 ? cfg->pair_capacity
                                                     : std::max<int64_t>(1 << 16, 8 * (int64_t)c->n));
+    c->cap_hint = c->cap;
     if(st != GB_OK)
     {
         gb_destroy(c);
@@ -901,11 +1071,12 @@ int gb_destroy(gb_ctx* c)
     if(c->stream)
         cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
-                    c->d_obs_mass, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
+                    c->d_obs_mass, c->d_obs_plane, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
-                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_ccount, c->d_spos, c->d_spos32, c->d_slot, c->d_obsmask, c->d_count,
+                    c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_ccount, c->d_spos, c->d_spos32, c->d_slot, c->d_sorted_of, c->d_obsmask_id, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
-                    c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_contacts,
+                    c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_done,
+                    c->d_contacts,
                     c->d_stage};
     for(void* p : ptrs)
         if(p)
@@ -919,7 +1090,7 @@ int gb_destroy(gb_ctx* c)
     if(c->h_pinned)
         cudaFreeHost(c->h_pinned);
     if(c->timing)
-        for(int b = 0; b < 2; ++b)
+        for(int b = 0; b < gb_ctx::kEvRing; ++b)
             for(int k = 0; k <= GB_N_PHASES; ++k)
                 cudaEventDestroy(c->ev[b][k]);
     if(c->own_stream)
@@ -1022,7 +1193,8 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
     }
     if(st)
         return st;
-    c->rb_set = true;
+    c->rb_set     = true;
+    c->mask_valid = false;
     return GB_OK;
 }
 
@@ -1077,7 +1249,8 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
     }
     if(st)
         return st;
-    c->obs_set = true;
+    c->obs_set    = true;
+    c->mask_valid = false;
     return GB_OK;
 }
 
@@ -1089,7 +1262,8 @@ int gb_set_rigid_body_ids(gb_ctx* c, const uint32_t* ids)
         if(ids[i] >= (uint32_t)c->nrb)
             return GB_E_INVALID_ARG;
     GB_CK(cudaMemcpy(c->d_rb_id, ids, c->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    c->ids_set = true;
+    c->ids_set    = true;
+    c->mask_valid = false;
     return GB_OK;
 }
 
@@ -1113,7 +1287,7 @@ int gb_set_transforms(gb_ctx* c, const double* t)
     GB_CK(cudaGetLastError());
     GB_CK(cudaStreamSynchronize(c->stream));
     c->tr_set      = true;
-    c->links_valid = c->detect_valid = false;
+    c->links_valid = c->detect_valid = c->mask_valid = false;
     return GB_OK;
 }
 
@@ -1230,9 +1404,7 @@ int gb_detect_collision_and_compute_contact_forces(gb_ctx* c, int32_t* result)
 {
     GB_TRY(ready(c));
     GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
-    GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, PHASE_DETECT, result); }));
-    c->torce_dirty = true;
-    return finish(c);
+    return run_steps(c, 1, PHASE_DETECT, result);
 }
 
 int gb_add_external_forces(gb_ctx* c)
@@ -1258,18 +1430,7 @@ int gb_step(gb_ctx* c, int32_t n_steps)
     if(n_steps < 0)
         return GB_E_INVALID_ARG;
     GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
-    int worst = GB_OK;
-    for(int32_t s = 0; s < n_steps; ++s)
-    {
-        // the first step adds to a torce left by separate calls, then resets it
-        GB_TRY(dispatch(c, [&](auto z) { return run_detect<decltype(z)>(c, PHASE_STEP, nullptr); }));
-        c->links_valid = false;
-        c->torce_dirty = false;
-    }
-    int st = finish(c);
-    if(st != GB_OK)
-        worst = st;
-    return worst;
+    return run_steps(c, n_steps, PHASE_STEP, nullptr);
 }
 
 int gb_synchronize(gb_ctx* c)

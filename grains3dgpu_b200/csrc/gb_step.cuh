@@ -35,6 +35,8 @@ struct Tables
     const RBShape<store_t<S>>*   obs_shape;
     const double*                obs_tr; // 12 per obstacle (basis, origin)
     const double*                obs_mass;
+    const double4*               obs_plane; // Rectangle planes: normal, normal . origin
+    uint32_t                     obs_rect;  // bit o: obstacle o (< 32) is a Rectangle
     int                          n_obs;
     // FP64 copies of the shape tables (the mixed mode's polish reads these)
     const RBShape<double>* shape64;
@@ -224,37 +226,52 @@ GB_D void obstacle_frame(const Tables<S>& tb, int o, const double xa[3], V3<S>& 
 // sides) cannot touch it, and the full test of closest_rectangle would reject
 // it too.  Other obstacle types are always candidates.
 template <typename S>
-GB_D uint32_t obstacle_mask(const State<store_t<S>>& st, const Tables<S>& tb, uint32_t a)
+GB_D uint32_t obstacle_mask_at(const Tables<S>& tb, uint32_t r, const M3<S>& RA, const double xa[3])
 {
-    if(tb.n_obs == 0)
+    const int nm = tb.n_obs < kMaskObstacles ? tb.n_obs : kMaskObstacles;
+    if(nm == 0)
         return 0u;
-    const uint32_t r     = st.rb_id[a];
-    const V3<S>    bb    = mk<S>(S(tb.shape[r].bb[0]), S(tb.shape[r].bb[1]), S(tb.shape[r].bb[2]));
-    const M3<S>    RA    = load_rot<S>(st, a);
-    const double   xa[3] = {st.pos[0][a], st.pos[1][a], st.pos[2][a]};
-    uint32_t       mask  = 0u;
-    const int      nm    = tb.n_obs < kMaskObstacles ? tb.n_obs : kMaskObstacles;
+    // in FP64 throughout: the plane distance from the exact centre, the box
+    // extent along the normal from this mode's rotation; the slack covers the
+    // rounding of both and the 1e-7 difference between the mixed mode's FP32
+    // rotation and the FP64 one its contact recomputation uses
+    const double bb[3] = {(double)tb.shape[r].bb[0], (double)tb.shape[r].bb[1],
+                          (double)tb.shape[r].bb[2]};
+    const double ax    = fabs(xa[0]) + fabs(xa[1]) + fabs(xa[2]);
+    uint32_t     mask  = ~tb.obs_rect & ((nm == 32) ? ~0u : ((1u << nm) - 1u));
     for(int o = 0; o < nm; ++o)
     {
-        bool cand = true;
-        if(tb.obs_shape[o].type == GB_RECTANGLE)
+        if(!((tb.obs_rect >> o) & 1u))
+            continue;
+        const double4 pl = tb.obs_plane[o];
+        const double  dc = fabs(pl.x * xa[0] + pl.y * xa[1] + pl.z * xa[2] - pl.w);
+        double        hb = 0.0;
+#pragma unroll
+        for(int k = 0; k < 3; ++k)
         {
-            V3<S> oA, oO;
-            M3<S> RO;
-            obstacle_frame(tb, o, xa, oA, oO, RO);
-            const V3<S> rn  = mk<S>(RO.m[2], RO.m[5], RO.m[8]);
-            const V3<S> nb  = mul_t(RA, rn);
-            const S     dc  = s_fabs(dot(rn, oA - oO));
-            const S     hb  = bb.x * s_fabs(nb.x) + bb.y * s_fabs(nb.y) + bb.z * s_fabs(nb.z);
-            const S     mag = s_fabs(oA.x) + s_fabs(oA.y) + s_fabs(oA.z) + s_fabs(oO.x)
-                          + s_fabs(oO.y) + s_fabs(oO.z) + hb;
-            const S slack = is_mixed<S>() ? S(1e-6) + S(1e-6) * mag : S(1e-12) * (S(1.0) + mag);
-            cand          = !(dc - hb > slack);
+            // (RA^T n)_k = sum_j RA[j][k] n_j
+            const double nk = to_d(RA.m[k]) * pl.x + to_d(RA.m[3 + k]) * pl.y
+                              + to_d(RA.m[6 + k]) * pl.z;
+            hb += bb[k] * fabs(nk);
         }
-        if(cand)
+        const double slack = 1e-6 * hb + 1e-12 * (1.0 + ax + fabs(pl.w));
+        if(!(dc - hb > slack))
             mask |= 1u << o;
     }
     return mask;
+}
+
+// The mask is computed where the pose is at hand: by k_particles right after
+// each move, and by k_obstacle_mask after the state was set from the host.
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+    k_obstacle_mask(int n, State<store_t<S>> st, Tables<S> tb, uint32_t* __restrict__ mask)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const double xa[3] = {st.pos[0][i], st.pos[1][i], st.pos[2][i]};
+    mask[i]            = obstacle_mask_at<S>(tb, st.rb_id[i], load_rot<S>(st, i), xa);
 }
 
 GB_D int obstacle_candidates(uint32_t mask, int n_obs)
@@ -288,10 +305,11 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
                 continue;
             const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
             const uint32_t t1  = cstart[row + (uint32_t)x1 + 1];
+            // the particle itself passes every test below and is dropped
+            // only on a hit, which keeps the common path short
+#pragma unroll 2
             for(uint32_t t = cstart[row + (uint32_t)x0]; t < t1; ++t)
             {
-                if(t == (uint32_t)s)
-                    continue;
                 if constexpr(PRE32)
                 {
                     const float4 q  = spos32[t];
@@ -316,7 +334,7 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
                     const double r  = pa.w + pb.w;
                     h               = dx * dx + dy * dy + dz * dz < r * r;
                 }
-                if(h)
+                if(h && t != (uint32_t)s)
                     hit(t);
             }
         }
@@ -333,15 +351,15 @@ GB_D constexpr bool is_strict()
 
 // Count pass: per particle (by id) the number of candidates -- particles,
 // then obstacles -- with the first kPairSlots particle candidates (sorted
-// positions t, in enumeration order) in slot[s] and the obstacle mask in
-// obsmask[s].
+// positions t, in enumeration order) in slot[s]; the obstacle candidates are
+// mask_by_id's (from k_particles or k_obstacle_mask).
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_count(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
                  uint32_t* __restrict__ count, uint32_t* __restrict__ slot,
-                 uint32_t* __restrict__ obsmask, State<store_t<S>> st, Tables<S> tb)
+                 const uint32_t* __restrict__ mask_by_id, int n_obs)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= n)
@@ -355,38 +373,39 @@ __global__ void __launch_bounds__(kBlock)
                                                           ++c;
                                                       });
     const uint32_t a    = sids[s];
-    const uint32_t mask = obstacle_mask<S>(st, tb, a);
-    obsmask[s]          = mask;
-    count[a]            = c + (uint32_t)obstacle_candidates(mask, tb.n_obs);
+    const uint32_t mask = n_obs ? mask_by_id[a] : 0u;
+    count[a]            = c + (uint32_t)obstacle_candidates(mask, n_obs);
 }
 
-// Fill pass: the pair records of particle a at offset[a] -- its particle
-// candidates copied from the slots (or enumerated again when there were more
-// than kPairSlots), then its obstacle candidates.
+// Fill pass, one thread per particle id a (most have no candidate and read
+// only count[a]): the pair records of a at offset[a] -- its particle
+// candidates copied from the slots of its sorted position s = sorted_of[a]
+// (or enumerated again when there were more than kPairSlots), then its
+// obstacle candidates.
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_fill(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
-                const double4* __restrict__ spos, const float4* __restrict__ spos32,
-                const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
-                const uint32_t* __restrict__ count, const uint32_t* __restrict__ slot,
-                const uint32_t* __restrict__ obsmask, int n_obs,
-                const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
+                const uint32_t* __restrict__ sorted_of, const double4* __restrict__ spos,
+                const float4* __restrict__ spos32, const uint32_t* __restrict__ cstart,
+                uint32_t nx, uint32_t ny, uint32_t nz, const uint32_t* __restrict__ count,
+                const uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
+                int n_obs, const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if(s >= n)
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if(a >= n || step_aborted(flags))
         return;
-    const uint32_t a = sids[s];
     const uint32_t c = count[a];
     if(c == 0)
         return;
+    const int s = (int)sorted_of[a];
     int64_t out = offset[a];
     if(out + c > cap)
     {
         atomicOr(flags, kFlagCapacity);
         return;
     }
-    const uint32_t mask = obsmask[s];
+    const uint32_t mask = n_obs ? mask_by_id[a] : 0u;
     const uint32_t cp   = c - (uint32_t)obstacle_candidates(mask, n_obs);
     if(cp <= kPairSlots)
     {
@@ -482,13 +501,12 @@ GB_D void store_pair(const PairOut<store_t<S>>& po, int64_t p, const Force<S>& F
 // Pair p of particle a with obstacle o: closestPointsRigidBodies against the
 // obstacle and the contact law with the obstacle at rest
 // (ComponentManagerCPU.cpp:301-351).  The history law starts a fresh spring
-// for obstacle contacts every step.  Kept out of line: it is rare and would
-// otherwise set the register count of the particle-pair path.
-template <typename S>
-__device__ __noinline__ void narrow_obstacle(int64_t p, uint32_t a, int o,
-                                             const State<store_t<S>>& st, const Tables<S>& tb,
-                                             const PairOut<store_t<S>>& po, int law_kind,
-                                             int has_kr, S dt, unsigned long long* counters)
+// for obstacle contacts every step.  GEN: some obstacle is not a Rectangle
+// and needs the general GJK.
+template <typename S, bool GEN>
+GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>& st,
+                          const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind,
+                          int has_kr, S dt, unsigned long long* counters)
 {
     const uint32_t ra    = st.rb_id[a];
     const Body<S>  A     = load_body<S>(tb.shape, ra, tb.verts);
@@ -520,12 +538,12 @@ __device__ __noinline__ void narrow_obstacle(int64_t p, uint32_t a, int o,
                                             mk<double>(ot[2], ot[5], ot[8])));
             }
         }
-        else
+        else if constexpr(GEN)
             ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
     }
     else if(O.type == GB_RECTANGLE)
         ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
-    else
+    else if constexpr(GEN)
         ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
     const bool hit = ci.overlap < S(0.0);
     Force<S>   F;
@@ -567,23 +585,16 @@ __device__ __noinline__ void narrow_obstacle(int64_t p, uint32_t a, int o,
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
 
+// particle pair record p (obstacle records are k_narrow_obstacles')
 template <typename S>
-__global__ void __launch_bounds__(128)
-    k_narrow(int64_t npairs, const uint32_t* __restrict__ pair_a,
-             const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
-             PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
-             unsigned long long* __restrict__ counters)
+GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
+                      const uint32_t* __restrict__ pair_b, const State<store_t<S>>& st,
+                      const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind, int has_kr,
+                      S dt, unsigned long long* __restrict__ counters)
 {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if(p >= npairs)
-        return;
     const uint32_t a = pair_a[p], b = pair_b[p];
-    if(b & kObstacleBit)
-    {
-        narrow_obstacle<S>(p, a, (int)(b & ~kObstacleBit), st, tb, po, law_kind, has_kr, dt,
-                           counters);
+    if(b & kObstacleBit) // k_narrow_obstacles
         return;
-    }
     const uint32_t ra = st.rb_id[a], rb = st.rb_id[b];
     const Body<S>  A = load_body<S>(tb.shape, ra, tb.verts);
     const Body<S>  B = load_body<S>(tb.shape, rb, tb.verts);
@@ -657,6 +668,23 @@ __global__ void __launch_bounds__(128)
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
 
+// The pair count is read on the device (*total, the scan's grand total), so
+// the host launches a resident-sized grid without waiting for it.
+template <typename S>
+__global__ void __launch_bounds__(128)
+    k_narrow(const uint32_t* __restrict__ total, const int* __restrict__ flags,
+             const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
+             State<store_t<S>> st, Tables<S> tb, PairOut<store_t<S>> po, int law_kind, int has_kr,
+             S dt, unsigned long long* __restrict__ counters)
+{
+    if(step_aborted(flags))
+        return;
+    const int64_t npairs = *total;
+    for(int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
+        p += (int64_t)gridDim.x * blockDim.x)
+        narrow_pair<S>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters);
+}
+
 // ---- per-particle kernel -------------------------------------------------------
 // PHASE_DETECT:  torce = sum of the particle's pair forces in enumeration
 //                order, then obstacle contacts in obstacle order
@@ -686,6 +714,29 @@ struct StepParams
     int      accumulate; // PHASE_DETECT adds to the stored torce instead of to zero
 };
 
+// The particle-obstacle records of the pair list, one thread per record, in a
+// kernel of their own: the two kinds interleave in the list, and one kernel
+// for both would run both code paths in every warp.
+template <typename S, bool GEN>
+__global__ void __launch_bounds__(128)
+    k_narrow_obstacles(const uint32_t* __restrict__ total, const int* __restrict__ flags,
+                       const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
+                       State<store_t<S>> st, Tables<S> tb, PairOut<store_t<S>> po, int law_kind,
+                       int has_kr, S dt, unsigned long long* __restrict__ counters)
+{
+    if(step_aborted(flags))
+        return;
+    const int64_t npairs = *total;
+    for(int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
+        p += (int64_t)gridDim.x * blockDim.x)
+    {
+        const uint32_t b = pair_b[p];
+        if(b & kObstacleBit)
+            narrow_obstacle<S, GEN>(p, pair_a[p], (int)(b & ~kObstacleBit), st, tb, po, law_kind,
+                                    has_kr, dt, counters);
+    }
+}
+
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
 // A streaming kernel: four 256-thread blocks per SM keep enough loads in
 // flight (the mixed instantiation fits 64 registers without spilling; the
@@ -693,11 +744,15 @@ struct StepParams
 template <typename S>
 __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
-                PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out)
+                PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
+                uint32_t* __restrict__ mask_out, const int* __restrict__ flags,
+                unsigned int* __restrict__ done)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= n)
+    if(i >= n || step_aborted(flags))
         return;
+    if(i == 0)
+        atomicAdd(done, 1u); // the host counts the launches that completed
     const uint32_t            r   = st.rb_id[i];
     const RBInertia<store_t<S>>* in = tb.inertia + r;
     const S                   m   = S(in->mass);
@@ -782,23 +837,31 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
             dq    = quaternion_change(w, sp.dt);
         }
         // Transform3::updateTransform (Transform3.cpp:324-329)
+        double xn[3];
 #pragma unroll
         for(int k = 0; k < 3; ++k)
         {
             const S tk[3] = {trans.x, trans.y, trans.z};
             if constexpr(is_mixed<S>())
-                st.pos[k][i] = st.pos[k][i] + (double)tk[k];
+                xn[k] = st.pos[k][i] + (double)tk[k];
             else
-                st.pos[k][i] = to_d(S(st.pos[k][i]) + tk[k]);
+                xn[k] = to_d(S(st.pos[k][i]) + tk[k]);
+            st.pos[k][i] = xn[k];
         }
         if constexpr(is_mixed<S>())
         {
             Quat<S> qn = qmul(dq, q);
             const S nq = s_sqrt(qn.w * qn.w + norm2(qn.v));
-            st.rot[0][i] = qn.w / nq;
-            st.rot[1][i] = qn.v.x / nq;
-            st.rot[2][i] = qn.v.y / nq;
-            st.rot[3][i] = qn.v.z / nq;
+            qn.w /= nq;
+            qn.v.x /= nq;
+            qn.v.y /= nq;
+            qn.v.z /= nq;
+            st.rot[0][i] = qn.w;
+            st.rot[1][i] = qn.v.x;
+            st.rot[2][i] = qn.v.y;
+            st.rot[3][i] = qn.v.z;
+            if(mask_out)
+                R = quat_to_matrix<S>(qn.w, qn.v.x, qn.v.y, qn.v.z);
         }
         else
         {
@@ -807,6 +870,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
             for(int k = 0; k < 9; ++k)
                 st.rot[k][i] = to_d(R.m[k]);
         }
+        // the obstacle candidates of the next detect, from the new pose
+        if(mask_out)
+            mask_out[i] = obstacle_mask_at<S>(tb, r, R, xn);
         st.vel[0][i] = (store_t<S>)to_d(v.x);
         st.vel[1][i] = (store_t<S>)to_d(v.y);
         st.vel[2][i] = (store_t<S>)to_d(v.z);

@@ -148,6 +148,28 @@ def test_crowded_cell_falls_back_to_radix_sort(gb, oracle, precision):
     assert np.abs(g.transforms()[:, 9:] - o.transforms()[:, 9:]).max() < 1e-9
 
 
+@pytest.mark.parametrize("law", [abi.GB_LAW_HOOKE, abi.GB_LAW_HOOKE_HISTORY])
+def test_pair_capacity_overflow_is_replayed(gb, law):
+    """A pair capacity far too small makes steps abort on the device; the
+    engine grows it and replays them.  The trajectory (and, with the history
+    law, the tangential springs carried across the regrowth) equals the one
+    of a context that never overflowed."""
+    scene = make_scene("sphere")
+    scene.contact_models = [dict(m, etat=0.3) for m in scene.contact_models]
+    small = scenes.System(gb, scene, precision=abi.GB_FP64_STRICT, contact_law=law,
+                          pair_capacity=64)
+    large = scenes.System(gb, scene, precision=abi.GB_FP64_STRICT, contact_law=law)
+    for s in (small, large):
+        s.step(2)
+        s.detect()
+        s.add_external_forces()
+        s.move()
+        s.step(6)
+    assert small.stats().candidate_pairs > 64
+    assert np.array_equal(small.transforms(), large.transforms())
+    assert np.array_equal(small.velocities(), large.velocities())
+
+
 @pytest.mark.parametrize("precision", [abi.GB_FP64_STRICT, abi.GB_MIXED])
 def test_torce_accumulation(gb, oracle, precision):
     """set_torces, two detects and gravity add onto one torce; the move (and
