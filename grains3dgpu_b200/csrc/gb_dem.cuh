@@ -33,7 +33,9 @@ GB_D Contact<S> no_contact()
 // closestPointsRigidBodies for two particles (CollisionDetection.cpp:182-284)
 // plus closestPointsSpheres (:26-48).  oA/oB are the frame origins in the
 // working coordinates (xA, xB absolute; or 0, xB-xA relative); d = xB - xA.
-template <typename S>
+// VAR selects the GJK (GB_GJK_JH, the reference's choice, or GB_GJK_SV /
+// GB_GJK_NESTEROV).
+template <int VAR = GB_GJK_JH, typename S>
 GB_D Contact<S> closest_points(const Body<S>& A, const Body<S>& B, const M3<S>& RA,
                                const M3<S>& RB, const V3<S>& oA, const V3<S>& oB,
                                const V3<S>& d, int* gjk_iters)
@@ -63,7 +65,7 @@ GB_D Contact<S> closest_points(const Body<S>& A, const Body<S>& B, const M3<S>& 
     const M3<S> RAt = transpose(RA);
     b2a.R           = mul(RAt, RB);
     b2a.o           = mul(RAt, d);
-    GjkResult<S> g  = gjk_jh(A, B, b2a);
+    GjkResult<S> g  = gjk<VAR>(A, B, b2a);
     *gjk_iters += g.iters;
     S distance = g.dist - (A.crust + B.crust);
     if(distance > S(0.0))

@@ -733,24 +733,34 @@ int run_detect(gb_ctx* c, int phases)
         const uint32_t* total = c->d_off[c->cur] + c->n;
         const int       grid  = (int)std::max<int64_t>(
             1, std::min<int64_t>(blocks(c->cap, 128), (int64_t)8 * c->sms));
-        const int kr = c->has_kr ? 1 : 0;
-        k_narrow<S><<<grid, 128, 0, s>>>(total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po,
-                                         c->cfg.contact_law, kr, S(c->cfg.dt), c->d_counters);
-        c->launches += 1;
-        if(c->nob)
-        {
+        const int kr  = c->has_kr ? 1 : 0;
+        const int law = c->cfg.contact_law;
+        // the GJK variant is a template parameter: each run compiles in one
+        auto with_variant = [&](auto var) {
+            constexpr int VAR = decltype(var)::value;
+            k_narrow<S, VAR><<<grid, 128, 0, s>>>(total, c->d_flags, c->d_pa, c->d_pb[c->cur], st,
+                                                  tb, po, law, kr, S(c->cfg.dt), c->d_counters);
+            c->launches += 1;
+            if(!c->nob)
+                return;
             const bool all_rect = c->nob <= kMaskObstacles
                                   && c->obs_rect == ((c->nob == 32) ? ~0u : ((1u << c->nob) - 1u));
             if(all_rect)
-                k_narrow_obstacles<S, false><<<grid, 128, 0, s>>>(
-                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law,
-                    kr, S(c->cfg.dt), c->d_counters);
+                k_narrow_obstacles<S, false, GB_GJK_JH><<<grid, 128, 0, s>>>(
+                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
+                    S(c->cfg.dt), c->d_counters);
             else
-                k_narrow_obstacles<S, true><<<grid, 128, 0, s>>>(
-                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, c->cfg.contact_law,
-                    kr, S(c->cfg.dt), c->d_counters);
+                k_narrow_obstacles<S, true, VAR><<<grid, 128, 0, s>>>(
+                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
+                    S(c->cfg.dt), c->d_counters);
             c->launches += 1;
-        }
+        };
+        if(c->cfg.gjk_variant == GB_GJK_SV)
+            with_variant(std::integral_constant<int, GB_GJK_SV>{});
+        else if(c->cfg.gjk_variant == GB_GJK_NESTEROV)
+            with_variant(std::integral_constant<int, GB_GJK_NESTEROV>{});
+        else
+            with_variant(std::integral_constant<int, GB_GJK_JH>{});
         GB_CK(cudaGetLastError());
     }
     mark(c, 6);
@@ -1016,8 +1026,9 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
        || (cfg->contact_law != GB_LAW_HOOKE && cfg->contact_law != GB_LAW_HOOKE_HISTORY)
        || (cfg->integrator != GB_FIRST_ORDER_EXPLICIT && cfg->integrator != GB_VELOCITY_VERLET))
         return fail(GB_E_INVALID_ARG);
-    if(cfg->gjk_variant != GB_GJK_JH)
-        return fail(GB_E_UNSUPPORTED);
+    if(cfg->gjk_variant != GB_GJK_JH && cfg->gjk_variant != GB_GJK_SV
+       && cfg->gjk_variant != GB_GJK_NESTEROV)
+        return fail(GB_E_INVALID_ARG);
     int ndev = 0;
     if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
         return fail(GB_E_NO_DEVICE);

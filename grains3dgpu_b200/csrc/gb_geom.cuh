@@ -416,4 +416,333 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
     return r;
 }
 
+// ---- signed-volume sub-algorithm (GJK_AY.cpp:15-368, Montanari et al. 2017) --
+template <typename S>
+GB_D S comp(const V3<S>& v, unsigned i)
+{
+    return i == 0 ? v.x : (i == 1 ? v.y : v.z);
+}
+
+template <typename S>
+GB_D unsigned sv_same_sign(S a, S b)
+{
+    return (unsigned)(!((a > S(0.0)) ^ (b > S(0.0)))); // compareSigns (GJK_AY.cpp:8-12)
+}
+
+// sum of lambda_i y_i over the used points (computeVector, GJK_AY.cpp:304-316)
+template <typename S>
+GB_D V3<S> sv_point(const V3<S> y[4], unsigned used, const S lambdas[4])
+{
+    V3<S> o = zero3<S>();
+#pragma unroll
+    for(unsigned i = 0; i < 4; ++i)
+        if(used & (1u << i))
+            o = o + lambdas[i] * y[i];
+    return o;
+}
+
+// s1d (GJK_AY.cpp:15-84)
+template <typename S>
+GB_D void sv_s1d(const V3<S> y[4], unsigned& bits, S lambdas[4])
+{
+    bool     s1_set = false;
+    unsigned i1 = 0, i2 = 0;
+    for(unsigned i = 0; i < 4; ++i)
+        if(bits & (1u << i))
+        {
+            if(s1_set)
+            {
+                i2 = i;
+                break;
+            }
+            i1     = i;
+            s1_set = true;
+        }
+    const V3<S> t      = y[i2] - y[i1];
+    unsigned    I      = 0;
+    S           neg_tI = -t.x;
+    if(s_fabs(t.y) > s_fabs(neg_tI))
+    {
+        I      = 1;
+        neg_tI = -t.y;
+    }
+    if(s_fabs(t.z) > s_fabs(neg_tI))
+    {
+        I      = 2;
+        neg_tI = -t.z;
+    }
+    const S pI  = dot(y[i2], t) / norm2(t) * neg_tI + comp(y[i2], I);
+    const S C0  = -comp(y[i2], I) + pI, C1 = comp(y[i1], I) - pI;
+    const unsigned sc0 = sv_same_sign(neg_tI, C0), sc1 = sv_same_sign(neg_tI, C1);
+    if(sc0 + sc1 == 2)
+    {
+        lambdas[i1] = C0 / neg_tI;
+        lambdas[i2] = C1 / neg_tI;
+    }
+    else if(sc0)
+    {
+        bits &= ~(1u << i2);
+        lambdas[i1] = S(1.0);
+    }
+    else
+    {
+        bits &= ~(1u << i1);
+        lambdas[i2] = S(1.0);
+    }
+}
+
+// s2d (GJK_AY.cpp:87-212)
+template <typename S>
+GB_D void sv_s2d(const V3<S> y[4], unsigned& bits, S lambdas[4])
+{
+    unsigned counter = 0, i0 = 0, i1 = 0, i2 = 0;
+    for(unsigned i = 0; i < 4; ++i)
+        if(bits & (1u << i))
+        {
+            if(counter == 0)
+                i0 = i;
+            else if(counter == 1)
+                i1 = i;
+            else
+                i2 = i;
+            counter += 1;
+        }
+    const V3<S> n  = cross(y[i1] - y[i0], y[i2] - y[i0]);
+    const V3<S> p0 = (dot(y[i0], n) / norm2(n)) * n;
+    const V3<S>& Y0 = y[i0];
+    const V3<S>& Y1 = y[i1];
+    const V3<S>& Y2 = y[i2];
+    unsigned     ix = 1, iy = 2;
+    S mu_max = (Y1.y * Y2.z + Y0.y * Y1.z + Y2.y * Y0.z - Y1.y * Y0.z - Y2.y * Y1.z - Y0.y * Y2.z);
+    S mu     = (Y1.z * Y0.x + Y2.z * Y1.x + Y0.z * Y2.x - Y1.z * Y2.x - Y0.z * Y1.x - Y2.z * Y0.x);
+    if(s_fabs(mu) > s_fabs(mu_max))
+    {
+        mu_max = mu;
+        ix     = 0;
+    }
+    mu = (Y1.x * Y2.y + Y0.x * Y1.y + Y2.x * Y0.y - Y1.x * Y0.y - Y2.x * Y1.y - Y0.x * Y2.y);
+    if(s_fabs(mu) > s_fabs(mu_max))
+    {
+        mu_max = mu;
+        ix     = 0;
+        iy     = 1;
+    }
+    const S px = comp(p0, ix), py = comp(p0, iy);
+    const S y0x = comp(Y0, ix), y0y = comp(Y0, iy), y1x = comp(Y1, ix), y1y = comp(Y1, iy);
+    const S y2x = comp(Y2, ix), y2y = comp(Y2, iy);
+    S       C[3];
+    C[0] = (px * y1y + py * y2x + y1x * y2y - px * y2y - py * y1x - y2x * y1y);
+    C[1] = (px * y2y + py * y0x + y2x * y0y - px * y0y - py * y2x - y0x * y2y);
+    C[2] = (px * y0y + py * y1x + y0x * y1y - px * y1y - py * y0x - y1x * y0y);
+    const unsigned sc[3] = {sv_same_sign(mu_max, C[0]), sv_same_sign(mu_max, C[1]),
+                            sv_same_sign(mu_max, C[2])};
+    if(sc[0] + sc[1] + sc[2] == 3)
+    {
+        lambdas[i0] = C[0] / mu_max;
+        lambdas[i1] = C[1] / mu_max;
+        lambdas[i2] = C[2] / mu_max;
+        return;
+    }
+    S              d        = S(100000.0);
+    unsigned       new_bits = 0;
+    const unsigned idx[3]   = {i0, i1, i2};
+    for(unsigned j = 0; j < 3; ++j)
+        if(!sc[j])
+        {
+            unsigned new_used       = bits & ~(1u << idx[j]);
+            S        new_lambdas[4] = {S(0.0), S(0.0), S(0.0), S(0.0)};
+            sv_s1d(y, new_used, new_lambdas);
+            const V3<S> np     = sv_point(y, new_used, new_lambdas);
+            const S     d_star = dot(np, np);
+            if(d_star < d)
+            {
+                new_bits = new_used;
+                d        = d_star;
+                for(unsigned i = 0; i < 4; ++i)
+                    lambdas[i] = new_lambdas[i];
+            }
+        }
+    bits = new_bits;
+}
+
+// s3d (GJK_AY.cpp:215-301)
+template <typename S>
+GB_D void sv_s3d(const V3<S> y[4], unsigned& bits, S lambdas[4])
+{
+    S C[4];
+    C[0] = y[3].x * y[2].y * y[1].z + y[2].x * y[1].y * y[3].z + y[1].x * y[3].y * y[2].z
+           - y[1].x * y[2].y * y[3].z - y[2].x * y[3].y * y[1].z - y[3].x * y[1].y * y[2].z;
+    C[1] = y[0].x * y[2].y * y[3].z + y[2].x * y[3].y * y[0].z + y[3].x * y[0].y * y[2].z
+           - y[3].x * y[2].y * y[0].z - y[2].x * y[0].y * y[3].z - y[0].x * y[3].y * y[2].z;
+    C[2] = y[3].x * y[1].y * y[0].z + y[1].x * y[0].y * y[3].z + y[0].x * y[3].y * y[1].z
+           - y[0].x * y[1].y * y[3].z - y[1].x * y[3].y * y[0].z - y[3].x * y[0].y * y[1].z;
+    C[3] = y[0].x * y[1].y * y[2].z + y[1].x * y[2].y * y[0].z + y[2].x * y[0].y * y[1].z
+           - y[2].x * y[1].y * y[0].z - y[1].x * y[0].y * y[2].z - y[0].x * y[2].y * y[1].z;
+    const S  dM = C[0] + C[1] + C[2] + C[3];
+    unsigned sc[4];
+#pragma unroll
+    for(int i = 0; i < 4; ++i)
+        sc[i] = sv_same_sign(dM, C[i]);
+    if(sc[0] + sc[1] + sc[2] + sc[3] == 4)
+    {
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+            lambdas[i] = C[i] / dM;
+        return;
+    }
+    S        d        = S(100000.0);
+    unsigned new_bits = 0;
+    for(unsigned j = 0; j < 4; ++j)
+        if(!sc[j])
+        {
+            unsigned new_used       = bits & ~(1u << j);
+            S        new_lambdas[4] = {S(0.0), S(0.0), S(0.0), S(0.0)};
+            sv_s2d(y, new_used, new_lambdas);
+            const V3<S> np     = sv_point(y, new_used, new_lambdas);
+            const S     d_star = dot(np, np);
+            if(d_star < d)
+            {
+                new_bits = new_used;
+                d        = d_star;
+                for(unsigned i = 0; i < 4; ++i)
+                    lambdas[i] = new_lambdas[i];
+            }
+        }
+    bits = new_bits;
+}
+
+// sv_subalgorithm (GJK_AY.cpp:340-368): new simplex, weights and closest point
+template <typename S>
+GB_D V3<S> sv_subalgorithm(const V3<S> y[4], unsigned& bits, S lambdas[4])
+{
+    unsigned num_used = 0;
+#pragma unroll
+    for(unsigned i = 0; i < 4; ++i)
+        num_used += (bits >> i) & 1u;
+    if(num_used == 1)
+    {
+        for(unsigned i = 0; i < 4; ++i)
+            if(bits & (1u << i))
+                lambdas[i] = S(1.0);
+    }
+    else if(num_used == 2)
+        sv_s1d(y, bits, lambdas);
+    else if(num_used == 3)
+        sv_s2d(y, bits, lambdas);
+    else
+        sv_s3d(y, bits, lambdas);
+    return sv_point(y, bits, lambdas);
+}
+
+// w equal to a vertex of the simplex `bits` (degenerate, GJK_AY.cpp:373-386)
+template <typename S>
+GB_D bool sv_degenerate(unsigned bits, const V3<S> y[4], const V3<S>& w)
+{
+    for(unsigned i = 0; i < 4; ++i)
+        if((bits & (1u << i)) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z)
+            return true;
+    return false;
+}
+
+// GJK with the signed-volume sub-algorithm; NESTEROV: the support direction
+// follows the momentum average of Montaut et al. (RSS 2022, Algorithm 2),
+// with GJK_AY's gap test redone along x_k (see oracle's gjk_nesterov):
+//   y_k = delta_k x_k + (1 - delta_k) s_{k-1},   delta_k = (k + 1)/(k + 3),
+//   d_k = delta_k d_{k-1}/|d_{k-1}| + (1 - delta_k) y_k/|y_k|.
+// Without NESTEROV it is computeClosestPoints_GJK_AY (GJK_AY.cpp:392-469).
+template <typename S, bool NESTEROV>
+GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
+{
+    unsigned bits = 0, last = 0;
+    V3<S>    p[4], q[4], y[4];
+    S        lambdas[4] = {S(0.0), S(0.0), S(0.0), S(0.0)};
+#pragma unroll
+    for(int i = 0; i < 4; ++i)
+        p[i] = q[i] = y[i] = zero3<S>();
+    int     num_iterations = 0;
+    bool    momentum       = NESTEROV;
+    const S rel_error      = k_loweps<S>();
+    const S abs_error      = S(1.e-4) * rel_error;
+    V3<S>   v = support(A, zero3<S>()) - apply(b2a, support(B, zero3<S>()));
+    V3<S>   w = v, d = v, s_prev = v;
+    S       dist = norm(v);
+    while(bits < 15 && dist > k_higheps<S>() && num_iterations < 1000)
+    {
+        for(unsigned k = 0; k < 4; ++k)
+            if(!(bits & (1u << k)))
+            {
+                last = k;
+                break;
+            }
+        if constexpr(NESTEROV)
+        {
+            if(momentum)
+            {
+                const S     kk    = S((double)num_iterations);
+                const S     delta = (kk + S(1.0)) / (kk + S(3.0));
+                const S     om    = S(1.0) - delta;
+                const V3<S> yk    = mk<S>(delta * v.x + om * s_prev.x, delta * v.y + om * s_prev.y,
+                                       delta * v.z + om * s_prev.z);
+                const S     ny = norm(yk), nd = norm(d);
+                if(ny > k_higheps<S>() && nd > k_higheps<S>())
+                    d = mk<S>(delta * (d.x / nd) + om * (yk.x / ny),
+                              delta * (d.y / nd) + om * (yk.y / ny),
+                              delta * (d.z / nd) + om * (yk.z / ny));
+                else
+                {
+                    momentum = false;
+                    d        = v;
+                }
+            }
+            else
+                d = v;
+        }
+        else
+            d = v;
+        p[last]   = support(A, -d);
+        q[last]   = support(B, mul_t(b2a.R, d));
+        w         = p[last] - apply(b2a, q[last]);
+        const S mu = dist - dot(v, w) / dist;
+        if(mu < dist * rel_error || mu < abs_error || sv_degenerate(bits, y, w))
+        {
+            if(!momentum)
+                break;
+            momentum = false; // not a certified gap: redo this iteration along x_k
+            continue;
+        }
+        y[last] = w;
+        bits |= 1u << last;
+        ++num_iterations;
+        v    = sv_subalgorithm(y, bits, lambdas);
+        dist = norm(v);
+        s_prev = w;
+    }
+    // computePoints (GJK_AY.cpp:319-337)
+    GjkResult<S> r;
+    r.pa = zero3<S>();
+    r.pb = zero3<S>();
+    for(unsigned i = 0; i < 4; ++i)
+        if(bits & (1u << i))
+        {
+            r.pa = r.pa + lambdas[i] * p[i];
+            r.pb = r.pb + lambdas[i] * q[i];
+        }
+    r.dist  = dist;
+    r.lower = S(0.0);
+    r.iters = num_iterations;
+    return r;
+}
+
+// the GJK of a variant (GB_GJK_JH | GB_GJK_SV | GB_GJK_NESTEROV)
+template <int VAR, typename S>
+GB_D GjkResult<S> gjk(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
+{
+    if constexpr(VAR == GB_GJK_SV)
+        return gjk_sv<S, false>(A, B, b2a);
+    else if constexpr(VAR == GB_GJK_NESTEROV)
+        return gjk_sv<S, true>(A, B, b2a);
+    else
+        return gjk_jh(A, B, b2a);
+}
+
 } // namespace gb

@@ -68,7 +68,9 @@ GB_D Contact<float> to_f(const Contact<double>& c)
     return r;
 }
 
-// closestPointsRigidBodies for the mixed mode; points relative to A's centre
+// closestPointsRigidBodies for the mixed mode; points relative to A's centre.
+// VAR: the GJK of the FP64 re-solve (the FP32 rejection is always Johnson's).
+template <int VAR>
 GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& st, uint32_t a,
                                   uint32_t b, uint32_t ra, uint32_t rb, const Body<float>& A,
                                   const Body<float>& B, const M3<float>& RA, const M3<float>& RB,
@@ -113,7 +115,7 @@ GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& s
     const M3<double>   RAt64 = transpose(RA64);
     b2a64.R                  = mul(RAt64, RB64);
     b2a64.o                  = mul(RAt64, d64);
-    const GjkResult<double> g = gjk_jh(A64, B64, b2a64);
+    const GjkResult<double> g = gjk<VAR>(A64, B64, b2a64);
     *iters += g.iters;
     const double distance = g.dist - (A64.crust + B64.crust);
     if(distance > 0.0)
@@ -502,8 +504,8 @@ GB_D void store_pair(const PairOut<store_t<S>>& po, int64_t p, const Force<S>& F
 // obstacle and the contact law with the obstacle at rest
 // (ComponentManagerCPU.cpp:301-351).  The history law starts a fresh spring
 // for obstacle contacts every step.  GEN: some obstacle is not a Rectangle
-// and needs the general GJK.
-template <typename S, bool GEN>
+// and needs the general GJK (of variant VAR).
+template <typename S, bool GEN, int VAR>
 GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>& st,
                           const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind,
                           int has_kr, S dt, unsigned long long* counters)
@@ -539,12 +541,12 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
             }
         }
         else if constexpr(GEN)
-            ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+            ci = closest_points<VAR>(A, O, RA, RO, oA, oO, oO - oA, &iters);
     }
     else if(O.type == GB_RECTANGLE)
         ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
     else if constexpr(GEN)
-        ci = closest_points(A, O, RA, RO, oA, oO, oO - oA, &iters);
+        ci = closest_points<VAR>(A, O, RA, RO, oA, oO, oO - oA, &iters);
     const bool hit = ci.overlap < S(0.0);
     Force<S>   F;
     F.f = F.t = F.m = zero3<S>();
@@ -585,8 +587,8 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
 
-// particle pair record p (obstacle records are k_narrow_obstacles')
-template <typename S>
+// particle pair record p (obstacle records are k_narrow_obstacles'); VAR: the GJK
+template <typename S, int VAR>
 GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
                       const uint32_t* __restrict__ pair_b, const State<store_t<S>>& st,
                       const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind, int has_kr,
@@ -617,9 +619,9 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
     int        iters = 0;
     Contact<S> ci;
     if constexpr(is_mixed<S>())
-        ci = closest_mixed(tb, st, a, b, ra, rb, A, B, RA, RB, xa, xb, &iters);
+        ci = closest_mixed<VAR>(tb, st, a, b, ra, rb, A, B, RA, RB, xa, xb, &iters);
     else
-        ci = closest_points(A, B, RA, RB, oA, oB, d, &iters);
+        ci = closest_points<VAR>(A, B, RA, RB, oA, oB, d, &iters);
     const bool hit = ci.overlap < S(0.0);
     Force<S>         F;
     F.f = F.t = F.m = zero3<S>();
@@ -670,7 +672,7 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
 
 // The pair count is read on the device (*total, the scan's grand total), so
 // the host launches a resident-sized grid without waiting for it.
-template <typename S>
+template <typename S, int VAR>
 __global__ void __launch_bounds__(128)
     k_narrow(const uint32_t* __restrict__ total, const int* __restrict__ flags,
              const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(128)
     const int64_t npairs = *total;
     for(int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
         p += (int64_t)gridDim.x * blockDim.x)
-        narrow_pair<S>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters);
+        narrow_pair<S, VAR>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters);
 }
 
 // ---- per-particle kernel -------------------------------------------------------
@@ -717,7 +719,7 @@ struct StepParams
 // The particle-obstacle records of the pair list, one thread per record, in a
 // kernel of their own: the two kinds interleave in the list, and one kernel
 // for both would run both code paths in every warp.
-template <typename S, bool GEN>
+template <typename S, bool GEN, int VAR>
 __global__ void __launch_bounds__(128)
     k_narrow_obstacles(const uint32_t* __restrict__ total, const int* __restrict__ flags,
                        const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
@@ -732,8 +734,8 @@ __global__ void __launch_bounds__(128)
     {
         const uint32_t b = pair_b[p];
         if(b & kObstacleBit)
-            narrow_obstacle<S, GEN>(p, pair_a[p], (int)(b & ~kObstacleBit), st, tb, po, law_kind,
-                                    has_kr, dt, counters);
+            narrow_obstacle<S, GEN, VAR>(p, pair_a[p], (int)(b & ~kObstacleBit), st, tb, po,
+                                         law_kind, has_kr, dt, counters);
     }
 }
 

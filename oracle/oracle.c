@@ -860,11 +860,403 @@ static double gjk_jh(const gb_convex* a, const double* va, const gb_convex* b,
     return dist;
 }
 
+/* ===========================================================================
+ * GJK with the signed-volume sub-algorithm
+ * (Grains/CollisionDetection/src/GJK_AY.cpp, Montanari et al. 2017)
+ * ======================================================================== */
+static unsigned sv_same_sign(double a, double b)
+{
+    /* compareSigns (GJK_AY.cpp:8-12) */
+    return (unsigned)(!((a > 0) ^ (b > 0)));
+}
+
+static void sv_s1d(double y[4][3], unsigned* bits, double lambdas[4])
+{
+    /* s1d (GJK_AY.cpp:15-84) */
+    int      s1_set = 0;
+    unsigned i1 = 0, i2 = 0;
+    for(unsigned i = 0; i < 4; ++i)
+        if(*bits & (1u << i))
+        {
+            if(s1_set)
+            {
+                i2 = i;
+                break;
+            }
+            i1     = i;
+            s1_set = 1;
+        }
+    double t[3];
+    sub3(y[i2], y[i1], t);
+    unsigned I      = 0;
+    double   neg_tI = -t[0];
+    if(fabs(t[1]) > fabs(neg_tI))
+    {
+        I      = 1;
+        neg_tI = -t[1];
+    }
+    if(fabs(t[2]) > fabs(neg_tI))
+    {
+        I      = 2;
+        neg_tI = -t[2];
+    }
+    const double pI   = dot3(y[i2], t) / norm2_3(t) * neg_tI + y[i2][I];
+    const double C[2] = {-y[i2][I] + pI, y[i1][I] - pI};
+    const unsigned sc0 = sv_same_sign(neg_tI, C[0]), sc1 = sv_same_sign(neg_tI, C[1]);
+    if(sc0 + sc1 == 2)
+    {
+        lambdas[i1] = C[0] / neg_tI;
+        lambdas[i2] = C[1] / neg_tI;
+    }
+    else if(sc0)
+    {
+        *bits &= ~(1u << i2);
+        lambdas[i1] = 1.0;
+    }
+    else
+    {
+        *bits &= ~(1u << i1);
+        lambdas[i2] = 1.0;
+    }
+}
+
+/* new_point = sum over the used points of lambda_i y_i, and its squared norm */
+static double sv_point(double y[4][3], unsigned used, const double lambdas[4], double o[3])
+{
+    zero3(o);
+    for(unsigned i = 0; i < 4; ++i)
+        if(used & (1u << i))
+        {
+            double t[3];
+            scal3(lambdas[i], y[i], t);
+            add3(o, t, o);
+        }
+    return dot3(o, o);
+}
+
+static void sv_s2d(double y[4][3], unsigned* bits, double lambdas[4])
+{
+    /* s2d (GJK_AY.cpp:87-212) */
+    unsigned counter = 0, i0 = 0, i1 = 0, i2 = 0;
+    for(unsigned i = 0; i < 4; ++i)
+        if(*bits & (1u << i))
+        {
+            if(counter == 0)
+                i0 = i;
+            else if(counter == 1)
+                i1 = i;
+            else
+                i2 = i;
+            counter += 1;
+        }
+    double e1[3], e2[3], n[3], p0[3];
+    sub3(y[i1], y[i0], e1);
+    sub3(y[i2], y[i0], e2);
+    cross3(e1, e2, n);
+    scal3(dot3(y[i0], n) / norm2_3(n), n, p0);
+    double* Y0 = y[i0];
+    double* Y1 = y[i1];
+    double* Y2 = y[i2];
+    unsigned ix = 1, iy = 2;
+    double   mu_max = (Y1[1] * Y2[2] + Y0[1] * Y1[2] + Y2[1] * Y0[2] - Y1[1] * Y0[2]
+                     - Y2[1] * Y1[2] - Y0[1] * Y2[2]);
+    double mu = (Y1[2] * Y0[0] + Y2[2] * Y1[0] + Y0[2] * Y2[0] - Y1[2] * Y2[0]
+                 - Y0[2] * Y1[0] - Y2[2] * Y0[0]);
+    if(fabs(mu) > fabs(mu_max))
+    {
+        mu_max = mu;
+        ix     = 0;
+    }
+    mu = (Y1[0] * Y2[1] + Y0[0] * Y1[1] + Y2[0] * Y0[1] - Y1[0] * Y0[1] - Y2[0] * Y1[1]
+          - Y0[0] * Y2[1]);
+    if(fabs(mu) > fabs(mu_max))
+    {
+        mu_max = mu;
+        ix     = 0;
+        iy     = 1;
+    }
+    double   C[3];
+    unsigned sc[3];
+    C[0] = (p0[ix] * Y1[iy] + p0[iy] * Y2[ix] + Y1[ix] * Y2[iy] - p0[ix] * Y2[iy]
+            - p0[iy] * Y1[ix] - Y2[ix] * Y1[iy]);
+    sc[0] = sv_same_sign(mu_max, C[0]);
+    C[1] = (p0[ix] * Y2[iy] + p0[iy] * Y0[ix] + Y2[ix] * Y0[iy] - p0[ix] * Y0[iy]
+            - p0[iy] * Y2[ix] - Y0[ix] * Y2[iy]);
+    sc[1] = sv_same_sign(mu_max, C[1]);
+    C[2] = (p0[ix] * Y0[iy] + p0[iy] * Y1[ix] + Y0[ix] * Y1[iy] - p0[ix] * Y1[iy]
+            - p0[iy] * Y0[ix] - Y1[ix] * Y0[iy]);
+    sc[2] = sv_same_sign(mu_max, C[2]);
+    if(sc[0] + sc[1] + sc[2] == 3)
+    {
+        lambdas[i0] = C[0] / mu_max;
+        lambdas[i1] = C[1] / mu_max;
+        lambdas[i2] = C[2] / mu_max;
+        return;
+    }
+    double   d        = 100000.0;
+    unsigned new_bits = 0;
+    const unsigned idx[3] = {i0, i1, i2};
+    for(unsigned j = 0; j < 3; ++j)
+        if(!sc[j])
+        {
+            unsigned new_used       = *bits & ~(1u << idx[j]);
+            double   new_lambdas[4] = {0.0, 0.0, 0.0, 0.0};
+            sv_s1d(y, &new_used, new_lambdas);
+            double       np[3];
+            const double d_star = sv_point(y, new_used, new_lambdas, np);
+            if(d_star < d)
+            {
+                new_bits = new_used;
+                d        = d_star;
+                for(unsigned i = 0; i < 4; ++i)
+                    lambdas[i] = new_lambdas[i];
+            }
+        }
+    *bits = new_bits;
+}
+
+static void sv_s3d(double y[4][3], unsigned* bits, double lambdas[4])
+{
+    /* s3d (GJK_AY.cpp:215-301) */
+    double C[4];
+    C[0] = y[3][0] * y[2][1] * y[1][2] + y[2][0] * y[1][1] * y[3][2] + y[1][0] * y[3][1] * y[2][2]
+           - y[1][0] * y[2][1] * y[3][2] - y[2][0] * y[3][1] * y[1][2]
+           - y[3][0] * y[1][1] * y[2][2];
+    C[1] = y[0][0] * y[2][1] * y[3][2] + y[2][0] * y[3][1] * y[0][2] + y[3][0] * y[0][1] * y[2][2]
+           - y[3][0] * y[2][1] * y[0][2] - y[2][0] * y[0][1] * y[3][2]
+           - y[0][0] * y[3][1] * y[2][2];
+    C[2] = y[3][0] * y[1][1] * y[0][2] + y[1][0] * y[0][1] * y[3][2] + y[0][0] * y[3][1] * y[1][2]
+           - y[0][0] * y[1][1] * y[3][2] - y[1][0] * y[3][1] * y[0][2]
+           - y[3][0] * y[0][1] * y[1][2];
+    C[3] = y[0][0] * y[1][1] * y[2][2] + y[1][0] * y[2][1] * y[0][2] + y[2][0] * y[0][1] * y[1][2]
+           - y[2][0] * y[1][1] * y[0][2] - y[1][0] * y[0][1] * y[2][2]
+           - y[0][0] * y[2][1] * y[1][2];
+    const double dM = C[0] + C[1] + C[2] + C[3];
+    unsigned     sc[4];
+    for(int i = 0; i < 4; ++i)
+        sc[i] = sv_same_sign(dM, C[i]);
+    if(sc[0] + sc[1] + sc[2] + sc[3] == 4)
+    {
+        for(int i = 0; i < 4; ++i)
+            lambdas[i] = C[i] / dM;
+        return;
+    }
+    double   d        = 100000.0;
+    unsigned new_bits = 0;
+    for(unsigned j = 0; j < 4; ++j)
+        if(!sc[j])
+        {
+            unsigned new_used       = *bits & ~(1u << j);
+            double   new_lambdas[4] = {0.0, 0.0, 0.0, 0.0};
+            sv_s2d(y, &new_used, new_lambdas);
+            double       np[3];
+            const double d_star = sv_point(y, new_used, new_lambdas, np);
+            if(d_star < d)
+            {
+                new_bits = new_used;
+                d        = d_star;
+                for(unsigned i = 0; i < 4; ++i)
+                    lambdas[i] = new_lambdas[i];
+            }
+        }
+    *bits = new_bits;
+}
+
+static void sv_subalgorithm(double y[4][3], unsigned* bits, double lambdas[4], double v[3])
+{
+    /* sv_subalgorithm (GJK_AY.cpp:340-368) */
+    unsigned num_used = 0;
+    for(unsigned i = 0; i < 4; ++i)
+        num_used += (*bits >> i) & 1u;
+    if(num_used == 1)
+    {
+        for(unsigned i = 0; i < 4; ++i)
+            if(*bits & (1u << i))
+                lambdas[i] = 1.0;
+    }
+    else if(num_used == 2)
+        sv_s1d(y, bits, lambdas);
+    else if(num_used == 3)
+        sv_s2d(y, bits, lambdas);
+    else
+        sv_s3d(y, bits, lambdas);
+    sv_point(y, *bits, lambdas, v); /* computeVector (GJK_AY.cpp:304-316) */
+}
+
+static double gjk_sv(const gb_convex* a, const double* va, const gb_convex* b,
+                     const double* vb, const double a2w[12], const double b2w[12],
+                     double pa[3], double pb[3], int* nb_iter)
+{
+    /* computeClosestPoints_GJK_AY (GJK_AY.cpp:392-469) */
+    unsigned     bits = 0, last = 0;
+    double       p[4][3], q[4][3], y[4][3], lambdas[4] = {0.0, 0.0, 0.0, 0.0};
+    int          num_iterations = 0;
+    const double rel_error      = OR_LOWEPS;
+    const double abs_error      = 1.e-4 * rel_error;
+    memset(p, 0, sizeof(p));
+    memset(q, 0, sizeof(q));
+    memset(y, 0, sizeof(y));
+    double b2a[12];
+    tr_relative(a2w, b2w, b2a);
+    double z[3] = {0.0, 0.0, 0.0}, sa[3], sb[3], tb[3], v[3], w[3];
+    convex_support(a, va, z, sa);
+    convex_support(b, vb, z, sb);
+    tr_apply(b2a, sb, tb);
+    sub3(sa, tb, v);
+    double dist = norm3(v);
+    while(bits < 15 && dist > OR_HIGHEPS && num_iterations < 1000)
+    {
+        for(unsigned k = 0; k < 4; ++k)
+            if(!(bits & (1u << k)))
+            {
+                last = k;
+                break;
+            }
+        double nv[3] = {-v[0], -v[1], -v[2]}, dir[3];
+        convex_support(a, va, nv, p[last]);
+        vec_mat(v, b2a, dir);
+        convex_support(b, vb, dir, q[last]);
+        tr_apply(b2a, q[last], tb);
+        sub3(p[last], tb, w);
+        const double mu = dist - dot3(v, w) / dist;
+        if(mu < dist * rel_error || mu < abs_error)
+            break;
+        if(jh_degenerate(bits, y, w)) /* degenerate (GJK_AY.cpp:373-386): the current simplex */
+            break;
+        copy3(w, y[last]);
+        bits |= 1u << last;
+        ++num_iterations;
+        sv_subalgorithm(y, &bits, lambdas, v);
+        dist = norm3(v);
+    }
+    /* computePoints (GJK_AY.cpp:319-337) */
+    zero3(pa);
+    zero3(pb);
+    for(unsigned i = 0; i < 4; ++i)
+        if(bits & (1u << i))
+        {
+            double t[3];
+            scal3(lambdas[i], p[i], t);
+            add3(pa, t, pa);
+            scal3(lambdas[i], q[i], t);
+            add3(pb, t, pb);
+        }
+    if(nb_iter)
+        *nb_iter = num_iterations;
+    return dist;
+}
+
+/* ===========================================================================
+ * Nesterov-accelerated GJK (no counterpart in the reference, whose GJK_JH.cpp
+ * and GJK_AY.cpp keep only commented-out momentum variables).  Restated from
+ * Montaut, Le Lidec, Petrik, Sivic and Carpentier, "Collision Detection
+ * Accelerated: An Optimization Perspective" (RSS 2022), Algorithm 2, on the
+ * signed-volume sub-algorithm above (the Johnson one's absolute determinant
+ * test stops it early on mm-size grains).  The support direction is the
+ * normalised momentum average
+ *   y_k = delta_k x_k + (1 - delta_k) s_{k-1},   delta_k = (k + 1) / (k + 3),
+ *   d_k = delta_k d_{k-1} / |d_{k-1}| + (1 - delta_k) y_k / |y_k|,
+ * of the current closest point x_k (v) and the last support point s_{k-1};
+ * x_0 = s_{-1} = d_{-1} is the first point.  The optimality gap of
+ * GJK_AY.cpp, |x_k| - x_k . s_k / |x_k|, is no certificate when s_k was taken
+ * along d_k rather than x_k (it can only understate the true gap), so when it
+ * falls below the tolerance, or s_k repeats a simplex vertex, the iteration is
+ * redone along x_k and the method continues as plain GJK, whose gap test then
+ * ends it.
+ * ======================================================================== */
+static double gjk_nesterov(const gb_convex* a, const double* va, const gb_convex* b,
+                           const double* vb, const double a2w[12], const double b2w[12],
+                           double pa[3], double pb[3], int* nb_iter)
+{
+    unsigned     bits = 0, last = 0;
+    double       p[4][3], q[4][3], y[4][3], lambdas[4] = {0.0, 0.0, 0.0, 0.0};
+    int          num_iterations = 0, momentum = 1;
+    const double rel_error = OR_LOWEPS;
+    const double abs_error = 1.e-4 * rel_error;
+    memset(p, 0, sizeof(p));
+    memset(q, 0, sizeof(q));
+    memset(y, 0, sizeof(y));
+    double b2a[12];
+    tr_relative(a2w, b2w, b2a);
+    double z[3] = {0.0, 0.0, 0.0}, sa[3], sb[3], tb[3], v[3], w[3], d[3], s_prev[3];
+    convex_support(a, va, z, sa);
+    convex_support(b, vb, z, sb);
+    tr_apply(b2a, sb, tb);
+    sub3(sa, tb, v);
+    copy3(v, d);
+    copy3(v, s_prev);
+    double dist = norm3(v);
+    while(bits < 15 && dist > OR_HIGHEPS && num_iterations < 1000)
+    {
+        for(unsigned k = 0; k < 4; ++k)
+            if(!(bits & (1u << k)))
+            {
+                last = k;
+                break;
+            }
+        if(momentum)
+        {
+            const double delta = ((double)num_iterations + 1.0) / ((double)num_iterations + 3.0);
+            double       yk[3];
+            for(int k = 0; k < 3; ++k)
+                yk[k] = delta * v[k] + (1.0 - delta) * s_prev[k];
+            const double ny = norm3(yk), nd = norm3(d);
+            if(ny > OR_HIGHEPS && nd > OR_HIGHEPS)
+                for(int k = 0; k < 3; ++k)
+                    d[k] = delta * (d[k] / nd) + (1.0 - delta) * (yk[k] / ny);
+            else
+            {
+                momentum = 0;
+                copy3(v, d);
+            }
+        }
+        else
+            copy3(v, d);
+        double nd_[3] = {-d[0], -d[1], -d[2]}, dir[3];
+        convex_support(a, va, nd_, p[last]);
+        vec_mat(d, b2a, dir);
+        convex_support(b, vb, dir, q[last]);
+        tr_apply(b2a, q[last], tb);
+        sub3(p[last], tb, w);
+        const double mu = dist - dot3(v, w) / dist;
+        if(mu < dist * rel_error || mu < abs_error || jh_degenerate(bits, y, w))
+        {
+            if(!momentum)
+                break;
+            momentum = 0; /* not a certified gap: redo this iteration along x_k */
+            continue;
+        }
+        copy3(w, y[last]);
+        bits |= 1u << last;
+        ++num_iterations;
+        sv_subalgorithm(y, &bits, lambdas, v);
+        dist = norm3(v);
+        copy3(w, s_prev);
+    }
+    zero3(pa);
+    zero3(pb);
+    for(unsigned i = 0; i < 4; ++i)
+        if(bits & (1u << i))
+        {
+            double t[3];
+            scal3(lambdas[i], p[i], t);
+            add3(pa, t, pa);
+            scal3(lambdas[i], q[i], t);
+            add3(pb, t, pb);
+        }
+    if(nb_iter)
+        *nb_iter = num_iterations;
+    return dist;
+}
+
 double or_gjk(int variant, const gb_convex* a, const double* verts_a,
               const gb_convex* b, const double* verts_b, const double a2w[12],
               const double b2w[12], double pa[3], double pb[3], int* n_iter)
 {
-    (void)variant; /* only the Johnson variant is restated so far */
+    if(variant == GB_GJK_SV)
+        return gjk_sv(a, verts_a, b, verts_b, a2w, b2w, pa, pb, n_iter);
+    if(variant == GB_GJK_NESTEROV)
+        return gjk_nesterov(a, verts_a, b, verts_b, a2w, b2w, pa, pb, n_iter);
     return gjk_jh(a, verts_a, b, verts_b, a2w, b2w, pa, pb, n_iter);
 }
 

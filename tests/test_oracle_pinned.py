@@ -163,6 +163,65 @@ def test_system_bit_exact_vs_reference(oracle, reference):
     assert np.array_equal(o.velocities(), r.velocities())
 
 
+def _random_pair(rng, offset=None):
+    kind = [abi.GB_SUPERQUADRIC, abi.GB_BOX, abi.GB_SPHERE][int(rng.integers(3))]
+    p = (list(rng.uniform(0.5e-3, 1.5e-3, 3)) + list(rng.uniform(2, 10, 2))
+         if kind == abi.GB_SUPERQUADRIC else list(rng.uniform(0.5e-3, 1.5e-3, 3)))
+    A = abi.rigid_body(kind, p, crust=5e-5, density=2500)
+    B = abi.rigid_body(abi.GB_SUPERQUADRIC,
+                       list(rng.uniform(0.5e-3, 1.5e-3, 3)) + list(rng.uniform(2, 10, 2)),
+                       crust=5e-5, density=2500)
+    ta, tb = np.zeros(12), np.zeros(12)
+    ta[:9], tb[:9] = _rot(rng), _rot(rng)
+    ta[9:] = rng.uniform(-1e-3, 1e-3, 3)
+    if offset is None:
+        tb[9:] = ta[9:] + rng.normal(size=3) * 1.6e-3
+    else:
+        u = rng.normal(size=3)
+        tb[9:] = ta[9:] + offset * u / np.linalg.norm(u)
+    return A, B, ta, tb
+
+
+def _gjk(lib, variant, A, B, ta, tb):
+    pa, pb, n = np.zeros(3), np.zeros(3), C.c_int(0)
+    d = lib.gjk(variant, C.byref(A.convex), None, C.byref(B.convex), None, abi.dptr(ta),
+                abi.dptr(tb), abi.dptr(pa), abi.dptr(pb), C.byref(n))
+    return d, pa, pb, n.value
+
+
+def test_signed_volume_gjk_bit_exact_vs_reference(oracle, reference):
+    """GB_GJK_SV restates computeClosestPoints_GJK_AY (GJK_AY.cpp:392-469)."""
+    rng = np.random.default_rng(21)
+    for _ in range(400):
+        A, B, ta, tb = _random_pair(rng)
+        d0, pa0, pb0, n0 = _gjk(oracle, abi.GB_GJK_SV, A, B, ta, tb)
+        d1, pa1, pb1, n1 = _gjk(reference, abi.GB_GJK_SV, A, B, ta, tb)
+        assert same([d0, *pa0, *pb0], [d1, *pa1, *pb1]) and n0 == n1
+
+
+def test_nesterov_gjk_converges_to_the_signed_volume_distance(oracle):
+    """Nesterov-accelerated GJK (no reference counterpart) on separated pairs:
+    the distance within the reference's relative tolerance (LOWEPS = 1e-5) of
+    the signed-volume GJK's, and witness points that realise it."""
+    rng = np.random.default_rng(22)
+    checked = 0
+    for _ in range(300):
+        A, B, ta, tb = _random_pair(rng, offset=5e-3)
+        ds, *_ = _gjk(oracle, abi.GB_GJK_SV, A, B, ta, tb)
+        dn, pa, pb, n = _gjk(oracle, abi.GB_GJK_NESTEROV, A, B, ta, tb)
+        if A.convex.type == abi.GB_SPHERE:
+            # Sphere::support(0) = radius * normalized(0) is NaN (Sphere.cpp:111-114),
+            # so every GJK of the reference starts from NaN with a sphere
+            assert ds != ds and dn != dn
+            continue
+        checked += 1
+        assert abs(dn - ds) <= 2e-5 * ds and 0 < n < 1000
+        wa = ta[:9].reshape(3, 3) @ pa + ta[9:]
+        wb = tb[:9].reshape(3, 3) @ pb + tb[9:]
+        assert abs(np.linalg.norm(wa - wb) - dn) <= 1e-9 * dn + 1e-15
+    assert checked > 150
+
+
 def test_torce_accumulation_vs_reference(oracle, reference):
     """setTorce, two detects and gravity accumulate onto one torce, which the
     move consumes (ComponentManagerCPU: addForce onto m_torce, reset in
