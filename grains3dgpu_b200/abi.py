@@ -113,6 +113,7 @@ SYSTEM_API = {
     "get_velocities": (C.c_int, [_P, _D]),
     "get_torces": (C.c_int, [_P, _D]),
     "set_torces": (C.c_int, [_P, _D]),
+    "adjoint_step": (C.c_int, [_P, _D, _D, _D]),
     "update_links": (C.c_int, [_P]),
     "detect_collision_and_compute_contact_forces": (C.c_int, [_P, _I32]),
     "add_external_forces": (C.c_int, [_P]),
@@ -150,6 +151,8 @@ ENGINE_API = {
     "synchronize": (C.c_int, [_P]),
     "set_stream": (C.c_int, [_P, _P]),
     "get_phase_times": (C.c_int, [_P, _D, _I64, C.c_int32]),
+    "save_state": (C.c_int, [_P, C.c_void_p]),
+    "load_state": (C.c_int, [_P, C.c_void_p]),
 }
 
 

@@ -1,0 +1,128 @@
+"""Differentiable trajectories: a torch.autograd.Function around the engine's
+hand-written adjoint step (gb_adjoint_step).
+
+A trajectory of n_steps maps the initial positions, velocities and angular
+velocities of the particles and the contact-law parameters (kn, en, etat,
+muc per material-pair law) to the final positions, velocities and angular
+velocities.  The forward pass stores the state every `every` steps; the
+backward pass replays each segment from its checkpoint, keeping the segment's
+states, and runs the adjoint steps backwards through it.  Device memory is
+(n_steps / every + every) states of 18 doubles per particle.
+
+Scope of the adjoint: spheres, the Hooke law with kr = 0, Rectangle walls,
+first-order explicit integration, FP64 (GB_FP64 or GB_FP64_STRICT).  The
+contacts of each step are those found at its start.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi, engine, scenes
+
+LAW_PARAMS = ("kn", "en", "etat", "muc")
+
+
+def _dp(t):
+    return C.cast(C.c_void_p(t.data_ptr()), abi._D)
+
+
+class Simulation:
+    """One engine context for a scene, with device-side state access."""
+
+    def __init__(self, scene, precision=abi.GB_FP64, device=0):
+        self.lib = engine.load()
+        self.scene = scene
+        self.sys = scenes.System(self.lib, scene, precision=precision, device=device)
+        self.n = scene.n
+        self.laws = [dict(m) for m in scene.contact_models]
+        self.dev = torch.device("cuda", device)
+
+    def _check(self, st, what):
+        if st not in (abi.GB_OK, abi.GB_E_OUT_OF_DOMAIN):
+            raise RuntimeError(f"gb_{what} returned {st}: "
+                               f"{self.lib.status_string(st).decode()}")
+
+    def save(self, out=None):
+        out = out if out is not None else torch.empty((18, self.n), dtype=torch.float64,
+                                                      device=self.dev)
+        torch.cuda.synchronize(self.dev)
+        self._check(self.lib.save_state(self.sys.ctx, C.c_void_p(out.data_ptr())), "save_state")
+        return out
+
+    def load(self, state):
+        torch.cuda.synchronize(self.dev)
+        self._check(self.lib.load_state(self.sys.ctx, C.c_void_p(state.data_ptr())), "load_state")
+
+    def set_laws(self, params):
+        """params: (n_laws, 4) tensor of kn, en, etat, muc."""
+        p = params.detach().cpu().numpy()
+        for m, row in zip(self.laws, p):
+            m.update(zip(LAW_PARAMS, map(float, row)))
+        self._check(self.lib.set_contact_models(self.sys.ctx, abi.contact_model_array(self.laws)),
+                    "set_contact_models")
+
+    def step(self, k=1):
+        self._check(self.lib.step(self.sys.ctx, k), "step")
+
+    def adjoint_step(self, adj_next, adj_prev, grad_laws):
+        torch.cuda.synchronize(self.dev)
+        self._check(self.lib.adjoint_step(self.sys.ctx, _dp(adj_next), _dp(adj_prev),
+                                          _dp(grad_laws)), "adjoint_step")
+
+    def law_tensor(self):
+        return torch.tensor([[m[k] for k in LAW_PARAMS] for m in self.laws], dtype=torch.float64)
+
+
+class Trajectory(torch.autograd.Function):
+    """(x0, v0, w0, laws) -> (x, v, w) after n_steps; x0, v0, w0 are (n, 3)
+    float64 tensors on the simulation's device, laws (n_laws, 4)."""
+
+    @staticmethod
+    def forward(ctx, sim, x0, v0, w0, laws, n_steps, every):
+        sim.set_laws(laws)
+        state = sim.save()
+        state[0:3] = x0.detach().T
+        state[12:15] = v0.detach().T
+        state[15:18] = w0.detach().T
+        sim.load(state)
+        checkpoints = []
+        for t in range(n_steps):
+            if t % every == 0:
+                checkpoints.append(sim.save())
+            sim.step(1)
+        final = sim.save()
+        ctx.sim, ctx.n_steps, ctx.every, ctx.checkpoints = sim, n_steps, every, checkpoints
+        ctx.n_laws = laws.shape[0]
+        ctx.laws_device = laws.device
+        return final[0:3].T.clone(), final[12:15].T.clone(), final[15:18].T.clone()
+
+    @staticmethod
+    def backward(ctx, gx, gv, gw):
+        sim, n = ctx.sim, ctx.sim.n
+        dev = sim.dev
+        z = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+        adj = torch.cat([(g if g is not None else z).T for g in (gx, gv, gw)]).contiguous()
+        prev = torch.empty_like(adj)
+        grad = torch.zeros(4 * ctx.n_laws, dtype=torch.float64, device=dev)
+        seg_states = [torch.empty((18, n), dtype=torch.float64, device=dev)
+                      for _ in range(ctx.every)]
+        for seg in reversed(range(len(ctx.checkpoints))):
+            t0 = seg * ctx.every
+            t1 = min(t0 + ctx.every, ctx.n_steps)
+            sim.load(ctx.checkpoints[seg])
+            for t in range(t0, t1):
+                sim.save(seg_states[t - t0])
+                if t + 1 < t1:
+                    sim.step(1)
+            for t in reversed(range(t0, t1)):
+                sim.load(seg_states[t - t0])
+                sim.adjoint_step(adj, prev, grad)
+                adj, prev = prev, adj
+        torch.cuda.synchronize(dev)
+        return (None, adj[0:3].T.clone(), adj[3:6].T.clone(), adj[6:9].T.clone(),
+                grad.view(ctx.n_laws, 4).to(ctx.laws_device), None, None)
+
+
+def trajectory(sim, x0, v0, w0, laws, n_steps, every=10):
+    return Trajectory.apply(sim, x0, v0, w0, laws, n_steps, every)

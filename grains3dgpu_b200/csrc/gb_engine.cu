@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "gb_io.cuh"
+#include "gb_adjoint.cuh"
 #include "gb_step.cuh"
 
 using namespace gb;
@@ -169,6 +170,9 @@ struct gb_ctx
     int64_t     launches = 0;
     // staging buffer for the host layouts (12 doubles per particle)
     double* d_stage = nullptr;
+    // adjoint scratch: force/torque adjoints (6n) and block partial sums
+    double* d_adj   = nullptr;
+    size_t  adj_cap = 0;
 };
 
 namespace
@@ -1088,7 +1092,7 @@ int gb_destroy(gb_ctx* c)
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_done,
                     c->d_contacts,
-                    c->d_stage};
+                    c->d_stage,     c->d_adj};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);
@@ -1442,6 +1446,108 @@ int gb_step(gb_ctx* c, int32_t n_steps)
         return GB_E_INVALID_ARG;
     GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), c->stream));
     return run_steps(c, n_steps, PHASE_STEP, nullptr);
+}
+
+// ---- differentiable stepping (no counterpart in the reference) ----------------
+int gb_save_state(gb_ctx* c, double* dst)
+{
+    if(!c || !dst)
+        return GB_E_INVALID_ARG;
+    if(c->prec == GB_MIXED)
+        return GB_E_UNSUPPORTED;
+    const size_t n = c->n;
+    cudaStream_t s = c->stream;
+    GB_CK(cudaMemcpyAsync(dst, c->d_pos, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(dst + 3 * n, c->d_rot, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(dst + 12 * n, c->d_vel, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(dst + 15 * n, c->d_omg, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaStreamSynchronize(s));
+    return GB_OK;
+}
+
+int gb_load_state(gb_ctx* c, const double* src)
+{
+    if(!c || !src)
+        return GB_E_INVALID_ARG;
+    if(c->prec == GB_MIXED)
+        return GB_E_UNSUPPORTED;
+    const size_t n = c->n;
+    cudaStream_t s = c->stream;
+    GB_CK(cudaMemcpyAsync(c->d_pos, src, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_rot, src + 3 * n, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_vel, src + 12 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_omg, src + 15 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaStreamSynchronize(s));
+    c->tr_set = c->vel_set = true;
+    c->links_valid = c->detect_valid = c->mask_valid = false;
+    return GB_OK;
+}
+
+int gb_adjoint_step(gb_ctx* c, const double* adj_next, double* adj_prev, double* grad_laws)
+{
+    GB_TRY(ready(c));
+    if(!adj_next || !adj_prev || !grad_laws)
+        return GB_E_INVALID_ARG;
+    const int nl = c->nmat * (c->nmat + 1) / 2;
+    if(c->prec == GB_MIXED || c->cfg.contact_law != GB_LAW_HOOKE
+       || c->cfg.integrator != GB_FIRST_ORDER_EXPLICIT || nl > kAdjMaxLaws)
+        return GB_E_UNSUPPORTED;
+    for(const auto& rb : c->rbs)
+        if(rb.convex.type != GB_SPHERE)
+            return GB_E_UNSUPPORTED;
+    for(const auto& ob : c->obs)
+        if(ob.convex.type != GB_RECTANGLE)
+            return GB_E_UNSUPPORTED;
+    AdjLaws laws{};
+    laws.n = nl;
+    for(int l = 0; l < nl; ++l)
+    {
+        const gb_contact_model& m = c->laws[l];
+        if(m.kr != 0.0)
+            return GB_E_UNSUPPORTED;
+        const double pi = 3.14159265358979323846, L = std::log(m.en), q = pi * pi + L * L;
+        laws.l[l] = {m.kn, m.en, m.etat, m.muc, L / std::sqrt(q), pi * pi / (q * std::sqrt(q)) / m.en};
+    }
+    const int    n  = c->n;
+    const int    nb = std::max(1, blocks(n, kBlock));
+    cudaStream_t s  = c->stream;
+    if(!c->d_adj || c->adj_cap < (size_t)(6 * n + nb * 4 * kAdjMaxLaws))
+    {
+        dfree(c->d_adj);
+        c->adj_cap = (size_t)6 * n + (size_t)nb * 4 * kAdjMaxLaws;
+        GB_TRY(dalloc(&c->d_adj, c->adj_cap));
+    }
+    // the contacts of the current state; the accumulated torces are kept aside
+    GB_TRY(ensure_stage(c));
+    GB_CK(cudaMemcpyAsync(c->d_stage, c->d_frc, 3 * (size_t)n * sizeof(double),
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_stage + 3 * (size_t)n, c->d_trq, 3 * (size_t)n * sizeof(double),
+                          cudaMemcpyDeviceToDevice, s));
+    const bool dirty = c->torce_dirty;
+    c->torce_dirty   = false;
+    GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    const int st = run_steps(c, 1, PHASE_DETECT, nullptr);
+    if(st != GB_OK && st != GB_E_OUT_OF_DOMAIN)
+        return st;
+    const State<double> state = state_of<double>(c);
+    const auto*         in    = (const RBInertia<double>*)c->d_inertia;
+    double*             lft   = c->d_adj;
+    double*             part  = c->d_adj + 6 * (size_t)n;
+    k_adj_integrate<<<nb, kBlock, 0, s>>>(n, c->cfg.dt, state, in, adj_next, adj_prev, lft);
+    k_adj_contacts<<<nb, kBlock, 0, s>>>(n, state, (const RBShape<double>*)c->d_shape, in,
+                                         c->d_off[c->cur], c->d_pb[c->cur], c->d_pc, lft,
+                                         c->d_obs_tr, (const RBShape<double>*)c->d_obs_shape,
+                                         laws, adj_prev, part);
+    k_adj_reduce<<<1, 4 * kAdjMaxLaws, 0, s>>>(nb, 4 * nl, part, grad_laws);
+    c->launches += 3;
+    GB_CK(cudaGetLastError());
+    GB_CK(cudaMemcpyAsync(c->d_frc, c->d_stage, 3 * (size_t)n * sizeof(double),
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_trq, c->d_stage + 3 * (size_t)n, 3 * (size_t)n * sizeof(double),
+                          cudaMemcpyDeviceToDevice, s));
+    c->torce_dirty = dirty;
+    GB_CK(cudaStreamSynchronize(s));
+    return st;
 }
 
 int gb_synchronize(gb_ctx* c)

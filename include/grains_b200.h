@@ -210,6 +210,20 @@ int gb_get_torces(gb_ctx* ctx, double* torce);
  * the next move consumes and resets them, as in ComponentManagerCPU. */
 int gb_set_torces(gb_ctx* ctx, const double* torce);
 
+/* ---- differentiable stepping (no counterpart in the reference) ------------------
+ * FP64 modes only.  A state is 18 rows of n doubles on the device: position
+ * (3), Transform3 basis (9, row-major), velocity (3), angular velocity (3). */
+int gb_save_state(gb_ctx* ctx, double* dst_device);
+int gb_load_state(gb_ctx* ctx, const double* src_device);
+/* Reverse-mode derivative of one step from the current state s, for spheres,
+ * GB_LAW_HOOKE with kr = 0, GB_FIRST_ORDER_EXPLICIT and Rectangle walls
+ * (GB_E_UNSUPPORTED otherwise).  adj_next = dL/ds' and adj_prev = dL/ds are
+ * 9 rows of n doubles on the device (position, velocity, angular velocity);
+ * dL/dtheta is added to grad_laws (device, 4 doubles per contact law: kn, en,
+ * etat, muc).  The contacts are those found at s; the state and the torces
+ * are left as they were. */
+int gb_adjoint_step(gb_ctx* ctx, const double* adj_next, double* adj_prev, double* grad_laws);
+
 /* ---- the time step: the ComponentManager hot-path calls ---------------------- */
 /* ComponentManager::updateLinks (ComponentManagerCPU.cpp:278-296). */
 int gb_update_links(gb_ctx* ctx);

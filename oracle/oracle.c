@@ -2524,3 +2524,275 @@ int or_debug_dump(or_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
     *count = avail;
     return GB_OK;
 }
+
+/* ===========================================================================
+ * Adjoint of one time step (NEW: the reference has no differentiation).
+ *
+ * Scope: spheres, the Hooke law with kr = 0 (normal spring-dashpot,
+ * tangential viscous force capped by Coulomb friction), Rectangle walls,
+ * gravity, first-order explicit integration, in FP64.  The step maps the
+ * state s = (x, v, omega) of every particle to s' = Phi(s, theta), with
+ * theta = (kn, en, etat, muc) per material-pair law; the set of contacts is
+ * the one found at s (frozen for the step).  For spheres the contact
+ * geometry (overlap, normal, point) is a closed-form function of the centres
+ * (closest_spheres / closest_rectangle above), so this is the exact
+ * derivative of the step wherever the contact set does not change.  The
+ * orientation of a sphere does not enter its forces and is not carried.
+ *
+ * Layout of a state adjoint: 9 rows of n doubles (x, y, z of the position,
+ * of the velocity, of the angular velocity).
+ * ======================================================================== */
+static double hooke_en_coef_grad(double en)
+{
+    /* d/den of log(en) / sqrt(pi^2 + log(en)^2) */
+    const double L = log(en), s = OR_PI * OR_PI + L * L;
+    return OR_PI * OR_PI / (s * sqrt(s)) / en;
+}
+
+/* Reverse of hooke_forces for one contact: given the gradients lf of the
+   force and lt of the torque arm x f, the gradients of vec, the contact
+   point, the arm, both bodies' velocities and the law's parameters. */
+static void hooke_vjp(const gb_contact_model* cm, double avmass, double omega0,
+                      const double vec[3], const double pt[3], const double arm[3],
+                      const double vA[3], const double wA[3], const double vB[3],
+                      const double wB[3], const double lf[3], const double lt[3],
+                      double g_vec[3], double g_pt[3], double g_arm[3], double g_vA[3],
+                      double g_wA[3], double g_vB[3], double g_wB[3], double g_law[4])
+{
+    /* forward (the operations of hooke_forces, in plain FP64) */
+    const double np = norm3(vec);
+    double       n[3], rel[3], t[3], c1[3], c2[3];
+    scal3(1.0 / np, vec, n);
+    cross3(wA, pt, c1);
+    cross3(wB, pt, c2);
+    for(int k = 0; k < 3; ++k)
+        rel[k] = vA[k] + c1[k] - vB[k] - c2[k];
+    const double rn = dot3(rel, n);
+    double       vn[3], vt[3], th[3] = {0, 0, 0};
+    scal3(rn, n, vn);
+    sub3(rel, vn, vt);
+    const double nvt = norm3(vt);
+    if(nvt > OR_EPS)
+        scal3(1.0 / nvt, vt, th);
+    const double c  = hooke_muen(cm->en);
+    double       FN[3];
+    for(int k = 0; k < 3; ++k)
+        FN[k] = cm->kn * vec[k] + 2.0 * omega0 * c * avmass * vn[k];
+    const double nFN = norm3(FN);
+    double       FT[3];
+    scal3(-2.0 * cm->etat * avmass, vt, FT);
+    const double fn = cm->muc * nFN, ft = norm3(FT);
+    const int    capped = fn < ft;
+    if(capped)
+        scal3(-fn, th, FT);
+    double f[3];
+    add3(FN, FT, f);
+    /* reverse */
+    double gf[3], gFN[3], gvt[3] = {0, 0, 0}, gvn[3], grel[3], gn[3];
+    cross3(lt, arm, t);
+    add3(lf, t, gf);
+    cross3(f, lt, g_arm);
+    copy3(gf, gFN);
+    double g_nFN = 0.0;
+    if(capped)
+    {
+        const double tg = dot3(th, gf);
+        g_law[3] += -nFN * tg;
+        g_nFN = -cm->muc * tg;
+        if(nvt > OR_EPS)
+        {
+            double gth[3];
+            scal3(-fn, gf, gth);
+            const double a = dot3(gth, th);
+            for(int k = 0; k < 3; ++k)
+                gvt[k] = (gth[k] - a * th[k]) / nvt;
+        }
+    }
+    else
+    {
+        scal3(-2.0 * cm->etat * avmass, gf, gvt);
+        g_law[2] += -2.0 * avmass * dot3(vt, gf);
+    }
+    if(nFN > 0.0)
+        for(int k = 0; k < 3; ++k)
+            gFN[k] += g_nFN * FN[k] / nFN;
+    g_law[0] += dot3(vec, gFN) + omega0 / (2.0 * cm->kn) * 2.0 * c * avmass * dot3(vn, gFN);
+    g_law[1] += 2.0 * omega0 * avmass * dot3(vn, gFN) * hooke_en_coef_grad(cm->en);
+    scal3(cm->kn, gFN, g_vec);
+    scal3(2.0 * omega0 * c * avmass, gFN, gvn);
+    copy3(gvt, grel);
+    sub3(gvn, gvt, gvn);
+    const double ngvn = dot3(n, gvn);
+    for(int k = 0; k < 3; ++k)
+    {
+        grel[k] += ngvn * n[k];
+        gn[k] = rn * gvn[k] + ngvn * rel[k];
+    }
+    const double ngn = dot3(n, gn);
+    for(int k = 0; k < 3; ++k)
+        g_vec[k] += (gn[k] - ngn * n[k]) / np;
+    copy3(grel, g_vA);
+    scal3(-1.0, grel, g_vB);
+    cross3(pt, grel, g_wA);
+    scal3(-1.0, g_wA, g_wB);
+    double dw[3];
+    sub3(wA, wB, dw);
+    cross3(grel, dw, g_pt);
+}
+
+static int adjoint_supported(const or_ctx* c)
+{
+    if(c->cfg.contact_law != GB_LAW_HOOKE || c->cfg.integrator != GB_FIRST_ORDER_EXPLICIT)
+        return 0;
+    for(int i = 0; i < c->nrb; ++i)
+        if(c->rbs[i].convex.type != GB_SPHERE)
+            return 0;
+    for(int o = 0; o < c->nob; ++o)
+        if(c->obs[o].convex.type != GB_RECTANGLE)
+            return 0;
+    const int nl = c->nmat * (c->nmat + 1) / 2;
+    for(int l = 0; l < nl; ++l)
+        if(c->cm[l].kr != 0.0)
+            return 0;
+    return 1;
+}
+
+static int law_index(int ma, int mb)
+{
+    const int s = ma < mb ? ma : mb, l = ma < mb ? mb : ma;
+    return l * (l + 1) / 2 + s;
+}
+
+int or_adjoint_step(or_ctx* c, const double* adj_next, double* adj_prev, double* grad_laws)
+{
+    if(!c || !adj_next || !adj_prev || !grad_laws)
+        return GB_E_INVALID_ARG;
+    if(!adjoint_supported(c))
+        return GB_E_UNSUPPORTED;
+    const int    n  = c->n;
+    const double dt = c->cfg.dt;
+#define ADJ(r, i) adj_prev[(size_t)(r) * n + (i)]
+#define NXT(r, i) adj_next[(size_t)(r) * n + (i)]
+    /* integration: x' = x + dt v, v' = v + dt F / m, omega' = omega + dt T / I */
+    double* lF = xcalloc((size_t)6 * n, sizeof(double));
+    for(int i = 0; i < n; ++i)
+    {
+        const gb_rigid_body_props* rb = c->rbp + c->rb_id[i];
+        for(int k = 0; k < 3; ++k)
+        {
+            ADJ(k, i)         = NXT(k, i);
+            ADJ(3 + k, i)     = NXT(3 + k, i) + dt * NXT(k, i);
+            ADJ(6 + k, i)     = NXT(6 + k, i);
+            lF[6 * i + k]     = dt / rb->mass * NXT(3 + k, i);
+            lF[6 * i + 3 + k] = dt * rb->inertia_inv[0] * NXT(6 + k, i);
+        }
+    }
+    /* contacts at s, each on its first particle */
+    for(int a = 0; a < n; ++a)
+    {
+        const gb_rigid_body_props* pa = c->rbp + c->rb_id[a];
+        const double               rA = c->rbs[c->rb_id[a]].convex.p[0];
+        const int                  ma = c->rbs[c->rb_id[a]].material;
+        const double*              xa = c->tr + 12 * a + 9;
+        double vA[3], wA[3], gx[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+        copy3(c->kin + 6 * a, vA);
+        copy3(c->kin + 6 * a + 3, wA);
+        const double* lf = lF + 6 * a;
+        const double* lt = lF + 6 * a + 3;
+        for(int b = 0; b < n; ++b)
+        {
+            if(b == a)
+                continue;
+            const gb_rigid_body_props* pb = c->rbp + c->rb_id[b];
+            const double               rB = c->rbs[c->rb_id[b]].convex.p[0];
+            const double*              xb = c->tr + 12 * b + 9;
+            double                     d[3];
+            sub3(xb, xa, d);
+            const double dn = norm3(d), delta = dn - rA - rB;
+            if(!(delta < 0.0))
+                continue;
+            double u[3], vec[3], pt[3], arm[3];
+            scal3(1.0 / dn, d, u);
+            scal3(delta, u, vec);
+            for(int k = 0; k < 3; ++k)
+                pt[k] = xa[k] + (rA + 0.5 * delta) * u[k];
+            sub3(pt, xa, arm);
+            const gb_contact_model* cm = c->cm + law_index(ma, c->rbs[c->rb_id[b]].material);
+            const double            avm = pa->mass * pb->mass / (pa->mass + pb->mass);
+            const double            w0  = sqrt(cm->kn / avm);
+            double gvec[3], gpt[3], garm[3], gvA[3], gwA[3], gvB[3], gwB[3];
+            hooke_vjp(cm, avm, w0, vec, pt, arm, vA, wA, c->kin + 6 * b, c->kin + 6 * b + 3, lf, lt,
+                      gvec, gpt, garm, gvA, gwA, gvB, gwB,
+                      grad_laws + 4 * law_index(ma, c->rbs[c->rb_id[b]].material));
+            /* geometry: pt = xa + (rA + delta/2) u, vec = delta u, arm = pt - xa */
+            for(int k = 0; k < 3; ++k)
+            {
+                gpt[k] += garm[k];
+                gx[k] -= garm[k];
+                gx[k] += gpt[k];
+            }
+            const double gdelta = 0.5 * dot3(u, gpt) + dot3(u, gvec);
+            double       gu[3], gd[3];
+            for(int k = 0; k < 3; ++k)
+                gu[k] = (rA + 0.5 * delta) * gpt[k] + delta * gvec[k];
+            const double ugu = dot3(u, gu);
+            for(int k = 0; k < 3; ++k)
+                gd[k] = (gu[k] - ugu * u[k]) / dn + gdelta * u[k];
+            for(int k = 0; k < 3; ++k)
+            {
+                gx[k] -= gd[k];
+                ADJ(k, b) += gd[k];
+                gv[k] += gvA[k];
+                gw[k] += gwA[k];
+                ADJ(3 + k, b) += gvB[k];
+                ADJ(6 + k, b) += gwB[k];
+            }
+        }
+        for(int o = 0; o < c->nob; ++o)
+        {
+            const double* ot = c->obs_tr + 12 * o;
+            double        rn[3] = {ot[2], ot[5], ot[8]}, e[3];
+            sub3(xa, ot + 9, e);
+            scal3(copysign(1.0, dot3(rn, e)), rn, rn);
+            const double h = dot3(rn, e), s = h - rA;
+            if(!(s < 0.0))
+                continue;
+            double vec[3], pt[3], arm[3];
+            scal3(-s, rn, vec);
+            for(int k = 0; k < 3; ++k)
+                pt[k] = xa[k] - rA * rn[k] - 0.5 * s * rn[k];
+            sub3(pt, xa, arm);
+            const int               mo  = c->obs[o].material;
+            const gb_contact_model* cm  = c->cm + law_index(ma, mo);
+            const double            avm = 0.5 * pa->mass; /* obstacle mass 0: HookeContactForceModel's rule */
+            const double            w0  = 2.0 * sqrt(cm->kn / avm);
+            const double            z[3] = {0, 0, 0};
+            double gvec[3], gpt[3], garm[3], gvA[3], gwA[3], gvB[3], gwB[3];
+            hooke_vjp(cm, avm, w0, vec, pt, arm, vA, wA, z, z, lf, lt, gvec, gpt, garm, gvA, gwA,
+                      gvB, gwB, grad_laws + 4 * law_index(ma, mo));
+            /* pt = xa - rA rn - s rn / 2, vec = -s rn, s = rn . (xa - o) - rA */
+            for(int k = 0; k < 3; ++k)
+            {
+                gpt[k] += garm[k];
+                gx[k] += gpt[k] - garm[k];
+            }
+            const double gs = -dot3(rn, gvec) - 0.5 * dot3(rn, gpt);
+            for(int k = 0; k < 3; ++k)
+            {
+                gx[k] += gs * rn[k];
+                gv[k] += gvA[k];
+                gw[k] += gwA[k];
+            }
+        }
+        for(int k = 0; k < 3; ++k)
+        {
+            ADJ(k, a) += gx[k];
+            ADJ(3 + k, a) += gv[k];
+            ADJ(6 + k, a) += gw[k];
+        }
+    }
+    free(lF);
+#undef ADJ
+#undef NXT
+    return GB_OK;
+}

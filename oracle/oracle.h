@@ -80,6 +80,10 @@ int or_get_transforms(or_ctx* ctx, double* transforms);
 int or_get_velocities(or_ctx* ctx, double* kin);
 int or_get_torces(or_ctx* ctx, double* torce);
 int or_set_torces(or_ctx* ctx, const double* torce);
+/* Adjoint of one step from the current state (spheres, Hooke, first order):
+   adj_next, adj_prev: 9 x n (position, velocity, angular velocity rows);
+   grad_laws: 4 per law (kn, en, etat, muc), accumulated. */
+int or_adjoint_step(or_ctx* ctx, const double* adj_next, double* adj_prev, double* grad_laws);
 int or_update_links(or_ctx* ctx);
 int or_detect_collision_and_compute_contact_forces(or_ctx* ctx, int32_t* result);
 int or_add_external_forces(or_ctx* ctx);
