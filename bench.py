@@ -173,6 +173,69 @@ def e2e_engine(sysm, steps, torch):
     return e0.elapsed_time(e1) / 1e3, wall, n * 18 * 8, n * 18 * 8
 
 
+def adjoint_box(n, pitch=2.05e-3, margin=1.6e-3, layers=100):
+    """A closed box whose lattice holds n sphere-bed sites in about `layers`
+    layers, with 30 mm of headroom."""
+    m = int(np.ceil(np.sqrt(n / layers)))
+    nz = int(np.ceil(n / (m * m)))
+    side = 2 * margin + (m - 0.5) * pitch
+    return (side, side, 2 * margin + (nz - 0.5) * pitch + 0.03)
+
+
+def measure_adjoint(torch, n, steps):
+    """Cost of the adjoint against the forward on the sphere bed in FP64:
+    the plain forward (one gb_step call of `steps` steps), the checkpointed
+    trajectory's forward, and its backward (segment replays + adjoint steps),
+    each timed with CUDA events on the engine's stream."""
+    from grains3dgpu_b200 import adjoint
+    scene = scenes.sphere_bed(seed=4, n=n, box=adjoint_box(n))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sim = adjoint.Simulation(scene, precision=abi.GB_FP64, device=dev.index)
+    stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    state0 = sim.save()
+    sim.step(3)
+    sim.load(state0)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1) / steps
+    contacts = sim.sys.stats().contacts
+    rng = np.random.default_rng(5)
+    wts = [torch.tensor(rng.normal(size=(n, 3)), device=dev) for _ in range(3)]
+    every = adjoint.checkpoint_interval(sim, steps)
+
+    def run():
+        x0 = torch.tensor(scene.transforms[:, 9:], device=dev, requires_grad=True)
+        v0 = torch.tensor(scene.velocities[:, :3], device=dev, requires_grad=True)
+        w0 = torch.tensor(scene.velocities[:, 3:], device=dev, requires_grad=True)
+        laws = sim.law_tensor().requires_grad_(True)
+        torch.cuda.synchronize()
+        a, b, c = ev(), ev(), ev()
+        a.record(stream)
+        out = adjoint.trajectory(sim, x0, v0, w0, laws, steps, every)
+        loss = sum((w * s).sum() for w, s in zip(wts, out))
+        b.record(stream)
+        loss.backward()
+        c.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps, b.elapsed_time(c) / steps
+
+    run()
+    t_fwd, t_bwd = run()
+    sim.sys.close()
+    return {"workload": f"{n:,} spheres r=1.1 mm on a 2.05 mm lattice (all lattice neighbours "
+                        "in contact) settling in a closed box, Hooke law etat=3000 muc=0.05, "
+                        "first-order explicit, FP64",
+            "n_particles": n, "contacts_per_step": int(contacts), "steps": steps,
+            "checkpoint_every": every, "forward_ms_per_step": t_plain,
+            "trajectory_forward_ms_per_step": t_fwd, "backward_ms_per_step": t_bwd,
+            "adjoint_over_forward": t_bwd / t_plain}
+
+
 def force_error(scene, torch):
     """Single-step force error of the mixed mode against the FP64 mode from
     one identical state: max |F_mixed - F_fp64| over particles divided by
@@ -322,6 +385,9 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=20_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint-n", type=int, default=1_000_000)
+    ap.add_argument("--adjoint-steps", type=int, default=10)
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -377,6 +443,10 @@ def main():
     value64 = aggregate(world, scene.n, args.fp64_steps, t64)
     ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
 
+    adj = None
+    if world == 1 and not args.no_adjoint:
+        adj = measure_adjoint(torch, args.adjoint_n, args.adjoint_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = time_reference(scene, args.ref_sample, args.cpu_seconds, cell=st.cell_size)
@@ -405,6 +475,7 @@ def main():
                      "steps": args.fp64_steps},
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
+            "adjoint": adj,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

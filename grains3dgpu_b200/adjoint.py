@@ -7,7 +7,9 @@ muc per material-pair law) to the final positions, velocities and angular
 velocities.  The forward pass stores the state every `every` steps; the
 backward pass replays each segment from its checkpoint, keeping the segment's
 states, and runs the adjoint steps backwards through it.  Device memory is
-(n_steps / every + every) states of 18 doubles per particle.
+(n_steps / every + every - 1) states of 18 doubles per particle; with
+every = 1 (the default while the states fit in a quarter of the free device
+memory) nothing is replayed.
 
 Scope of the adjoint: spheres, the Hooke law with kr = 0, Rectangle walls,
 first-order explicit integration, FP64 (GB_FP64 or GB_FP64_STRICT).  The
@@ -37,6 +39,11 @@ class Simulation:
         self.n = scene.n
         self.laws = [dict(m) for m in scene.contact_models]
         self.dev = torch.device("cuda", device)
+        # the engine works on torch's current stream, so that the state
+        # tensors written by torch and the engine's copies are ordered
+        stream = torch.cuda.current_stream(self.dev)
+        self._check(self.lib.set_stream(self.sys.ctx, C.c_void_p(stream.cuda_stream)),
+                    "set_stream")
 
     def _check(self, st, what):
         if st not in (abi.GB_OK, abi.GB_E_OUT_OF_DOMAIN):
@@ -46,12 +53,10 @@ class Simulation:
     def save(self, out=None):
         out = out if out is not None else torch.empty((18, self.n), dtype=torch.float64,
                                                       device=self.dev)
-        torch.cuda.synchronize(self.dev)
         self._check(self.lib.save_state(self.sys.ctx, C.c_void_p(out.data_ptr())), "save_state")
         return out
 
     def load(self, state):
-        torch.cuda.synchronize(self.dev)
         self._check(self.lib.load_state(self.sys.ctx, C.c_void_p(state.data_ptr())), "load_state")
 
     def set_laws(self, params):
@@ -66,7 +71,6 @@ class Simulation:
         self._check(self.lib.step(self.sys.ctx, k), "step")
 
     def adjoint_step(self, adj_next, adj_prev, grad_laws):
-        torch.cuda.synchronize(self.dev)
         self._check(self.lib.adjoint_step(self.sys.ctx, _dp(adj_next), _dp(adj_prev),
                                           _dp(grad_laws)), "adjoint_step")
 
@@ -89,7 +93,7 @@ class Trajectory(torch.autograd.Function):
         checkpoints = []
         for t in range(n_steps):
             if t % every == 0:
-                checkpoints.append(sim.save())
+                checkpoints.append(state if t == 0 else sim.save())
             sim.step(1)
         final = sim.save()
         ctx.sim, ctx.n_steps, ctx.every, ctx.checkpoints = sim, n_steps, every, checkpoints
@@ -106,17 +110,19 @@ class Trajectory(torch.autograd.Function):
         prev = torch.empty_like(adj)
         grad = torch.zeros(4 * ctx.n_laws, dtype=torch.float64, device=dev)
         seg_states = [torch.empty((18, n), dtype=torch.float64, device=dev)
-                      for _ in range(ctx.every)]
+                      for _ in range(ctx.every - 1)]
         for seg in reversed(range(len(ctx.checkpoints))):
             t0 = seg * ctx.every
             t1 = min(t0 + ctx.every, ctx.n_steps)
-            sim.load(ctx.checkpoints[seg])
-            for t in range(t0, t1):
-                sim.save(seg_states[t - t0])
-                if t + 1 < t1:
+            # the segment's states: its checkpoint, then the replayed steps
+            states = [ctx.checkpoints[seg]]
+            if t1 - t0 > 1:
+                sim.load(states[0])
+                for t in range(t0 + 1, t1):
                     sim.step(1)
+                    states.append(sim.save(seg_states[t - t0 - 1]))
             for t in reversed(range(t0, t1)):
-                sim.load(seg_states[t - t0])
+                sim.load(states[t - t0])
                 sim.adjoint_step(adj, prev, grad)
                 adj, prev = prev, adj
         torch.cuda.synchronize(dev)
@@ -124,5 +130,23 @@ class Trajectory(torch.autograd.Function):
                 grad.view(ctx.n_laws, 4).to(ctx.laws_device), None, None)
 
 
-def trajectory(sim, x0, v0, w0, laws, n_steps, every=10):
+def checkpoint_interval(sim, n_steps, budget_fraction=0.25):
+    """The smallest checkpoint interval whose states (n_steps / every
+    checkpoints plus every - 1 replayed states, 144 bytes per particle each)
+    fit in `budget_fraction` of the device's free memory: every step is kept
+    while that fits, so the backward pass replays nothing."""
+    free, _ = torch.cuda.mem_get_info(sim.dev)
+    per_state = 18 * 8 * sim.n
+    budget = budget_fraction * free
+    for every in range(1, n_steps + 1):
+        if (-(-n_steps // every) + every - 1) * per_state <= budget:
+            return every
+    return n_steps
+
+
+def trajectory(sim, x0, v0, w0, laws, n_steps, every=None):
+    """(x, v, w) after n_steps from (x0, v0, w0) under `laws`, differentiable
+    in all four; `every` is the checkpoint interval (None: checkpoint_interval)."""
+    if every is None:
+        every = checkpoint_interval(sim, n_steps)
     return Trajectory.apply(sim, x0, v0, w0, laws, n_steps, every)

@@ -430,7 +430,7 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_slot, (size_t)n * kPairSlots));
     GB_TRY(dalloc(&c->d_sorted_of, n));
     GB_TRY(dalloc(&c->d_obsmask_id, n));
-    GB_TRY(dalloc(&c->d_count, n + 1));
+    GB_TRY(dalloc(&c->d_count, 2 * ((size_t)n + 1))); // count by id, then slot index by sorted position
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
     GB_TRY(dalloc(&c->d_counters, 4));
@@ -659,9 +659,10 @@ int build_pairs(gb_ctx* c)
         GB_CK(cudaGetLastError());
         c->mask_valid = true;
     }
+    GB_CK(cudaMemsetAsync(c->d_count, 0, 2 * ((size_t)n + 1) * sizeof(uint32_t), s));
     k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
                                           c->dims[0], c->dims[1], c->dims[2], c->d_count,
-                                          c->d_slot, c->d_obsmask_id, c->nob);
+                                          c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));

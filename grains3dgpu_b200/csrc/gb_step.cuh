@@ -281,6 +281,68 @@ GB_D int obstacle_candidates(uint32_t mask, int n_obs)
     return __popc(mask) + (n_obs > kMaskObstacles ? n_obs - kMaskObstacles : 0);
 }
 
+template <typename S>
+GB_D constexpr bool is_strict()
+{
+    return std::is_same<S, dstrict>::value;
+}
+
+// The candidate test of sorted particles a and b: |d| - (rA + rB) < 0 in
+// FP64 (ComponentManagerCPU.cpp:372-380; the strict mode in the reference's
+// operation order), behind the FP32 pre-test of the mixed mode, whose
+// rejection is certified (k_gather_sorted inflates the FP32 radii).  The
+// products and sums are written as explicit round-to-nearest operations, so
+// that every kernel that enumerates candidates -- the count pass and the
+// re-enumeration of the fill pass -- takes the same decisions.
+template <bool PRE32>
+GB_D bool pretest_rejects(const float4& a32, const float4& q)
+{
+    if constexpr(PRE32)
+    {
+        const float fx = __fsub_rn(q.x, a32.x), fy = __fsub_rn(q.y, a32.y);
+        const float fz = __fsub_rn(q.z, a32.z), fr = __fadd_rn(a32.w, q.w);
+        return __fmaf_rn(fz, fz, __fmaf_rn(fy, fy, __fmul_rn(fx, fx))) >= __fmul_rn(fr, fr);
+    }
+    else
+        return false;
+}
+
+template <bool STRICT>
+GB_D bool exact_hit(const double4& pa, const double4& pb)
+{
+    if constexpr(STRICT)
+    {
+        const dstrict dx = dstrict(pb.x) - dstrict(pa.x);
+        const dstrict dy = dstrict(pb.y) - dstrict(pa.y);
+        const dstrict dz = dstrict(pb.z) - dstrict(pa.z);
+        return s_sqrt(dx * dx + dy * dy + dz * dz) - (dstrict(pa.w) + dstrict(pb.w))
+               < dstrict(0.0);
+    }
+    else
+    {
+        const double dx = __dsub_rn(pb.x, pa.x), dy = __dsub_rn(pb.y, pa.y);
+        const double dz = __dsub_rn(pb.z, pa.z), r = __dadd_rn(pa.w, pb.w);
+        return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx))) < __dmul_rn(r, r);
+    }
+}
+
+// The 27 neighbour cells of cell (cx, cy, cz) in the reference's enumeration
+// order (LinkedCell.cpp:66-112, k then j then i) are 9 rows of up to 3 cells;
+// the cells of a row are consecutive keys, so each row is one contiguous
+// range [begin, end) of sorted positions.
+GB_D void neighbour_row(const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
+                        int cx, int cy, int cz, int r, uint32_t& begin, uint32_t& end)
+{
+    const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+    begin = end = 0;
+    if(z < 0 || z >= (int)nz || y < 0 || y >= (int)ny)
+        return;
+    const int      x0  = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < (int)nx ? cx + 1 : cx;
+    const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
+    begin              = cstart[row + (uint32_t)x0];
+    end                = cstart[row + (uint32_t)x1 + 1];
+}
+
 template <bool STRICT, bool PRE32, typename Hit>
 GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
                              const double4* __restrict__ spos,
@@ -294,96 +356,94 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
     if constexpr(PRE32)
         pa32 = spos32[s];
     const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
-    const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx + 1 < (int)nx ? cx + 1 : cx;
-    for(int k = -1; k < 2; ++k)
+    for(int r = 0; r < 9; ++r)
     {
-        const int z = cz + k;
-        if(z < 0 || z >= (int)nz)
-            continue;
-        for(int j = -1; j < 2; ++j)
-        {
-            const int y = cy + j;
-            if(y < 0 || y >= (int)ny)
-                continue;
-            const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
-            const uint32_t t1  = cstart[row + (uint32_t)x1 + 1];
-            // the particle itself passes every test below and is dropped
-            // only on a hit, which keeps the common path short
+        uint32_t t0, t1;
+        neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
+        // the particle itself passes every test below and is dropped
+        // only on a hit, which keeps the common path short
 #pragma unroll 2
-            for(uint32_t t = cstart[row + (uint32_t)x0]; t < t1; ++t)
-            {
-                if constexpr(PRE32)
-                {
-                    const float4 q  = spos32[t];
-                    const float  fx = q.x - pa32.x, fy = q.y - pa32.y, fz = q.z - pa32.z;
-                    const float  fr = pa32.w + q.w;
-                    if(fx * fx + fy * fy + fz * fz >= fr * fr)
-                        continue;
-                }
-                const double4 pb = spos[t];
-                bool          h;
-                if constexpr(STRICT)
-                {
-                    const dstrict dx = dstrict(pb.x) - dstrict(pa.x);
-                    const dstrict dy = dstrict(pb.y) - dstrict(pa.y);
-                    const dstrict dz = dstrict(pb.z) - dstrict(pa.z);
-                    h = s_sqrt(dx * dx + dy * dy + dz * dz) - (dstrict(pa.w) + dstrict(pb.w))
-                        < dstrict(0.0);
-                }
-                else
-                {
-                    const double dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
-                    const double r  = pa.w + pb.w;
-                    h               = dx * dx + dy * dy + dz * dz < r * r;
-                }
-                if(h && t != (uint32_t)s)
-                    hit(t);
-            }
+        for(uint32_t t = t0; t < t1; ++t)
+        {
+            if constexpr(PRE32)
+                if(pretest_rejects<PRE32>(pa32, spos32[t]))
+                    continue;
+            if(exact_hit<STRICT>(pa, spos[t]) && t != (uint32_t)s)
+                hit(t);
         }
     }
 }
 
-// Count pass: the number of candidates of each particle (by id) and the first
-// kPairSlots of them (sorted positions t, in enumeration order) in slot[s].
-template <typename S>
-GB_D constexpr bool is_strict()
-{
-    return std::is_same<S, dstrict>::value;
-}
-
-// Count pass: per particle (by id) the number of candidates -- particles,
-// then obstacles -- with the first kPairSlots particle candidates (sorted
-// positions t, in enumeration order) in slot[s]; the obstacle candidates are
-// mask_by_id's (from k_particles or k_obstacle_mask).
+// Count pass over half of the stencil, one thread per sorted particle s.
+// The candidate test is symmetric bit for bit (b - a is -(a - b) exactly, and
+// the radius sum commutes), so each unordered pair is tested once: by s for
+// the partners t after it in the stencil's enumeration order -- the rest of
+// its own row (the cells x, x + 1 of row (dz, dy) = (0, 0) from s + 1 on,
+// one contiguous range) and the 4 rows (0, +1), (+1, -1), (+1, 0), (+1, +1).
+// A hit counts for both particles: count[id] (zeroed; the scan's input) and
+// pslot[sorted position] (zeroed; the slot index) by atomics, and the first
+// kPairSlots partners of each sorted position go to its slots in arrival
+// order.  The enumeration order of a particle's candidates is ascending
+// sorted position (rows ascend in (z, y), cells in x, ids within a cell), so
+// the fill pass restores it by sorting the slots.  Obstacle candidates are
+// added to count[id] by the particle itself.
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_count(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
-                 uint32_t* __restrict__ count, uint32_t* __restrict__ slot,
-                 const uint32_t* __restrict__ mask_by_id, int n_obs)
+                 uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
+                 uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
+    const int      s      = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= n)
         return;
-    uint32_t  c    = 0;
-    uint32_t* mine = slot + (size_t)s * kPairSlots;
-    for_each_candidate<is_strict<S>(), is_mixed<S>()>(s, skeys, spos, spos32, cstart, nx, ny, nz,
-                                                      [&](uint32_t t) {
-                                                          if(c < kPairSlots)
-                                                              mine[c] = t;
-                                                          ++c;
-                                                      });
-    const uint32_t a    = sids[s];
-    const uint32_t mask = n_obs ? mask_by_id[a] : 0u;
-    count[a]            = c + (uint32_t)obstacle_candidates(mask, n_obs);
+    if(n_obs)
+    {
+        const uint32_t a   = sids[s];
+        const int      obs = obstacle_candidates(mask_by_id[a], n_obs);
+        if(obs)
+            atomicAdd(count + a, (uint32_t)obs);
+    }
+    const uint32_t key = skeys[s];
+    const double4  pa  = spos[s];
+    float4         pa32;
+    if constexpr(PRE32)
+        pa32 = spos32[s];
+    const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+    auto record = [&](uint32_t u, uint32_t v) {
+        const uint32_t k = atomicAdd(pslot + u, 1u);
+        if(k < kPairSlots)
+            slot[(size_t)u * kPairSlots + k] = v;
+        atomicAdd(count + sids[u], 1u);
+    };
+    for(int r = 4; r < 9; ++r)
+    {
+        uint32_t t0, t1;
+        neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
+        if(r == 4)
+            t0 = (uint32_t)s + 1;
+#pragma unroll 2
+        for(uint32_t t = t0; t < t1; ++t)
+        {
+            if constexpr(PRE32)
+                if(pretest_rejects<PRE32>(pa32, spos32[t]))
+                    continue;
+            if(exact_hit<STRICT>(pa, spos[t]))
+            {
+                record((uint32_t)s, t);
+                record(t, (uint32_t)s);
+            }
+        }
+    }
 }
 
 // Fill pass, one thread per particle id a (most have no candidate and read
 // only count[a]): the pair records of a at offset[a] -- its particle
-// candidates copied from the slots of its sorted position s = sorted_of[a]
-// (or enumerated again when there were more than kPairSlots), then its
-// obstacle candidates.
+// candidates from the slots of its sorted position s = sorted_of[a], sorted
+// ascending (the enumeration order), or enumerated again in order when there
+// were more than kPairSlots -- then its obstacle candidates.
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_fill(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
@@ -412,10 +472,20 @@ __global__ void __launch_bounds__(kBlock)
     if(cp <= kPairSlots)
     {
         const uint32_t* mine = slot + (size_t)s * kPairSlots;
+        uint32_t        t[kPairSlots];
+        for(uint32_t k = 0; k < cp; ++k)
+        {
+            // insertion sort: a particle has a handful of candidates
+            const uint32_t v = mine[k];
+            uint32_t       j = k;
+            for(; j > 0 && t[j - 1] > v; --j)
+                t[j] = t[j - 1];
+            t[j] = v;
+        }
         for(uint32_t k = 0; k < cp; ++k)
         {
             pair_a[out + k] = a;
-            pair_b[out + k] = sids[mine[k]];
+            pair_b[out + k] = sids[t[k]];
         }
         out += cp;
     }

@@ -320,6 +320,25 @@ def superquadric_column_on_plate(seed=3, n=10_000, column_height=None):
                  tr, vel, walls, wtr, [law()] * 3)
 
 
+def sphere_bed(seed=1, n=60, box=(0.009, 0.009, 0.016), pitch=2.05e-3, sink=0.55e-3):
+    """Spheres of radius 1.1 mm on a 2.05 mm jittered lattice (every lattice
+    neighbour overlaps), lowered by `sink` so that the bottom layer presses on
+    the floor, with velocities N(0, 0.05 m/s) - 0.2 m/s downwards, angular
+    velocities N(0, 5 rad/s), a viscous tangential coefficient etat = 3000
+    and muc = 0.05, so that Coulomb capping occurs: the differentiable
+    workload (spheres, Hooke law, walls)."""
+    scene = superquadric_column(n=n, pitch=pitch, box=box, shape="sphere")
+    rng = np.random.default_rng(seed)
+    scene.velocities[:, :3] = rng.normal(size=(n, 3)) * 0.05
+    scene.velocities[:, 3:] = rng.normal(size=(n, 3)) * 5.0
+    scene.transforms[:, 11] -= sink
+    scene.velocities[:, 2] -= 0.2
+    scene.contact_models = [dict(m, etat=3000.0, muc=0.05) for m in scene.contact_models]
+    scene.name = "sphere_bed"
+    scene.notes = f"{n} spheres r=1.1 mm, lattice pitch {pitch*1e3:.2f} mm"
+    return scene
+
+
 # ---------------------------------------------------------------------------
 class System:
     """Applies a Scene to one engine library bound by abi.Bound (gb_, or_ or
