@@ -456,7 +456,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (f64 positions, f64 GJK polish near contact)",
+            "dtype": "f32 (f64 positions, f64 GJK)",
             "data": "synthetic (seeded jittered-lattice packing)",
             "config": {"workload": f"{scene.n:,} polydisperse superquadrics in a "
                                    "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision",
@@ -472,7 +472,9 @@ def main():
                     "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                     "ms_per_step": max(e2e_dev, e2e_wall) / args.e2e_steps * 1e3},
             "fp64": {"value": value64, "ms_per_step": t64 / args.fp64_steps * 1e3,
-                     "steps": args.fp64_steps},
+                     "steps": args.fp64_steps,
+                     "phases_ms": {k: round(float(v), 4) for k, v in
+                                   zip(abi.PHASES, ms64 / max(n64, 1))}},
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
             "adjoint": adj,

@@ -101,7 +101,7 @@ struct gb_ctx
     uint32_t obs_rect    = 0u;      // bit o: obstacle o (< 32) is a Rectangle
     double*  d_rcirc64 = nullptr;
     // FP64 shape tables: aliases of the above in the FP64 modes, separate
-    // copies in the mixed mode (read by its FP64 polish)
+    // copies in the mixed mode (read by its FP64 GJK)
     void* d_shape64 = nullptr;
     void* d_verts64 = nullptr;
     void* d_obs_shape64 = nullptr;
@@ -158,6 +158,10 @@ struct gb_ctx
     gb_stats            last{};
 
     cudaStream_t own_stream = nullptr; // the context's stream (gb_set_stream may replace it)
+    // the particle-obstacle narrow phase runs beside the particle-particle
+    // one: forked from the context's stream and joined back by these events
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t  ev_fork = nullptr, ev_join = nullptr;
     // phase timing: two alternating event sets; a set is read once the next
     // step's host synchronisation has passed it
     bool                 timing = false, in_step = false;
@@ -733,39 +737,62 @@ int run_detect(gb_ctx* c, int phases)
     const State<St> st = state_of<St>(c);
     const Tables<S> tb = tables_of<S>(c);
     {
-        // grid-stride over the device-side total (off[n]) with a grid of
-        // 8 blocks per SM (at most what the capacity needs)
+        // one wave of resident blocks walks the device-side total (off[n]):
+        // a short list is spread over all of its warps (for_each_pair)
         const uint32_t* total = c->d_off[c->cur] + c->n;
-        const int       grid  = (int)std::max<int64_t>(
-            1, std::min<int64_t>(blocks(c->cap, 128), (int64_t)8 * c->sms));
+        auto one_wave = [&](const void* kernel) {
+            int per_sm = 0;
+            if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0)
+                   != cudaSuccess
+               || per_sm < 1)
+                per_sm = 1;
+            return (int)std::max<int64_t>(
+                1, std::min<int64_t>(blocks(c->cap, 128), (int64_t)per_sm * c->sms));
+        };
         const int kr  = c->has_kr ? 1 : 0;
         const int law = c->cfg.contact_law;
-        // the GJK variant is a template parameter: each run compiles in one
-        auto with_variant = [&](auto var) {
+        // the GJK variant is a template parameter: each run compiles in one.
+        // The two kernels write disjoint records (particle pairs, obstacle
+        // pairs); both are latency-bound on few warps, so they run side by
+        // side, the obstacle one on the auxiliary stream.
+        auto with_variant = [&](auto var) -> int {
             constexpr int VAR = decltype(var)::value;
-            k_narrow<S, VAR><<<grid, 128, 0, s>>>(total, c->d_flags, c->d_pa, c->d_pb[c->cur], st,
-                                                  tb, po, law, kr, S(c->cfg.dt), c->d_counters);
+            cudaStream_t  so  = s;
+            if(c->nob)
+            {
+                GB_CK(cudaEventRecord(c->ev_fork, s));
+                GB_CK(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
+                so = c->aux_stream;
+            }
+            k_narrow<S, VAR><<<one_wave((const void*)k_narrow<S, VAR>), 128, 0, s>>>(
+                total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr, S(c->cfg.dt),
+                c->d_counters);
             c->launches += 1;
             if(!c->nob)
-                return;
+                return GB_OK;
             const bool all_rect = c->nob <= kMaskObstacles
                                   && c->obs_rect == ((c->nob == 32) ? ~0u : ((1u << c->nob) - 1u));
             if(all_rect)
-                k_narrow_obstacles<S, false, GB_GJK_JH><<<grid, 128, 0, s>>>(
+                k_narrow_obstacles<S, false, GB_GJK_JH>
+                    <<<one_wave((const void*)k_narrow_obstacles<S, false, GB_GJK_JH>), 128, 0, so>>>(
                     total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
                     S(c->cfg.dt), c->d_counters);
             else
-                k_narrow_obstacles<S, true, VAR><<<grid, 128, 0, s>>>(
+                k_narrow_obstacles<S, true, VAR>
+                    <<<one_wave((const void*)k_narrow_obstacles<S, true, VAR>), 128, 0, so>>>(
                     total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
                     S(c->cfg.dt), c->d_counters);
             c->launches += 1;
+            GB_CK(cudaEventRecord(c->ev_join, so));
+            GB_CK(cudaStreamWaitEvent(s, c->ev_join, 0));
+            return GB_OK;
         };
         if(c->cfg.gjk_variant == GB_GJK_SV)
-            with_variant(std::integral_constant<int, GB_GJK_SV>{});
+            GB_TRY(with_variant(std::integral_constant<int, GB_GJK_SV>{}));
         else if(c->cfg.gjk_variant == GB_GJK_NESTEROV)
-            with_variant(std::integral_constant<int, GB_GJK_NESTEROV>{});
+            GB_TRY(with_variant(std::integral_constant<int, GB_GJK_NESTEROV>{}));
         else
-            with_variant(std::integral_constant<int, GB_GJK_JH>{});
+            GB_TRY(with_variant(std::integral_constant<int, GB_GJK_JH>{}));
         GB_CK(cudaGetLastError());
     }
     mark(c, 6);
@@ -1051,7 +1078,10 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
     if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) == cudaSuccess
        && sms > 0)
         c->sms = sms;
-    if(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    if(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess
+       || cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess
+       || cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess
+       || cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
         st = GB_E_CUDA;
     c->stream = c->own_stream;
     c->timing = (cfg->flags & GB_FLAG_PHASE_TIMING) != 0;
@@ -1109,6 +1139,12 @@ int gb_destroy(gb_ctx* c)
         for(int b = 0; b < gb_ctx::kEvRing; ++b)
             for(int k = 0; k <= GB_N_PHASES; ++k)
                 cudaEventDestroy(c->ev[b][k]);
+    if(c->ev_fork)
+        cudaEventDestroy(c->ev_fork);
+    if(c->ev_join)
+        cudaEventDestroy(c->ev_join);
+    if(c->aux_stream)
+        cudaStreamDestroy(c->aux_stream);
     if(c->own_stream)
         cudaStreamDestroy(c->own_stream);
     delete c;

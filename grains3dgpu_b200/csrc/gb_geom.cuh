@@ -83,6 +83,24 @@ GB_D S sgn(S x)
     return S(double((S(0.0) < x) - (x < S(0.0))));
 }
 
+// Superquadric::support for v.x != 0 in plain FP64: the reference's
+// expressions with every power x^y written as 2^(y log2 x) and kept in the
+// log domain between the steps.  The dependent chain falls from five pow
+// calls and a division to three log2/exp2 pairs (pow is the longest-latency
+// FP64 function); the values agree with pow's to a few ulps times
+// |y log2 x|.  Zero y or z components give log2 0 = -inf and 2^-inf = 0, as
+// pow(0, y) does.  Straight-line code, so that two calls interleave.
+GB_D V3<double> support_sq_log(const Body<double>& b, const V3<double>& v)
+{
+    const double abvx = fabs(v.x), abvy = fabs(v.y), abvz = fabs(v.z);
+    const double la = b.k[4] * log2(b.k[0] * abvy / abvx);              // log2 alpha
+    const double lt = log2(1.0 + exp2(b.p[4] * la));                     // log2 temp
+    const double lb = b.k[5] * lt + b.k[3] * log2(b.k[1] * abvz / abvx); // log2 beta
+    const double xt = exp2(-b.k[7] * log2(exp2(b.k[6] * lt) + exp2(b.p[3] * lb)));
+    return mk<double>(sgn(v.x) * b.p[0] * xt, sgn(v.y) * exp2(la) * b.p[1] * xt,
+                      sgn(v.z) * exp2(lb) * b.p[2] * xt);
+}
+
 // Superquadric::support (Grains/Geometry/src/Superquadric.cpp:169-205)
 template <typename S>
 GB_D V3<S> support_sq(const Body<S>& b, const V3<S>& v)
@@ -90,6 +108,18 @@ GB_D V3<S> support_sq(const Body<S>& b, const V3<S>& v)
     const S abvx = s_fabs(v.x), abvy = s_fabs(v.y), abvz = s_fabs(v.z);
     const S signx = sgn(v.x), signy = sgn(v.y), signz = sgn(v.z);
     const S one = S(1.0);
+    if constexpr(std::is_same<S, double>::value)
+    {
+        if(abvx == 0.0)
+        {
+            if(abvy == 0.0)
+                return mk<S>(0.0, 0.0, signz * b.p[2]);
+            const double la = b.k[3] * log2(b.k[2] * abvz / abvy); // log2 alpha
+            const double yt = exp2(-b.k[7] * log2(1.0 + exp2(b.p[3] * la)));
+            return mk<S>(0.0, signy * b.p[1] * yt, signz * exp2(la) * b.p[2] * yt);
+        }
+        return support_sq_log(b, v);
+    }
     if(abvx == S(0.0))
     {
         if(abvy == S(0.0))
@@ -151,6 +181,29 @@ GB_D V3<S> support(const Body<S>& b, const V3<S>& v)
         default:
             return mk<S>(S(0.0), S(0.0), S(0.0));
     }
+}
+
+// The supports of A along va and of B along vb.  Two FP64 superquadrics take
+// the straight-line log-domain form side by side, so that the compiler
+// interleaves their two dependent chains (the rare v.x = 0 direction is
+// redone on the general path); the results are those of two support calls.
+template <typename S>
+GB_D void support2(const Body<S>& A, const V3<S>& va, const Body<S>& B, const V3<S>& vb,
+                   V3<S>& pa, V3<S>& pb)
+{
+    if constexpr(std::is_same<S, double>::value)
+        if(A.type == GB_SUPERQUADRIC && B.type == GB_SUPERQUADRIC)
+        {
+            pa = support_sq_log(A, va);
+            pb = support_sq_log(B, vb);
+            if(va.x == 0.0)
+                pa = support_sq(A, va);
+            if(vb.x == 0.0)
+                pb = support_sq(B, vb);
+            return;
+        }
+    pa = support(A, va);
+    pb = support(B, vb);
 }
 
 // intersectOrientedBoundingBox (Grains/CollisionDetection/src/OBB.cpp:32-94):
@@ -336,12 +389,10 @@ struct GjkResult
 };
 
 // computeClosestPoints_GJK_JH (GJK_JH.cpp:310-391), in A's frame with b2a.
-// `max_iter` caps the iterations (the reference's cap is 1000); the loop also
-// stops once the lower bound mu exceeds `reject_above` (the mixed mode's FP32
-// rejection test; +inf keeps the reference loop).
+// `max_iter` caps the iterations (the reference's cap is 1000).
 template <typename S>
 GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
-                         int max_iter = 1000, S reject_above = S(INFINITY))
+                         int max_iter = 1000)
 {
     unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
     V3<S>    p[4], q[4];
@@ -376,14 +427,11 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
             ++last;
             last_bit <<= 1;
         }
-        p[last] = support(A, -v);
-        q[last] = support(B, mul_t(b2a.R, v));
+        support2(A, -v, B, mul_t(b2a.R, v), p[last], q[last]);
         w       = p[last] - apply(b2a, q[last]);
         const S g = dot(v, w) / dist;
         if(mu < g)
             mu = g;
-        if(mu > reject_above)
-            break;
         if(dist - mu <= dist * rel_error || mu < abs_error)
             break;
         if(jh.degenerate(all_bits, w))
@@ -699,8 +747,7 @@ GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
         }
         else
             d = v;
-        p[last]   = support(A, -d);
-        q[last]   = support(B, mul_t(b2a.R, d));
+        support2(A, -d, B, mul_t(b2a.R, d), p[last], q[last]);
         w         = p[last] - apply(b2a, q[last]);
         const S mu = dist - dot(v, w) / dist;
         if(mu < dist * rel_error || mu < abs_error || sv_degenerate(bits, y, w))

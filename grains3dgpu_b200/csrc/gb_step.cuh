@@ -38,20 +38,21 @@ struct Tables
     const double4*               obs_plane; // Rectangle planes: normal, normal . origin
     uint32_t                     obs_rect;  // bit o: obstacle o (< 32) is a Rectangle
     int                          n_obs;
-    // FP64 copies of the shape tables (the mixed mode's polish reads these)
+    // FP64 copies of the shape tables (read by the mixed mode's FP64 GJK)
     const RBShape<double>* shape64;
     const Vert<double>*    verts64;
     const RBShape<double>* obs_shape64;
 };
 
-// ---- mixed precision: FP32 contact detection, FP64 polish near contact ------
-// FP32 GJK serves only as a certified rejection: its lower bound never exceeds
-// the true distance, so a pair whose bound clears the crusts by kPolishMargin
-// times the pair's size has no contact.  Every other pair is re-solved from
-// scratch by the FP64 GJK of the FP64 mode: FP32 support points on mm-size
-// grains carry ~1e-10 m of rounding, the order of a resting contact's overlap
-// (m g / kn ~ 1e-8 m), so contact points and overlaps come from FP64.
-constexpr float kPolishMargin = 64.0f * 1.1920929e-7f;
+// ---- mixed precision narrow phase --------------------------------------------
+// The bounding-sphere and OBB tests run in FP32 on FP32 poses (their margins
+// are absolute: LOWEPS on the OBB axes, the crust-free bounding box), and every
+// pair that survives them is solved by the FP64 GJK of the FP64 mode, with
+// FP64 shape tables and the FP32 quaternion widened: FP32 support points on
+// mm-size grains carry ~1e-10 m of rounding, the order of a resting contact's
+// overlap (m g / kn ~ 1e-8 m), so contact points and overlaps come from FP64.
+// (An FP32 GJK as a rejection stage before the FP64 solve measured slower than
+// the FP64 solve alone once its supports took the log-domain form.)
 
 GB_D M3<double> load_rot64(const State<float>& st, uint32_t i)
 {
@@ -69,7 +70,7 @@ GB_D Contact<float> to_f(const Contact<double>& c)
 }
 
 // closestPointsRigidBodies for the mixed mode; points relative to A's centre.
-// VAR: the GJK of the FP64 re-solve (the FP32 rejection is always Johnson's).
+// VAR: the GJK variant of the FP64 solve.
 template <int VAR>
 GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& st, uint32_t a,
                                   uint32_t b, uint32_t ra, uint32_t rb, const Body<float>& A,
@@ -96,18 +97,8 @@ GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& s
         return no_contact<float>();
     if(!obb_overlap(A.bb, B.bb, RA, RB, d))
         return no_contact<float>();
-    Tr<float>       b2a;
-    const M3<float> RAt = transpose(RA);
-    b2a.R               = mul(RAt, RB);
-    b2a.o               = mul(RAt, d);
-    // FP32 rejection: GJK's lower bound mu never exceeds the true distance, so a
-    // pair whose mu clears the crusts by the rounding margin is not in contact
-    const float reject = (A.crust + B.crust) + kPolishMargin * (A.rcirc + B.rcirc);
-    const GjkResult<float> g32 = gjk_jh(A, B, b2a, 32, reject);
-    *iters += g32.iters;
-    if(g32.lower > reject)
-        return no_contact<float>();
-    // every possible contact is re-solved on the FP64 path of the FP64 mode
+    // every pair that passes the bounding tests is solved on the FP64 path of
+    // the FP64 mode
     const Body<double> A64 = load_body<double>(tb.shape64, ra, tb.verts64);
     const Body<double> B64 = load_body<double>(tb.shape64, rb, tb.verts64);
     const M3<double>   RA64 = load_rot64(st, a), RB64 = load_rot64(st, b);
@@ -740,6 +731,32 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
 
+// The pair records of a narrow-phase launch, p in [0, npairs).  A list longer
+// than the grid is walked with a grid stride (consecutive records in
+// consecutive lanes).  A shorter one -- the common case of a loose packing,
+// a few thousand candidates -- is spread over all warps, ceil(npairs / warps)
+// consecutive records per warp: one thread's GJK is a long dependent chain,
+// and the divergent chains of a warp run one after the other, so the step
+// waits for the warp with the most records, not for the longest chain alone.
+template <typename F>
+GB_D void for_each_pair(int64_t npairs, F&& f)
+{
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid      = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if(npairs < nthreads)
+    {
+        const int64_t nwarps = nthreads >> 5;
+        const int64_t k      = (npairs + nwarps - 1) / nwarps; // <= 32
+        const int64_t lane   = threadIdx.x & 31;
+        const int64_t p      = (tid >> 5) * k + lane;
+        if(lane < k && p < npairs)
+            f(p);
+    }
+    else
+        for(int64_t p = tid; p < npairs; p += nthreads)
+            f(p);
+}
+
 // The pair count is read on the device (*total, the scan's grand total), so
 // the host launches a resident-sized grid without waiting for it.
 template <typename S, int VAR>
@@ -751,10 +768,9 @@ __global__ void __launch_bounds__(128)
 {
     if(step_aborted(flags))
         return;
-    const int64_t npairs = *total;
-    for(int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
-        p += (int64_t)gridDim.x * blockDim.x)
+    for_each_pair(*total, [&](int64_t p) {
         narrow_pair<S, VAR>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters);
+    });
 }
 
 // ---- per-particle kernel -------------------------------------------------------
@@ -798,15 +814,12 @@ __global__ void __launch_bounds__(128)
 {
     if(step_aborted(flags))
         return;
-    const int64_t npairs = *total;
-    for(int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npairs;
-        p += (int64_t)gridDim.x * blockDim.x)
-    {
+    for_each_pair(*total, [&](int64_t p) {
         const uint32_t b = pair_b[p];
         if(b & kObstacleBit)
             narrow_obstacle<S, GEN, VAR>(p, pair_a[p], (int)(b & ~kObstacleBit), st, tb, po,
                                          law_kind, has_kr, dt, counters);
-    }
+    });
 }
 
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
