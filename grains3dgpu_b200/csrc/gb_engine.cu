@@ -316,6 +316,8 @@ int upload_tables(gb_ctx* c)
             in[i].I[k]  = (St)c->props[i].inertia[k];
             in[i].I1[k] = (St)c->props[i].inertia_inv[k];
         }
+        for(int k = 0; k < 3; ++k)
+            in[i].bb[k] = sh[i].bb[k];
         rc[i] = c->props[i].circumscribed_radius;
     }
     const size_t nv = c->verts.size() / 3;
@@ -807,7 +809,8 @@ int run_detect(gb_ctx* c, int phases)
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
     sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
-    launch_particles<S>(c, st, tb, po, sp, c->d_contacts);
+    // the per-particle contact counts are read only by the detect call
+    launch_particles<S>(c, st, tb, po, sp, phases == PHASE_STEP ? nullptr : c->d_contacts);
     GB_CK(cudaGetLastError());
     mark(c, 7);
     close_event_set(c);

@@ -27,14 +27,16 @@ struct RBShape
     int32_t pad;
 };
 
-// Inertial part, as read by the integrator (RigidBody.hh:28-37).
+// Inertial part, as read by the per-particle kernel (RigidBody.hh:28-37),
+// with the bounding box the obstacle mask needs: 16 values, one aligned
+// record (64 B in FP32), so that a particle's body costs two 32-byte sectors.
 template <typename St>
-struct RBInertia
+struct alignas(16 * sizeof(St)) RBInertia
 {
     St mass;
     St I[6];
     St I1[6];
-    St pad;
+    St bb[3];
 };
 
 template <typename St>

@@ -228,8 +228,8 @@ GB_D uint32_t obstacle_mask_at(const Tables<S>& tb, uint32_t r, const M3<S>& RA,
     // extent along the normal from this mode's rotation; the slack covers the
     // rounding of both and the 1e-7 difference between the mixed mode's FP32
     // rotation and the FP64 one its contact recomputation uses
-    const double bb[3] = {(double)tb.shape[r].bb[0], (double)tb.shape[r].bb[1],
-                          (double)tb.shape[r].bb[2]};
+    const double bb[3] = {(double)tb.inertia[r].bb[0], (double)tb.inertia[r].bb[1],
+                          (double)tb.inertia[r].bb[2]};
     const double ax    = fabs(xa[0]) + fabs(xa[1]) + fabs(xa[2]);
     uint32_t     mask  = ~tb.obs_rect & ((nm == 32) ? ~0u : ((1u << nm) - 1u));
     for(int o = 0; o < nm; ++o)
