@@ -489,11 +489,12 @@ def main():
 
 
 # DRAM bytes (read + write) per particle of the dominant kernels, from one
-# ncu capture of this workload with 400,000 particles
-# (profiles/k_pair_count_k_particles_superquadrics_400k.md); the traffic scales
-# with the particle count, so a full launch moves this many bytes per particle.
-TRAFFIC_PER_PARTICLE = {"particle": (89.93e6 + 16.81e6) / 400_000,
-                        "pair_count": (23.55e6 + 0.0003e6) / 400_000}
+# ncu capture of this workload with 1,000,000 particles
+# (profiles/k_pair_count_k_narrow_k_particles_superquadrics_1M.md); their
+# traffic scales with the particle count.  The narrow phase's scales with the
+# pairs that reach GJK and is not extrapolated.
+TRAFFIC_PER_PARTICLE = {"particle": (136.10e6 + 28.58e6) / 1_000_000,
+                        "pair_count": (62.02e6 + 0.93e6) / 1_000_000}
 
 
 def traffic_bytes(phase, n):
