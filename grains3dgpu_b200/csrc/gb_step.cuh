@@ -823,11 +823,12 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
-// A streaming kernel: four 256-thread blocks per SM keep enough loads in
-// flight (the mixed instantiation fits 64 registers without spilling; the
-// FP64 ones need about 100 and get two blocks).
+// A latency-bound streaming kernel: the mixed instantiation runs five
+// 256-thread blocks per SM at 48 registers (a few spilled values of the rare
+// paths) for more loads in flight, which measured faster than four blocks at
+// 64; the FP64 ones need about 100 registers and get two blocks.
 template <typename S>
-__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
                 uint32_t* __restrict__ mask_out, const int* __restrict__ flags,
