@@ -406,8 +406,10 @@ def main():
     fd, clk_path = tempfile.mkstemp(prefix=f"gb_clocks_rank{rank}_", suffix=".csv")
     os.close(fd)
     sampler, fh = clocks_sampler(clk_path)
-    sysm, elapsed, launches, ms, nsteps, st = run_engine(
-        args, scene, abi.GB_MIXED, args.steps, args.warmup, torch, rank, world)
+    # the timed run carries no phase events; the phase split comes from a
+    # second, instrumented run of the same workload
+    sysm, elapsed, launches, _, _, st = run_engine(
+        args, scene, abi.GB_MIXED, args.steps, args.warmup, torch, rank, world, timing=False)
     if sampler:
         sampler.terminate()
         fh.close()
@@ -415,6 +417,13 @@ def main():
     os.unlink(clk_path)
     t_max = max_over_ranks(elapsed, torch, world, "cuda")
     value = aggregate(world, scene.n, args.steps, t_max)
+
+    e2e_dev, e2e_wall, h2d, d2h = e2e_engine(sysm, args.e2e_steps, torch)
+    e2e_value = world * scene.n * args.e2e_steps / max(e2e_dev, e2e_wall)
+    sysm.close()
+    sys_ph, _, _, ms, nsteps, _ = run_engine(args, scene, abi.GB_MIXED, min(args.steps, 10), 3,
+                                             torch, rank, world, timing=True)
+    sys_ph.close()
 
     # per-phase roofline (phase device time from CUDA events on the launch stream)
     hbm, hbm_kind = measured_hbm()
@@ -432,13 +441,14 @@ def main():
                 "peak": hbm, "unit": "GB/s", "frac": phases[top]["frac_of_measured_hbm"],
                 "traffic": traffic_bytes(top, scene.n), "peak_kind": hbm_kind}
 
-    e2e_dev, e2e_wall, h2d, d2h = e2e_engine(sysm, args.e2e_steps, torch)
-    e2e_value = world * scene.n * args.e2e_steps / max(e2e_dev, e2e_wall)
-    sysm.close()
-
-    # the all-FP64 run of the same kernels on the same workload
-    _, el64, _, ms64, n64, _ = run_engine(args, scene, abi.GB_FP64, args.fp64_steps, 3, torch,
-                                          rank, world)
+    # the all-FP64 run of the same kernels on the same workload (timed, then
+    # instrumented for its phase split)
+    s64, el64, _, _, _, _ = run_engine(args, scene, abi.GB_FP64, args.fp64_steps, 3, torch,
+                                       rank, world, timing=False)
+    s64.close()
+    s64, _, _, ms64, n64, _ = run_engine(args, scene, abi.GB_FP64, args.fp64_steps, 3, torch,
+                                         rank, world, timing=True)
+    s64.close()
     t64 = max_over_ranks(el64, torch, world, "cuda")
     value64 = aggregate(world, scene.n, args.fp64_steps, t64)
     ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
