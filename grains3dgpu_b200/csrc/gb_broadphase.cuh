@@ -22,6 +22,7 @@ constexpr int kFlagCapacity    = 1 << 8;
 constexpr int kFlagCellCrowded = 1 << 9; // a cell too full for the counting sort's rank pass
 // Either one aborts the step: the kernels that write pair lists or state
 // return at entry once it is set, and the host replays the step.
+constexpr int kFlagScanStall   = 1 << 10; // a one-pass scan gave up waiting (never expected)
 constexpr int kFlagAbort = kFlagCapacity | kFlagCellCrowded;
 
 __device__ __forceinline__ bool step_aborted(const int* flags)
@@ -386,6 +387,98 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply(const uint32_t* __restric
         s += v[j];
     }
     uint32_t run = partial[blockIdx.x] + block_excl_scan(s, nullptr);
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+        if(base + j < n)
+        {
+            out[base + j] = run;
+            run += v[j];
+        }
+}
+
+// One-pass exclusive scan (decoupled look-back: Merrill and Garland, "Single-
+// pass Parallel Prefix Scan with Decoupled Look-back", 2016).  Each tile
+// publishes its aggregate, then its inclusive prefix, in one 64-bit word:
+// value in bits 0-31, status in bits 32-33 (1 aggregate, 2 inclusive prefix),
+// the scan's epoch in bits 34-63.  A tile's exclusive prefix is the sum over
+// its predecessors' words back to the first inclusive prefix.  Tiles are
+// numbered in the order their blocks start (a ticket counter that only grows;
+// `ticket_base` is its value before this launch), so every predecessor of a
+// tile is already running and the look-back ends; a bound on the wait still
+// stops it and flags kFlagScanStall.  Words of earlier scans carry another
+// epoch and read as unpublished, so the state needs no clearing between scans.
+// In place (in == out) is allowed.  abort_flags as for k_scan_apply.
+constexpr unsigned long long kScanAggregate = 1ull, kScanPrefix = 2ull;
+constexpr uint32_t           kScanEpochMask = (1u << 30) - 1u;
+constexpr uint32_t           kScanSpinLimit = 1u << 20;
+
+__global__ void __launch_bounds__(kBlock)
+    k_scan_onepass(const uint32_t* in, uint32_t* out, int64_t n,
+                   unsigned long long* __restrict__ tile_state,
+                   unsigned long long* __restrict__ ticket, unsigned long long ticket_base,
+                   uint32_t epoch, uint32_t* __restrict__ grand_total,
+                   const int* abort_flags, int* __restrict__ flags)
+{
+    __shared__ uint32_t s_tile, s_prefix;
+    if(threadIdx.x == 0)
+        s_tile = (uint32_t)(atomicAdd(ticket, 1ull) - ticket_base);
+    __syncthreads();
+    if(step_aborted(abort_flags)) // every block alike, after taking its ticket
+        return;
+    const uint32_t tile = s_tile;
+    if(tile >= gridDim.x) // a ticket count out of step with the host's: never expected
+    {
+        if(threadIdx.x == 0)
+            atomicOr(flags, kFlagScanStall);
+        return;
+    }
+    const int64_t  base = (int64_t)tile * kTile + (int64_t)threadIdx.x * kItems;
+    uint32_t       v[kItems];
+    uint32_t       s = 0;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j)
+    {
+        v[j] = base + j < n ? in[base + j] : 0u;
+        s += v[j];
+    }
+    uint32_t       agg;
+    const uint32_t ex = block_excl_scan(s, &agg);
+    if(threadIdx.x == 0)
+    {
+        const uint32_t           ep  = epoch & kScanEpochMask;
+        const unsigned long long tag = (unsigned long long)ep << 34;
+        uint32_t                 prefix = 0;
+        if(tile > 0)
+        {
+            atomicExch(tile_state + tile, tag | (kScanAggregate << 32) | agg);
+            int64_t  p     = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while(p >= 0)
+            {
+                const unsigned long long w  = *(volatile unsigned long long*)(tile_state + p);
+                const unsigned long long st = (w >> 32) & 3ull;
+                if((uint32_t)(w >> 34) != ep || st == 0)
+                {
+                    if(++spins > kScanSpinLimit)
+                    {
+                        atomicOr(flags, kFlagScanStall);
+                        break;
+                    }
+                    continue;
+                }
+                prefix += (uint32_t)w;
+                if(st == kScanPrefix)
+                    break;
+                --p;
+            }
+        }
+        atomicExch(tile_state + tile, tag | (kScanPrefix << 32) | (prefix + agg));
+        s_prefix = prefix;
+        if(grand_total && (int64_t)(tile + 1) * kTile >= n)
+            *grand_total = prefix + agg;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + ex;
 #pragma unroll
     for(int j = 0; j < kItems; ++j)
         if(base + j < n)

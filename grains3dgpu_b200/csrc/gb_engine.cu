@@ -126,10 +126,19 @@ struct gb_ctx
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
+    uint32_t* d_gjkq   = nullptr; // the step's pairs that need GJK (pair capacity)
+    uint32_t* d_gjkn   = nullptr; // their number (reset by the fill pass)
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
     uint32_t* d_obsmask_id = nullptr; // the same per particle id, from the last move
     bool      mask_valid   = false;   // d_obsmask_id matches the current poses
     size_t    part_cap = 0, hist_cap = 0;
+    // one-pass scans: per-tile state words, the tile ticket counter, the
+    // tickets taken so far and the epoch of the next scan
+    unsigned long long* d_tile_state = nullptr;
+    unsigned long long* d_ticket     = nullptr;
+    size_t              tile_cap     = 0;
+    unsigned long long  tickets      = 0;
+    uint32_t            scan_epoch   = 0;
 
     // pairs (double-buffered for the tangential history)
     uint32_t* d_count = nullptr;
@@ -440,6 +449,14 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
     GB_TRY(dalloc(&c->d_counters, 4));
+    GB_TRY(dalloc(&c->d_gjkn, 1));
+    GB_CK(cudaMemset(c->d_gjkn, 0, sizeof(uint32_t)));
+    if(!c->d_ticket)
+    {
+        GB_TRY(dalloc(&c->d_ticket, 1));
+        GB_CK(cudaMemset(c->d_ticket, 0, sizeof(unsigned long long)));
+        c->tickets = 0;
+    }
     GB_CK(cudaMemset(c->d_flags, 0, sizeof(int)));
     GB_CK(cudaMemset(c->d_counters, 0, 4 * sizeof(unsigned long long)));
     GB_CK(cudaMemset(c->d_contacts, 0, std::max<size_t>(1, n) * sizeof(int)));
@@ -490,6 +507,8 @@ int ensure_pairs(gb_ctx* c, int64_t need)
     dfree(c->d_pf);
     dfree(c->d_pc);
     dfree(c->d_info);
+    dfree(c->d_gjkq);
+    GB_TRY(dalloc(&c->d_gjkq, ncap));
     GB_TRY(dalloc(&c->d_pa, ncap));
     GB_CK(cudaMalloc(&c->d_pf, 9 * ncap * ss));
     GB_TRY(dalloc(&c->d_pc, ncap));
@@ -502,20 +521,34 @@ int ensure_pairs(gb_ctx* c, int64_t need)
 // exclusive scan of n uint32 (in place allowed); *d_total (device) gets the sum
 // exclusive scan of n values; with abort_flags, an aborted step's scan writes
 // nothing
+// exclusive scan of n counts in one launch (k_scan_onepass); every block
+// takes a ticket, so the host knows the counter's value before each launch
 int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* d_total,
              const int* abort_flags = nullptr)
 {
     const int nb = std::max(1, blocks(n, kTile));
-    if((size_t)nb > c->part_cap)
+    if((size_t)nb > c->tile_cap)
     {
-        dfree(c->d_part);
-        GB_TRY(dalloc(&c->d_part, nb));
-        c->part_cap = nb;
+        // growing the state mid-step: wait for the scans that may still read it
+        GB_CK(cudaStreamSynchronize(c->stream));
+        dfree(c->d_tile_state);
+        GB_TRY(dalloc(&c->d_tile_state, nb));
+        GB_CK(cudaMemset(c->d_tile_state, 0, nb * sizeof(unsigned long long)));
+        c->tile_cap = nb;
     }
-    k_scan_reduce<<<nb, kBlock, 0, c->stream>>>(in, n, c->d_part);
-    k_scan_partials<<<1, 1024, 0, c->stream>>>(c->d_part, nb, d_total, abort_flags);
-    k_scan_apply<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_part, abort_flags);
-    c->launches += 3;
+    c->scan_epoch = (c->scan_epoch + 1) & kScanEpochMask;
+    if(c->scan_epoch == 0)
+    {
+        // the epoch wrapped: clear the words so that no old one can match
+        GB_CK(cudaMemsetAsync(c->d_tile_state, 0, c->tile_cap * sizeof(unsigned long long),
+                              c->stream));
+        c->scan_epoch = 1;
+    }
+    k_scan_onepass<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_tile_state, c->d_ticket,
+                                                  c->tickets, c->scan_epoch, d_total,
+                                                  abort_flags, c->d_flags);
+    c->tickets += (unsigned long long)nb;
+    c->launches += 1;
     GB_CK(cudaGetLastError());
     return GB_OK;
 }
@@ -676,7 +709,7 @@ int build_pairs(gb_ctx* c)
     k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_sorted_of, c->d_spos,
                                          spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
                                          c->d_count, c->d_slot, c->d_obsmask_id, c->nob, off,
-                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags);
+                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags, c->d_gjkn);
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 5);
@@ -768,8 +801,11 @@ int run_detect(gb_ctx* c, int phases)
             }
             k_narrow<S, VAR><<<one_wave((const void*)k_narrow<S, VAR>), 128, 0, s>>>(
                 total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr, S(c->cfg.dt),
-                c->d_counters);
-            c->launches += 1;
+                c->d_counters, c->d_gjkq, c->d_gjkn);
+            k_narrow_gjk<S, VAR><<<one_wave((const void*)k_narrow_gjk<S, VAR>), 128, 0, s>>>(
+                c->d_gjkn, c->d_flags, c->d_gjkq, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
+                S(c->cfg.dt), c->d_counters);
+            c->launches += 2;
             if(!c->nob)
                 return GB_OK;
             const bool all_rect = c->nob <= kMaskObstacles
@@ -888,6 +924,8 @@ int finish(gb_ctx* c)
     c->last.status_flags |= flags;
     if(flags & kFlagCapacity)
         return GB_E_CAPACITY;
+    if(flags & kFlagScanStall)
+        return GB_E_CUDA;
     if(flags & kFlagNonFinite)
         return GB_E_NONFINITE;
     if(flags & kFlagOutOfDomain)
@@ -1001,6 +1039,8 @@ int run_steps(gb_ctx* c, int32_t n_steps, int phases, int32_t* result)
     const int flags = n_steps > 0 ? (int)c->h_pinned[1] : 0;
     GB_CK(cudaMemsetAsync(c->d_flags, 0, sizeof(int), s));
     c->last.status_flags |= flags;
+    if(flags & kFlagScanStall)
+        return GB_E_CUDA;
     if(flags & kFlagNonFinite)
         return GB_E_NONFINITE;
     if(flags & kFlagOutOfDomain)
@@ -1126,7 +1166,7 @@ int gb_destroy(gb_ctx* c)
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_done,
                     c->d_contacts,
-                    c->d_stage,     c->d_adj};
+                    c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);

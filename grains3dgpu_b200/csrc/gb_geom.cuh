@@ -185,14 +185,60 @@ GB_D V3<S> support(const Body<S>& b, const V3<S>& v)
     }
 }
 
-// The supports of A along va and of B along vb.  Two FP64 superquadrics take
-// the straight-line log-domain form side by side, so that the compiler
-// interleaves their two dependent chains (the rare v.x = 0 direction is
-// redone on the general path); the results are those of two support calls.
-template <typename S>
+// A GJK variant flag: the solve runs on two adjacent lanes, which compute
+// the same iterates; the even lane evaluates A's support and the odd lane B's,
+// in parallel, and they exchange them by shuffles.  (A support is the longest
+// dependent chain of an iteration: ~2,000 cycles for an FP64 superquadric.)
+constexpr int kGjkPaired = 8;
+
+GB_D float lane_shfl(unsigned mask, float v, unsigned src)
+{
+    return __shfl_sync(mask, v, src);
+}
+GB_D double lane_shfl(unsigned mask, double v, unsigned src)
+{
+    return __shfl_sync(mask, v, src);
+}
+GB_D dstrict lane_shfl(unsigned mask, dstrict v, unsigned src)
+{
+    return dstrict(__shfl_sync(mask, v.v, src));
+}
+
+// The supports of A along va and of B along vb, the results of two support
+// calls.  PAIRED: one per lane of a lane pair (kGjkPaired).  Otherwise two
+// FP64 superquadrics take the straight-line log-domain form side by side
+// (the rare v.x = 0 direction is redone on the general path).
+template <bool PAIRED = false, typename S>
 GB_D void support2(const Body<S>& A, const V3<S>& va, const Body<S>& B, const V3<S>& vb,
                    V3<S>& pa, V3<S>& pb)
 {
+    if constexpr(PAIRED)
+    {
+        const unsigned lane   = threadIdx.x & 31u;
+        const unsigned even   = lane & ~1u;
+        const unsigned mask   = 3u << even;
+        const bool     second = (lane & 1u) != 0u;
+        // field by field, so that the two lanes select data, not code paths
+        Body<S> X;
+        X.type   = second ? B.type : A.type;
+        X.nverts = second ? B.nverts : A.nverts;
+        X.verts  = second ? B.verts : A.verts;
+#pragma unroll
+        for(int i = 0; i < 5; ++i)
+            X.p[i] = second ? B.p[i] : A.p[i];
+#pragma unroll
+        for(int i = 0; i < 8; ++i)
+            X.k[i] = second ? B.k[i] : A.k[i];
+        X.crust = second ? B.crust : A.crust;
+        X.rcirc = second ? B.rcirc : A.rcirc;
+        X.bb    = second ? B.bb : A.bb;
+        const V3<S> r = support(X, second ? vb : va);
+        pa = mk<S>(lane_shfl(mask, r.x, even), lane_shfl(mask, r.y, even),
+                   lane_shfl(mask, r.z, even));
+        pb = mk<S>(lane_shfl(mask, r.x, even + 1u), lane_shfl(mask, r.y, even + 1u),
+                   lane_shfl(mask, r.z, even + 1u));
+        return;
+    }
     if constexpr(std::is_same<S, double>::value)
         if(A.type == GB_SUPERQUADRIC && B.type == GB_SUPERQUADRIC)
         {
@@ -392,7 +438,7 @@ struct GjkResult
 
 // computeClosestPoints_GJK_JH (GJK_JH.cpp:310-391), in A's frame with b2a.
 // `max_iter` caps the iterations (the reference's cap is 1000).
-template <typename S>
+template <typename S, bool PAIRED = false>
 GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
                          int max_iter = 1000)
 {
@@ -417,7 +463,9 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
     const S rel_error      = k_loweps<S>();
     const S abs_error      = S(1.e-4) * rel_error;
 
-    V3<S> v    = support(A, zero3<S>()) - apply(b2a, support(B, zero3<S>()));
+    V3<S> s0A, s0B;
+    support2<PAIRED>(A, zero3<S>(), B, zero3<S>(), s0A, s0B);
+    V3<S> v    = s0A - apply(b2a, s0B);
     V3<S> w    = v;
     S     dist = norm(v);
     while(bits < 15 && dist > k_higheps<S>() && num_iterations < max_iter)
@@ -429,7 +477,7 @@ GB_D GjkResult<S> gjk_jh(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a,
             ++last;
             last_bit <<= 1;
         }
-        support2(A, -v, B, mul_t(b2a.R, v), p[last], q[last]);
+        support2<PAIRED>(A, -v, B, mul_t(b2a.R, v), p[last], q[last]);
         w       = p[last] - apply(b2a, q[last]);
         const S g = dot(v, w) / dist;
         if(mu < g)
@@ -700,7 +748,7 @@ GB_D bool sv_degenerate(unsigned bits, const V3<S> y[4], const V3<S>& w)
 //   y_k = delta_k x_k + (1 - delta_k) s_{k-1},   delta_k = (k + 1)/(k + 3),
 //   d_k = delta_k d_{k-1}/|d_{k-1}| + (1 - delta_k) y_k/|y_k|.
 // Without NESTEROV it is computeClosestPoints_GJK_AY (GJK_AY.cpp:392-469).
-template <typename S, bool NESTEROV>
+template <typename S, bool NESTEROV, bool PAIRED = false>
 GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
 {
     unsigned bits = 0, last = 0;
@@ -713,7 +761,9 @@ GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
     bool    momentum       = NESTEROV;
     const S rel_error      = k_loweps<S>();
     const S abs_error      = S(1.e-4) * rel_error;
-    V3<S>   v = support(A, zero3<S>()) - apply(b2a, support(B, zero3<S>()));
+    V3<S>   s0A, s0B;
+    support2<PAIRED>(A, zero3<S>(), B, zero3<S>(), s0A, s0B);
+    V3<S>   v = s0A - apply(b2a, s0B);
     V3<S>   w = v, d = v, s_prev = v;
     S       dist = norm(v);
     while(bits < 15 && dist > k_higheps<S>() && num_iterations < 1000)
@@ -749,7 +799,7 @@ GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
         }
         else
             d = v;
-        support2(A, -d, B, mul_t(b2a.R, d), p[last], q[last]);
+        support2<PAIRED>(A, -d, B, mul_t(b2a.R, d), p[last], q[last]);
         w         = p[last] - apply(b2a, q[last]);
         const S mu = dist - dot(v, w) / dist;
         if(mu < dist * rel_error || mu < abs_error || sv_degenerate(bits, y, w))
@@ -782,16 +832,19 @@ GB_D GjkResult<S> gjk_sv(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
     return r;
 }
 
-// the GJK of a variant (GB_GJK_JH | GB_GJK_SV | GB_GJK_NESTEROV)
+// the GJK of a variant (GB_GJK_JH | GB_GJK_SV | GB_GJK_NESTEROV), optionally
+// with kGjkPaired
 template <int VAR, typename S>
 GB_D GjkResult<S> gjk(const Body<S>& A, const Body<S>& B, const Tr<S>& b2a)
 {
-    if constexpr(VAR == GB_GJK_SV)
-        return gjk_sv<S, false>(A, B, b2a);
-    else if constexpr(VAR == GB_GJK_NESTEROV)
-        return gjk_sv<S, true>(A, B, b2a);
+    constexpr bool PAIRED = (VAR & kGjkPaired) != 0;
+    constexpr int  KIND   = VAR & ~kGjkPaired;
+    if constexpr(KIND == GB_GJK_SV)
+        return gjk_sv<S, false, PAIRED>(A, B, b2a);
+    else if constexpr(KIND == GB_GJK_NESTEROV)
+        return gjk_sv<S, true, PAIRED>(A, B, b2a);
     else
-        return gjk_jh(A, B, b2a);
+        return gjk_jh<S, PAIRED>(A, B, b2a);
 }
 
 } // namespace gb

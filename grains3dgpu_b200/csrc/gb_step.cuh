@@ -443,9 +443,12 @@ __global__ void __launch_bounds__(kBlock)
                 uint32_t nx, uint32_t ny, uint32_t nz, const uint32_t* __restrict__ count,
                 const uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
                 int n_obs, const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
-                uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags)
+                uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
+                uint32_t* __restrict__ gjk_count)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if(a == 0)
+        *gjk_count = 0; // the narrow phase's GJK queue of this step starts empty
     if(a >= n || step_aborted(flags))
         return;
     const uint32_t c = count[a];
@@ -649,11 +652,40 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
 }
 
 // particle pair record p (obstacle records are k_narrow_obstacles'); VAR: the GJK
+// Whether a particle pair reaches GJK: the bounding tests of
+// closestPointsRigidBodies (CollisionDetection.cpp:195-228) as closest_mixed
+// and closest_points evaluate them -- not two spheres (closed form), bounding
+// spheres overlapping, OBBs overlapping -- so that the GJK pass repeats
+// exactly these decisions.
+template <typename S>
+GB_D bool needs_gjk(const Body<S>& A, const Body<S>& B, const M3<S>& RA, const M3<S>& RB,
+                    const double xa[3], const double xb[3], const V3<S>& d)
+{
+    if(A.type == GB_SPHERE && B.type == GB_SPHERE)
+        return false;
+    if constexpr(is_mixed<S>())
+    {
+        const V3<double> d64 = mk<double>(xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]);
+        const V3<float>  df  = cvt3<float>(d64);
+        if(!(norm(df) - (A.rcirc + B.rcirc) < 0.0f))
+            return false;
+        return obb_overlap(A.bb, B.bb, RA, RB, df);
+    }
+    else
+    {
+        if(!(norm(d) - (A.rcirc + B.rcirc) < S(0.0)))
+            return false;
+        return obb_overlap(A.bb, B.bb, RA, RB, d);
+    }
+}
+
 template <typename S, int VAR>
 GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
                       const uint32_t* __restrict__ pair_b, const State<store_t<S>>& st,
                       const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind, int has_kr,
-                      S dt, unsigned long long* __restrict__ counters)
+                      S dt, unsigned long long* __restrict__ counters,
+                      uint32_t* __restrict__ gjk_queue = nullptr,
+                      uint32_t* __restrict__ gjk_count = nullptr)
 {
     const uint32_t a = pair_a[p], b = pair_b[p];
     if(b & kObstacleBit) // k_narrow_obstacles
@@ -676,6 +708,12 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
         oA = mk<S>(S(xa[0]), S(xa[1]), S(xa[2]));
         oB = mk<S>(S(xb[0]), S(xb[1]), S(xb[2]));
         d  = oB - oA;
+    }
+    if(gjk_queue && needs_gjk<S>(A, B, RA, RB, xa, xb, d))
+    {
+        // the GJK pass (k_narrow_gjk) takes this pair and stores its outputs
+        gjk_queue[atomicAdd(gjk_count, 1u)] = (uint32_t)p;
+        return;
     }
     int        iters = 0;
     Contact<S> ci;
@@ -726,6 +764,9 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
             F = hooke_history(L, ci, rel, m1, m2, dt, xi_prev, xi_new, arm);
         }
     }
+    // a lane pair (kGjkPaired) holds the same results: its even lane stores them
+    if((VAR & kGjkPaired) && (threadIdx.x & 1u))
+        return;
     store_pair<S>(po, p, F, xi_new, hit ? kContactParticle : uint8_t(0), law_kind, has_kr, ci, xa);
     if(iters)
         atomicAdd(&counters[1], (unsigned long long)iters);
@@ -757,20 +798,63 @@ GB_D void for_each_pair(int64_t npairs, F&& f)
             f(p);
 }
 
-// The pair count is read on the device (*total, the scan's grand total), so
-// the host launches a resident-sized grid without waiting for it.
+// The particle-particle narrow phase in two passes.  k_narrow walks the pair
+// list (its length is read on the device, *total, the scan's grand total, so
+// the host launches a resident-sized grid without waiting for it): every
+// pair that its bounding tests cull, and every sphere pair, is finished
+// there; a pair that needs GJK goes to a queue instead.  k_narrow_gjk then
+// spreads the queue -- a few hundred to a few thousand pairs -- over all
+// resident warps, so that a warp holds one or two GJK chains rather than
+// every GJK pair among 32 consecutive records of the list.
 template <typename S, int VAR>
 __global__ void __launch_bounds__(128)
     k_narrow(const uint32_t* __restrict__ total, const int* __restrict__ flags,
              const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
              State<store_t<S>> st, Tables<S> tb, PairOut<store_t<S>> po, int law_kind, int has_kr,
-             S dt, unsigned long long* __restrict__ counters)
+             S dt, unsigned long long* __restrict__ counters, uint32_t* __restrict__ gjk_queue,
+             uint32_t* __restrict__ gjk_count)
 {
     if(step_aborted(flags))
         return;
     for_each_pair(*total, [&](int64_t p) {
-        narrow_pair<S, VAR>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters);
+        narrow_pair<S, VAR>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters,
+                            gjk_queue, gjk_count);
     });
+}
+
+// One queued pair per lane pair (kGjkPaired: the two supports of a GJK
+// iteration in parallel); a short queue is spread over all warps as in
+// for_each_pair, a long one walked with a stride.  Both lanes of a pair take
+// the same path throughout, so their shuffles always meet.
+template <typename S, int VAR>
+__global__ void __launch_bounds__(128)
+    k_narrow_gjk(const uint32_t* __restrict__ gjk_count, const int* __restrict__ flags,
+                 const uint32_t* __restrict__ gjk_queue, const uint32_t* __restrict__ pair_a,
+                 const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
+                 PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
+                 unsigned long long* __restrict__ counters)
+{
+    if(step_aborted(flags))
+        return;
+    const int64_t nq     = *gjk_count;
+    const int64_t nslots = ((int64_t)gridDim.x * blockDim.x) >> 1;
+    const int64_t slot   = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
+    auto          one    = [&](int64_t q) {
+        narrow_pair<S, VAR | kGjkPaired>(gjk_queue[q], pair_a, pair_b, st, tb, po, law_kind,
+                                         has_kr, dt, counters);
+    };
+    if(nq < nslots)
+    {
+        const int64_t nwarps = nslots >> 4;                 // 16 lane pairs per warp
+        const int64_t k      = (nq + nwarps - 1) / nwarps;  // <= 16
+        const int64_t pl     = (threadIdx.x & 31) >> 1;     // the lane pair within the warp
+        const int64_t q      = (slot >> 4) * k + pl;
+        if(pl < k && q < nq)
+            one(q);
+    }
+    else
+        for(int64_t q = slot; q < nq; q += nslots)
+            one(q);
 }
 
 // ---- per-particle kernel -------------------------------------------------------
