@@ -294,7 +294,10 @@ def superquadric_column_on_plate(seed=3, n=10_000, column_height=None):
     """Superquadrics with n1, n2 ~ U(2, 8) and semi-axes ~ U(0.8, 1.2) mm in a
     column resting on a plate (its bottom layer within crust range of the
     plate, so contacts exist within the 2,000-step window); initial
-    velocities N(0, 0.05 m/s) per component."""
+    velocities N(0, 0.05 m/s) per component.  The lattice pitch exceeds twice
+    the largest bounding-box half-diagonal, so that no two particles overlap
+    at the start whatever their orientations (randomly oriented boxy grains
+    closer than that start with intersecting cores and blow apart)."""
     rng = np.random.default_rng(seed)
     axes = rng.uniform(0.8e-3, 1.2e-3, size=(n, 3))
     ns = rng.uniform(2.0, 8.0, size=(n, 2))
@@ -304,12 +307,19 @@ def superquadric_column_on_plate(seed=3, n=10_000, column_height=None):
     rbs["crust"] = 0.05 * axes.min(1)
     rbs["density"] = 2500.0
     side = int(np.ceil(np.sqrt(n / 40)))
-    pitch = 2.6e-3
-    box = (side * pitch + 2e-3, side * pitch + 2e-3, 0.2)
-    pos, _ = lattice(box, pitch, 1.0e-3 + 0.5 * pitch - 1.2e-3, n, rng, 0.1e-3)
-    pos[:, 2] += 1.2e-3 - pos[:, 2].min() + 2e-5
+    rmax = float(np.linalg.norm(axes, axis=1).max())
+    pitch = 2.0 * rmax + 0.05e-3
+    margin = rmax + 0.05e-3
+    jitter = 0.02e-3
+    wide = 2 * margin + (side - 0.5) * pitch
+    box = (wide, wide, 0.2 + 40 * pitch)
+    pos, counts = lattice(box, pitch, margin, n, rng, jitter)
     tr = np.zeros((n, 12))
     tr[:, :9] = random_rotations(rng, n)
+    # the bottom layer lowered onto the plate: its lowest OBB corner 20 um up
+    bottom = np.arange(n) < counts[0] * counts[1]
+    h = (np.abs(tr[:, 6:9]) * axes).sum(1)  # OBB half-extent along z
+    pos[bottom, 2] = h[bottom] + 2e-5
     tr[:, 9:] = pos
     vel = np.zeros((n, 6))
     vel[:, :3] = rng.normal(0.0, 0.05, size=(n, 3))
