@@ -42,22 +42,34 @@ def measured_hbm():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-# Algorithmic bytes per phase for one step (unique bytes a phase must move;
-# N particles, C cells, P candidate pairs; S = bytes of a state scalar, 4 in
-# the mixed mode, 8 in FP64; positions are always FP64).
-def phase_bytes(n, c, p, s, quat):
-    rot = (4 if quat else 9) * s
-    shape = 16 + 18 * s + 8          # RBShape record
-    inertia = 14 * s                 # RBInertia record
-    return {
-        "hash": n * (24 + 8),
-        "sort": n * 16,
-        "cell_start": n * (4 + 4 + 24 + 4 + 8 + 32) + 4 * (c + 1),
-        "pair_count": n * (4 + 4 + 32 + 4 + 8) + 4 * (c + 1),
-        "pair_fill": n * (4 + 4 + 32 + 4) + 4 * (c + 1) + 8 * p,
-        "narrow": n * (24 + rot + 4 + shape) + p * (8 + 6 * s + 1),
-        "particle": n * (2 * (24 + rot + 6 * s) + 4 + inertia + 8) + p * (6 * s + 1),
-    }
+# Algorithmic bytes for one step (N particles, C cells; S_p = 8, positions are
+# FP64 in every mode; S = 4 in the mixed mode, 8 in FP64).  The HBM-rated
+# stages, as the hot-path scope defines them:
+#   broad phase (hash, sort, cell start): N (3 S_p + 4 + 4 + 8 + 8 + 4) + 8 C
+#   integration (the per-particle kernel): N (6 S_p + 30 S)
+# and candidate enumeration (the count kernel and its scan): the sorted key,
+# FP64 position + radius, FP32 copy (mixed), id, count and the scan's read and
+# write, N (4 + 32 + 16 + 4 + 4 + 8) + 4 C.  The narrow phase is latency-bound
+# and is rated in pairs and GJK iterations per second instead.
+def stage_bytes(n, c, s):
+    return {"broad_phase": n * (3 * 8 + 4 + 4 + 8 + 8 + 4) + 8 * c,
+            "integration": n * (6 * 8 + 30 * s),
+            "pair_count": n * (4 + 32 + (16 if s == 4 else 0) + 4 + 4 + 8) + 4 * c}
+
+
+STAGE_PHASES = {"broad_phase": ("hash", "sort", "cell_start"), "integration": ("particle",),
+                "pair_count": ("pair_count",)}
+
+
+def stage_report(per_step_ms, n, c, s, hbm):
+    out = {}
+    for stage, names in STAGE_PHASES.items():
+        ms = sum(float(per_step_ms[abi.PHASES.index(k)]) for k in names)
+        b = stage_bytes(n, c, s)[stage]
+        gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out[stage] = {"ms": round(ms, 4), "algorithmic_bytes": b, "achieved_gbs": round(gbs, 1),
+                      "frac_of_measured_hbm": round(gbs / hbm, 4)}
+    return out
 
 
 def clocks_sampler(out_path):
@@ -421,25 +433,25 @@ def main():
     e2e_dev, e2e_wall, h2d, d2h = e2e_engine(sysm, args.e2e_steps, torch)
     e2e_value = world * scene.n * args.e2e_steps / max(e2e_dev, e2e_wall)
     sysm.close()
-    sys_ph, _, _, ms, nsteps, _ = run_engine(args, scene, abi.GB_MIXED, min(args.steps, 10), 3,
-                                             torch, rank, world, timing=True)
+    sys_ph, _, _, ms, nsteps, st_ph = run_engine(args, scene, abi.GB_MIXED, min(args.steps, 10),
+                                                 3, torch, rank, world, timing=True)
     sys_ph.close()
 
-    # per-phase roofline (phase device time from CUDA events on the launch stream)
+    # per-stage roofline (phase device time from CUDA events on the launch stream)
     hbm, hbm_kind = measured_hbm()
     per_step = ms / max(nsteps, 1)
-    pb = phase_bytes(scene.n, st.n_cells, st.candidate_pairs, 4, True)
-    phases = {}
-    for k, name in enumerate(abi.PHASES):
-        sec = per_step[k] / 1e3
-        gbs = pb[name] / sec / 1e9 if sec > 0 else 0.0
-        phases[name] = {"ms": per_step[k], "share": per_step[k] / max(per_step.sum(), 1e-12),
-                        "algorithmic_bytes": pb[name], "achieved_gbs": gbs,
-                        "frac_of_measured_hbm": gbs / hbm}
-    top = max(phases, key=lambda k: phases[k]["ms"])
-    roofline = {"kernel": top, "bound": "hbm", "achieved": phases[top]["achieved_gbs"],
-                "peak": hbm, "unit": "GB/s", "frac": phases[top]["frac_of_measured_hbm"],
-                "traffic": traffic_bytes(top, scene.n), "peak_kind": hbm_kind}
+    stages = stage_report(per_step, scene.n, st.n_cells, 4, hbm)
+    top = max(stages, key=lambda k: stages[k]["ms"])
+    roofline = {"kernel": top, "bound": "hbm", "achieved": stages[top]["achieved_gbs"],
+                "peak": hbm, "unit": "GB/s", "frac": stages[top]["frac_of_measured_hbm"],
+                "traffic": traffic_bytes(top, scene.n), "peak_kind": hbm_kind,
+                "limiter": LIMITER.get(top)}
+    narrow_ms = float(per_step[abi.PHASES.index("narrow")])
+    narrow = {"ms": round(narrow_ms, 4), "candidate_pairs": int(st_ph.candidate_pairs),
+              "pairs_per_s": st_ph.candidate_pairs / (narrow_ms * 1e-3) if narrow_ms else None,
+              "gjk_iterations_per_step": st_ph.gjk_iterations / max(nsteps, 1),
+              "gjk_iterations_per_s": st_ph.gjk_iterations / max(nsteps, 1) / (narrow_ms * 1e-3)
+              if narrow_ms else None}
 
     # the all-FP64 run of the same kernels on the same workload (timed, then
     # instrumented for its phase split)
@@ -475,8 +487,9 @@ def main():
                        "l2": "per-step working set > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline,
-            "phases_ms": {k: round(v["ms"], 4) for k, v in phases.items()},
-            "phases_hbm_frac": {k: round(v["frac_of_measured_hbm"], 4) for k, v in phases.items()},
+            "phases_ms": {k: round(float(v), 4) for k, v in zip(abi.PHASES, per_step)},
+            "stages": stages,
+            "narrow": narrow,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
@@ -484,7 +497,8 @@ def main():
             "fp64": {"value": value64, "ms_per_step": t64 / args.fp64_steps * 1e3,
                      "steps": args.fp64_steps,
                      "phases_ms": {k: round(float(v), 4) for k, v in
-                                   zip(abi.PHASES, ms64 / max(n64, 1))}},
+                                   zip(abi.PHASES, ms64 / max(n64, 1))},
+                     "stages": stage_report(ms64 / max(n64, 1), scene.n, st.n_cells, 8, hbm)},
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
             "adjoint": adj,
@@ -503,8 +517,15 @@ def main():
 # (profiles/k_pair_count_k_narrow_k_particles_superquadrics_1M.md); their
 # traffic scales with the particle count.  The narrow phase's scales with the
 # pairs that reach GJK and is not extrapolated.
-TRAFFIC_PER_PARTICLE = {"particle": (136.10e6 + 28.58e6) / 1_000_000,
+TRAFFIC_PER_PARTICLE = {"integration": (136.10e6 + 28.58e6) / 1_000_000,
                         "pair_count": (62.02e6 + 0.93e6) / 1_000_000}
+
+
+# what bounds each stage, from the ncu capture named above
+LIMITER = {"pair_count": "issue slots: 64% active, 26 of 32 lanes per instruction; "
+                         "~45 L1-resident neighbour tests per particle",
+           "integration": "memory latency: 45% warps active, 33% of DRAM peak",
+           "broad_phase": "launch and tail latency of short kernels"}
 
 
 def traffic_bytes(phase, n):

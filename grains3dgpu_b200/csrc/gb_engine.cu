@@ -72,6 +72,10 @@ struct gb_ctx
     int          n = 0, nrb = 0, nob = 0, nmat = 0;
     bool         rb_set = false, law_set = false, ids_set = false, tr_set = false,
          vel_set = false, obs_set = false;
+    // every particle has its own rigid body, id i for particle i: the
+    // per-particle kernel reads body i without the dependent id load (off once
+    // the ids' device array is handed out for writing)
+    bool rb_identity = false;
 
     // host copies of the set-up
     std::vector<gb_rigid_body_desc>  rbs;
@@ -845,6 +849,7 @@ int run_detect(gb_ctx* c, int phases)
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
     sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
+    sp.rb_identity = c->rb_identity ? 1 : 0;
     // the per-particle contact counts are read only by the detect call
     launch_particles<S>(c, st, tb, po, sp, phases == PHASE_STEP ? nullptr : c->d_contacts);
     GB_CK(cudaGetLastError());
@@ -876,6 +881,7 @@ int run_particles(gb_ctx* c, int phases)
     sp.has_kr     = c->has_kr ? 1 : 0;
     sp.phases     = phases;
     sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
+    sp.rb_identity = c->rb_identity ? 1 : 0;
     PairOut<St> po = pair_out<S>(c);
     launch_particles<S>(c, state_of<St>(c), tables_of<S>(c), po, sp, nullptr);
     GB_CK(cudaGetLastError());
@@ -1357,8 +1363,11 @@ int gb_set_rigid_body_ids(gb_ctx* c, const uint32_t* ids)
         if(ids[i] >= (uint32_t)c->nrb)
             return GB_E_INVALID_ARG;
     GB_CK(cudaMemcpy(c->d_rb_id, ids, c->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    c->ids_set    = true;
-    c->mask_valid = false;
+    c->ids_set     = true;
+    c->mask_valid  = false;
+    c->rb_identity = c->nrb == c->n;
+    for(int i = 0; i < c->n && c->rb_identity; ++i)
+        c->rb_identity = ids[i] == (uint32_t)i;
     return GB_OK;
 }
 
@@ -1808,7 +1817,7 @@ int gb_device_pointer(gb_ctx* c, const char* name, void** ptr)
             return *ptr = (char*)c->d_trq + k * n * ss, GB_OK;
     }
     if(s == "rb_id")
-        return *ptr = c->d_rb_id, GB_OK;
+        return c->rb_identity = false, *ptr = c->d_rb_id, GB_OK;
     if(s == "rotation")
         return *ptr = c->d_rot, GB_OK;
     return GB_E_INVALID_ARG;

@@ -884,6 +884,7 @@ struct StepParams
     int      has_kr;
     int      phases;
     int      accumulate; // PHASE_DETECT adds to the stored torce instead of to zero
+    int      rb_identity; // particle i's rigid body is body i
 };
 
 // The particle-obstacle records of the pair list, one thread per record, in a
@@ -923,7 +924,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
         return;
     if(i == 0)
         atomicAdd(done, 1u); // the host counts the launches that completed
-    const uint32_t            r   = st.rb_id[i];
+    const uint32_t            r   = sp.rb_identity ? (uint32_t)i : st.rb_id[i];
     const RBInertia<store_t<S>>* in = tb.inertia + r;
     const S                   m   = S(in->mass);
     V3<S>                     F, T;
