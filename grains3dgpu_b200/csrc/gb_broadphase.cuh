@@ -401,7 +401,8 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply(const uint32_t* __restric
 // publishes its aggregate, then its inclusive prefix, in one 64-bit word:
 // value in bits 0-31, status in bits 32-33 (1 aggregate, 2 inclusive prefix),
 // the scan's epoch in bits 34-63.  A tile's exclusive prefix is the sum over
-// its predecessors' words back to the first inclusive prefix.  Tiles are
+// its predecessors' words back to the first inclusive prefix, read 32 at a
+// time by one warp.  Tiles are
 // numbered in the order their blocks start (a ticket counter that only grows;
 // `ticket_base` is its value before this launch), so every predecessor of a
 // tile is already running and the look-back ends; a bound on the wait still
@@ -443,39 +444,69 @@ __global__ void __launch_bounds__(kBlock)
     }
     uint32_t       agg;
     const uint32_t ex = block_excl_scan(s, &agg);
-    if(threadIdx.x == 0)
+    // the first warp looks back over 32 predecessors at a time: lane l reads
+    // tile - 1 - l - 32 r; once none of the window is unpublished, the sum up
+    // to the nearest inclusive prefix (or over the whole window) is taken
+    if(threadIdx.x < 32)
     {
-        const uint32_t           ep  = epoch & kScanEpochMask;
-        const unsigned long long tag = (unsigned long long)ep << 34;
+        const unsigned           lane = threadIdx.x;
+        const uint32_t           ep   = epoch & kScanEpochMask;
+        const unsigned long long tag  = (unsigned long long)ep << 34;
         uint32_t                 prefix = 0;
         if(tile > 0)
         {
-            atomicExch(tile_state + tile, tag | (kScanAggregate << 32) | agg);
-            int64_t  p     = (int64_t)tile - 1;
+            if(lane == 0)
+                atomicExch(tile_state + tile, tag | (kScanAggregate << 32) | agg);
+            int64_t  top   = (int64_t)tile - 1; // the window's newest predecessor
             uint32_t spins = 0;
-            while(p >= 0)
+            bool     done  = false;
+            while(!done)
             {
-                const unsigned long long w  = *(volatile unsigned long long*)(tile_state + p);
-                const unsigned long long st = (w >> 32) & 3ull;
-                if((uint32_t)(w >> 34) != ep || st == 0)
+                const int64_t      p = top - (int64_t)lane;
+                unsigned long long w = 0;
+                unsigned long long st;
+                while(true)
                 {
-                    if(++spins > kScanSpinLimit)
+                    if(p < 0)
+                        st = kScanPrefix; // before the first tile: prefix 0
+                    else
                     {
-                        atomicOr(flags, kFlagScanStall);
-                        break;
+                        w  = *(volatile unsigned long long*)(tile_state + p);
+                        st = (uint32_t)(w >> 34) == ep ? (w >> 32) & 3ull : 0ull;
                     }
-                    continue;
+                    if(!__any_sync(0xffffffffu, st == 0ull))
+                        break;
+                    if(++spins > kScanSpinLimit)
+                        break;
                 }
-                prefix += (uint32_t)w;
-                if(st == kScanPrefix)
+                if(spins > kScanSpinLimit)
+                {
+                    if(lane == 0)
+                        atomicOr(flags, kFlagScanStall);
                     break;
-                --p;
+                }
+                const uint32_t v       = p < 0 ? 0u : (uint32_t)w;
+                const unsigned pmask   = __ballot_sync(0xffffffffu, st == kScanPrefix);
+                const int      nearest = pmask ? __ffs(pmask) - 1 : 31;
+                uint32_t       part    = (int)lane <= nearest ? v : 0u;
+#pragma unroll
+                for(int o = 16; o > 0; o >>= 1)
+                    part += __shfl_xor_sync(0xffffffffu, part, o);
+                prefix += part;
+                done = pmask != 0u;
+                top -= 32;
             }
+            if(lane == 0)
+                atomicExch(tile_state + tile, tag | (kScanPrefix << 32) | (prefix + agg));
         }
-        atomicExch(tile_state + tile, tag | (kScanPrefix << 32) | (prefix + agg));
-        s_prefix = prefix;
-        if(grand_total && (int64_t)(tile + 1) * kTile >= n)
-            *grand_total = prefix + agg;
+        else if(lane == 0)
+            atomicExch(tile_state + tile, tag | (kScanPrefix << 32) | agg);
+        if(lane == 0)
+        {
+            s_prefix = prefix;
+            if(grand_total && (int64_t)(tile + 1) * kTile >= n)
+                *grand_total = prefix + agg;
+        }
     }
     __syncthreads();
     uint32_t run = s_prefix + ex;
