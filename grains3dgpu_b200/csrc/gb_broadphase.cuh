@@ -25,9 +25,12 @@ constexpr int kFlagCellCrowded = 1 << 9; // a cell too full for the counting sor
 constexpr int kFlagScanStall   = 1 << 10; // a one-pass scan gave up waiting (never expected)
 constexpr int kFlagAbort = kFlagCapacity | kFlagCellCrowded;
 
+// The flags a kernel checks at entry were set by earlier kernels, so a plain
+// (L1-cached) load sees them; a volatile load from every thread of a
+// million-thread launch would queue a million requests on one L2 line.
 __device__ __forceinline__ bool step_aborted(const int* flags)
 {
-    return flags && (*(volatile const int*)flags & kFlagAbort);
+    return flags && (*flags & kFlagAbort);
 }
 
 // ---- cell hash: LinkedCell::computeCellId / computeLinearCellHash

@@ -126,6 +126,7 @@ struct gb_ctx
     uint32_t *d_skeys = nullptr, *d_sids = nullptr; // results (alias into d_k/d_i)
     uint32_t *d_hist = nullptr, *d_part = nullptr, *d_cstart = nullptr;
     uint32_t* d_ccount   = nullptr; // per-cell counts of the counting sort (C + 1)
+    bool      ccount_zero = false;   // the scatter pass leaves every count at zero
     bool      radix_sort = false;   // a crowded cell was seen: sort with the radix kernels
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
@@ -635,7 +636,8 @@ int broad_phase_counting(gb_ctx* c)
     const int    nb = std::max(1, blocks(n, kBlock));
     cudaStream_t s  = c->stream;
     mark(c, 0);
-    GB_CK(cudaMemsetAsync(c->d_ccount, 0, ((size_t)c->ncells + 1) * sizeof(uint32_t), s));
+    if(!c->ccount_zero)
+        GB_CK(cudaMemsetAsync(c->d_ccount, 0, ((size_t)c->ncells + 1) * sizeof(uint32_t), s));
     k_hash_count<<<nb, kBlock, 0, s>>>(n, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
                                        c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2],
                                        c->cell, c->dims[0], c->dims[1], c->dims[2], c->d_hash,
@@ -645,6 +647,7 @@ int broad_phase_counting(gb_ctx* c)
     mark(c, 1);
     GB_TRY(scan_u32(c, c->d_ccount, c->d_cstart, (int64_t)c->ncells + 1, nullptr));
     k_cell_scatter<<<nb, kBlock, 0, s>>>(n, c->d_hash, c->d_cstart, c->d_ccount, c->d_i[0]);
+    c->ccount_zero = true; // each particle took back the count it added
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 2);
@@ -1277,6 +1280,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
     dfree(c->d_cstart);
     GB_TRY(dalloc(&c->d_cstart, (size_t)nc + 1));
     dfree(c->d_ccount);
+    c->ccount_zero = false;
     GB_TRY(dalloc(&c->d_ccount, (size_t)nc + 1));
     if(c->d_shape64 && c->d_shape64 != c->d_shape)
     {
