@@ -126,6 +126,7 @@ struct gb_ctx
     uint32_t *d_skeys = nullptr, *d_sids = nullptr; // results (alias into d_k/d_i)
     uint32_t *d_hist = nullptr, *d_part = nullptr, *d_cstart = nullptr;
     uint32_t* d_ccount   = nullptr; // per-cell counts of the counting sort (C + 1)
+    bool      count_zero = false;   // the fill pass leaves the candidate counts at zero
     bool      ccount_zero = false;   // the scatter pass leaves every count at zero
     bool      radix_sort = false;   // a crowded cell was seen: sort with the radix kernels
     double4*  d_spos = nullptr;
@@ -705,7 +706,8 @@ int build_pairs(gb_ctx* c)
         GB_CK(cudaGetLastError());
         c->mask_valid = true;
     }
-    GB_CK(cudaMemsetAsync(c->d_count, 0, 2 * ((size_t)n + 1) * sizeof(uint32_t), s));
+    if(!c->count_zero)
+        GB_CK(cudaMemsetAsync(c->d_count, 0, 2 * ((size_t)n + 1) * sizeof(uint32_t), s));
     k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
                                           c->dims[0], c->dims[1], c->dims[2], c->d_count,
                                           c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob);
@@ -716,7 +718,9 @@ int build_pairs(gb_ctx* c)
     k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_sorted_of, c->d_spos,
                                          spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
                                          c->d_count, c->d_slot, c->d_obsmask_id, c->nob, off,
-                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags, c->d_gjkn);
+                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags, c->d_gjkn,
+                                         c->d_count + n + 1);
+    c->count_zero = true; // the fill pass zeroes each count it reads
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 5);
@@ -966,6 +970,7 @@ void restore(gb_ctx* c, const StepSnap& s)
     c->detect_valid   = s.detect_valid;
     c->links_valid    = s.links_valid;
     c->steps_done     = s.steps_done;
+    c->count_zero     = false; // an aborted fill pass may have left counts behind
 }
 
 // Launches n_steps detects (PHASE_DETECT) or fused steps (PHASE_STEP) with no

@@ -442,11 +442,11 @@ __global__ void __launch_bounds__(kBlock)
     k_pair_fill(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                 const uint32_t* __restrict__ sorted_of, const double4* __restrict__ spos,
                 const float4* __restrict__ spos32, const uint32_t* __restrict__ cstart,
-                uint32_t nx, uint32_t ny, uint32_t nz, const uint32_t* __restrict__ count,
+                uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* __restrict__ count,
                 const uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
                 int n_obs, const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
-                uint32_t* __restrict__ gjk_count)
+                uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if(a == 0)
@@ -463,6 +463,10 @@ __global__ void __launch_bounds__(kBlock)
         atomicOr(flags, kFlagCapacity);
         return;
     }
+    // the count pass's counters start the next step at zero (an aborted step
+    // leaves them for the host's memset before its replay)
+    count[a] = 0u;
+    pslot[s] = 0u;
     const uint32_t mask = n_obs ? mask_by_id[a] : 0u;
     const uint32_t cp   = c - (uint32_t)obstacle_candidates(mask, n_obs);
     if(cp <= kPairSlots)
