@@ -514,17 +514,17 @@ def main():
 
 # DRAM bytes (read + write) per particle of the dominant kernels, from one
 # ncu capture of this workload with 1,000,000 particles
-# (profiles/k_pair_count_k_narrow_k_particles_superquadrics_1M.md); their
+# (profiles/k_pair_count_k_narrow_gjk_k_particles_superquadrics_1M.md); their
 # traffic scales with the particle count.  The narrow phase's scales with the
 # pairs that reach GJK and is not extrapolated.
-TRAFFIC_PER_PARTICLE = {"integration": (136.10e6 + 28.58e6) / 1_000_000,
-                        "pair_count": (62.02e6 + 0.93e6) / 1_000_000}
+TRAFFIC_PER_PARTICLE = {"integration": (132.09e6 + 28.99e6) / 1_000_000,
+                        "pair_count": (62.03e6 + 1.48e6) / 1_000_000}
 
 
 # what bounds each stage, from the ncu capture named above
-LIMITER = {"pair_count": "issue slots: 64% active, 26 of 32 lanes per instruction; "
-                         "~45 L1-resident neighbour tests per particle",
-           "integration": "memory latency: 45% warps active, 33% of DRAM peak",
+LIMITER = {"pair_count": "issue slots: 71% active, 26 of 32 lanes per instruction; "
+                         "~48 L1-resident neighbour tests per particle",
+           "integration": "memory latency: 55% warps active, 34% of DRAM peak",
            "broad_phase": "launch and tail latency of short kernels"}
 
 
