@@ -68,6 +68,28 @@ def test_broad_phase_and_pairs_bit_exact(gb, oracle, kind):
     assert g.stats().contacts + g.stats().obstacle_contacts > 0
 
 
+@pytest.mark.parametrize("precision", [abi.GB_FP64_STRICT, abi.GB_MIXED])
+def test_broad_phase_and_pairs_bit_exact_large(gb, oracle, precision):
+    """The benchmark packing, 1,000,000 polydisperse superquadrics: ~500 tiles
+    in each one-pass scan, so the look-back across tiles is exercised; cell
+    hashes, sorted ids, cell starts, neighbour counts, candidate and contact
+    pairs equal the oracle's, and so do the mixed mode's (its FP32 pre-test
+    is certified)."""
+    scene = scenes.polydisperse_superquadrics(n=1_000_000)
+    g = scenes.System(gb, scene, precision=precision, flags=abi.GB_FLAG_RECORD_CONTACT_INFO)
+    o = scenes.System(oracle, scene)
+    share_props(g, o, oracle)
+    g.detect()
+    o.detect()
+    for kind_ in BROAD_DUMPS + [abi.GB_DUMP_CONTACT_PAIRS]:
+        a, b = g.dump(kind_), o.dump(kind_)
+        assert a.shape == b.shape and np.array_equal(a, b), f"dump {kind_} differs"
+    assert g.dump(abi.GB_DUMP_CANDIDATE_PAIRS).shape[0] > 1000
+    assert g.stats().contacts == o.stats().contacts
+    g.close()
+    o.close()
+
+
 @pytest.mark.parametrize("kind", ["sphere", "box-on-walls", "polyhedron"])
 def test_single_step_torce_bit_exact(gb, oracle, kind):
     scene = make_scene(kind)
