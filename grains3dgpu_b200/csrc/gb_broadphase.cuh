@@ -295,7 +295,8 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
-// ---- exclusive scan of uint32 (three kernels, no inter-block waiting) -------
+// ---- exclusive scan of uint32 in three kernels, no inter-block waiting ------
+// (the static-scratch sort's scan; the engine's scans use k_scan_onepass below)
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
 {
     const int lane = threadIdx.x & 31;

@@ -175,7 +175,7 @@ GB_D Law<S> load_law(const Law<store_t<S>>* t, int ma, int mb)
 // The three cells x-1, x, x+1 of one (y, z) row have consecutive keys, so
 // their particles are one contiguous range of the sorted order: the walk is
 // nine ranges, visiting the candidates in the same order as the 27 cells.
-// PRE32 (the mixed mode): a conservative FP32 test on spos32 (k_gather_sorted
+// PRE32 (the mixed mode): a conservative FP32 test on spos32 (put_sorted
 // inflates its radii by a bound on the FP32 rounding, so an FP32 rejection
 // implies an FP64 rejection) skips most non-candidates before the FP64 test:
 // the candidate set is the FP64 test's.  The FP64 modes test in FP64 only.
@@ -281,7 +281,7 @@ GB_D constexpr bool is_strict()
 // The candidate test of sorted particles a and b: |d| - (rA + rB) < 0 in
 // FP64 (ComponentManagerCPU.cpp:372-380; the strict mode in the reference's
 // operation order), behind the FP32 pre-test of the mixed mode, whose
-// rejection is certified (k_gather_sorted inflates the FP32 radii).  The
+// rejection is certified (put_sorted inflates the FP32 radii).  The
 // products and sums are written as explicit round-to-nearest operations, so
 // that every kernel that enumerates candidates -- the count pass and the
 // re-enumeration of the fill pass -- takes the same decisions.

@@ -64,7 +64,7 @@ extern "C" {
 
 /* ---- run modes -------------------------------------------------------------- */
 #define GB_FP64 0        /* every kernel in double precision, FMA contraction on  */
-#define GB_MIXED 1       /* FP32 bulk; FP64 positions, FP64 GJK polish near contact */
+#define GB_MIXED 1       /* FP32 bulk; FP64 positions and candidate tests, FP64 GJK */
 #define GB_FP64_STRICT 2 /* FP64 in the reference's IEEE operation order (no FMA
                             contraction): the parity mode                          */
 

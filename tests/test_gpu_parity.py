@@ -247,7 +247,7 @@ def test_rerun_is_bitwise_deterministic(gb):
 
 @pytest.mark.parametrize("kind", ["superquadric", "polyhedron", "box-on-walls"])
 def test_mixed_precision_single_step(gb, kind):
-    """Mixed mode (FP32 bulk, FP64 positions and GJK polish near contact)
+    """Mixed mode (FP32 bulk, FP64 positions, FP64 GJK past the bounding tests)
     against the FP64 mode from one identical state: same contact pairs, and
     force error <= 1e-5 of the largest force."""
     scene = make_scene(kind)
