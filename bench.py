@@ -248,6 +248,39 @@ def measure_adjoint(torch, n, steps):
             "adjoint_over_forward": t_bwd / t_plain}
 
 
+def measure_shapes(args, torch):
+    """The same step on the other benchmark shapes, mixed and FP64, on one
+    GPU: 200,000 convex polyhedra (hulls of 8-32 points on an ellipsoid, the
+    polyhedra packing) and 1,000,000 spheres (the sphere bed, every lattice
+    neighbour in contact)."""
+    from grains3dgpu_b200 import engine
+    lib = engine.load()
+
+    def centroid(v):
+        c, vol = np.zeros(3), abi.C.c_double(0.0)
+        assert lib.convex_hull_centroid(abi.dptr(np.ascontiguousarray(v)), v.shape[0],
+                                        abi.dptr(c), abi.C.byref(vol)) == 0
+        return c
+
+    out = {}
+    cases = (("polyhedra_200k", lambda: scenes.polyhedra_box(n=200_000, hull_centroid=centroid)),
+             ("spheres_1M", lambda: scenes.sphere_bed(seed=4, n=1_000_000,
+                                                      box=adjoint_box(1_000_000))))
+    for name, build in cases:
+        scene, res = build(), {}
+        for prec, key in ((abi.GB_MIXED, "mixed"), (abi.GB_FP64, "fp64")):
+            s, el, _, _, _, st = run_engine(args, scene, prec, args.shape_steps, 3, torch, 0, 1,
+                                            timing=False)
+            s.close()
+            res[key] = {"value": scene.n * args.shape_steps / el,
+                        "ms_per_step": el / args.shape_steps * 1e3}
+        res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+        res["n_particles"] = scene.n
+        res["candidate_pairs_last_step"] = int(st.candidate_pairs)
+        out[name] = res
+    return out
+
+
 def force_error(scene, torch):
     """Single-step force error of the mixed mode against the FP64 mode from
     one identical state: max |F_mixed - F_fp64| over particles divided by
@@ -400,6 +433,8 @@ def main():
     ap.add_argument("--adjoint-n", type=int, default=1_000_000)
     ap.add_argument("--adjoint-steps", type=int, default=10)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--shape-steps", type=int, default=10)
+    ap.add_argument("--no-shapes", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -465,6 +500,10 @@ def main():
     value64 = aggregate(world, scene.n, args.fp64_steps, t64)
     ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
 
+    shapes = None
+    if world == 1 and not args.no_shapes:
+        shapes = measure_shapes(args, torch)
+
     adj = None
     if world == 1 and not args.no_adjoint:
         adj = measure_adjoint(torch, args.adjoint_n, args.adjoint_steps)
@@ -502,6 +541,7 @@ def main():
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
             "adjoint": adj,
+            "other_shapes": shapes,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
