@@ -3,9 +3,17 @@
 Workload: the mixed-precision configuration -- 1,000,000 polydisperse
 superquadrics (equivalent radius lognormal, median 1 mm, sigma 0.25, clipped
 to 0.5-2 mm; b/a, c/a ~ U(0.5, 2); n1, n2 ~ U(2, 10)) on a jittered lattice in a
-closed 0.3 x 0.3 x 1.2 m box, dt = 1e-6 s, Hooke law kn=1e4 N/m, en=0.7,
+closed 0.3 x 0.3 x 1.2 m box, dt = 1e-6 s, linear spring-dashpot kn=1e4 N/m,
+en=0.7, tangential stiffness 0.8 kn with per-pair tangential history, Coulomb
 mu=0.5, gravity -z.  One step = one GrainsCPU::simulate loop iteration
 (collide + force, gravity, move) over all particles.
+
+The engine arm runs the tangential-history law (GB_LAW_HOOKE_HISTORY), the
+workload's law.  The reference has only its Hooke law, whose relative
+velocity takes the absolute contact point as lever arm: in this 1.2 m tall box
+a spinning grain's damping force grows with its height, and the packing blows
+up within ~100 steps.  The reference CPU path (cpu_baseline, --impl reference)
+is timed with that Hooke law, a little less work per contact.
 
   python bench.py [--gpus N --steps K --warmup W]          the engine (mixed)
   python bench.py --impl reference [...]                   the reference CPU path
@@ -28,6 +36,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from grains3dgpu_b200 import abi, scenes  # noqa: E402
+
+LAW = abi.GB_LAW_HOOKE_HISTORY  # the engine arm's contact law
 
 HBM_FALLBACK_GBS = 6650.0
 METRIC = "particle-steps/s"
@@ -132,7 +142,7 @@ def run_engine(args, scene, precision, steps, warmup, torch, rank, world, timing
     lib = engine.load()
     flags = abi.GB_FLAG_PHASE_TIMING if timing else 0
     sysm = scenes.System(lib, scene, precision=precision, device=torch.cuda.current_device(),
-                         flags=flags)
+                         flags=flags, contact_law=LAW)
     stream = torch.cuda.current_stream()
     assert lib.set_stream(sysm.ctx, abi.C.c_void_p(stream.cuda_stream)) == 0
     for _ in range(warmup):
@@ -289,7 +299,8 @@ def force_error(scene, torch):
     lib = engine.load()
     out = {}
     for prec in (abi.GB_MIXED, abi.GB_FP64):
-        s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device())
+        s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device(),
+                          contact_law=LAW)
         s.detect()
         out[prec] = (s.torces(), s.stats().contacts)
         s.close()
@@ -522,6 +533,8 @@ def main():
             "config": {"workload": f"{scene.n:,} polydisperse superquadrics in a "
                                    "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision",
                        "n_particles": scene.n, "precision": "mixed",
+                       "contact_law": "linear spring-dashpot, kt = 0.8 kn, Coulomb mu = 0.5, "
+                                      "per-pair tangential history",
                        "n_cells": st.n_cells, "candidate_pairs_last_step": st.candidate_pairs,
                        "l2": "per-step working set > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}"},

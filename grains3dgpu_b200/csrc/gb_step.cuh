@@ -914,12 +914,12 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
-// A latency-bound streaming kernel: the mixed instantiation runs five
-// 256-thread blocks per SM at 48 registers (a few spilled values of the rare
-// paths) for more loads in flight, which measured faster than four blocks at
-// 64; the FP64 ones need about 100 registers and get two blocks.
+// A latency-bound streaming kernel.  Its loads are all issued before the pair
+// loop; holding them takes the mixed instantiation to 64 registers (four
+// 256-thread blocks per SM, which measured faster than five blocks at 48 with
+// spills); the FP64 ones need about 100 registers and get two blocks.
 template <typename S>
-__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
+__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
                 uint32_t* __restrict__ mask_out, const int* __restrict__ flags,
@@ -928,14 +928,39 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n || step_aborted(flags))
         return;
-    if(i == 0)
-        atomicAdd(done, 1u); // the host counts the launches that completed
     const uint32_t            r   = sp.rb_identity ? (uint32_t)i : st.rb_id[i];
     const RBInertia<store_t<S>>* in = tb.inertia + r;
     const S                   m   = S(in->mass);
     V3<S>                     F, T;
     V3<S>                     v = load3<S>(st.vel, i), w = load3<S>(st.omg, i);
     int                       nc = 0;
+    // The pose and the body record do not depend on the pair loop: they are
+    // loaded before it, and every store comes after all loads, so that these
+    // loads and the loop's gathers are in flight together.
+    const bool move = (sp.phases & PHASE_MOVE) != 0;
+    S          I[6], I1[6];
+    Quat<S>    q;
+    M3<S>      R;
+    double     x0[3];
+    if(move)
+    {
+#pragma unroll
+        for(int k = 0; k < 6; ++k)
+        {
+            I[k]  = S(in->I[k]);
+            I1[k] = S(in->I1[k]);
+        }
+        if constexpr(is_mixed<S>())
+        {
+            q.w = S(st.rot[0][i]);
+            q.v = mk<S>(S(st.rot[1][i]), S(st.rot[2][i]), S(st.rot[3][i]));
+        }
+        else
+            R = load_rot<S>(st, i);
+#pragma unroll
+        for(int k = 0; k < 3; ++k)
+            x0[k] = st.pos[k][i];
+    }
     if(sp.phases & PHASE_DETECT)
     {
         // Torce::addForce onto the torce accumulated since the last move
@@ -962,8 +987,6 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
             if(sp.has_kr)
                 T = T + mk<S>(S(po.m[0][p]), S(po.m[1][p]), S(po.m[2][p]));
         }
-        if(contacts_out)
-            contacts_out[i] = nc;
     }
     else
     {
@@ -972,29 +995,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
     }
     if(sp.phases & PHASE_GRAVITY)
         F = F + m * sp.g; // Torce::addForce(mass * g)
-    if(sp.phases & PHASE_MOVE)
+    if(move)
     {
         // RigidBody::computeMomentum + FirstOrderExplicit::Move
         // (RigidBody.cpp:267-307, FirstOrderExplicit.cpp:46-60) or the Verlet kick-drift
-        S I[6], I1[6];
-#pragma unroll
-        for(int k = 0; k < 6; ++k)
-        {
-            I[k]  = S(in->I[k]);
-            I1[k] = S(in->I1[k]);
-        }
-        Quat<S> q;
-        M3<S>   R;
-        if constexpr(is_mixed<S>())
-        {
-            q.w = S(st.rot[0][i]);
-            q.v = mk<S>(S(st.rot[1][i]), S(st.rot[2][i]), S(st.rot[3][i]));
-        }
-        else
-        {
-            R = load_rot<S>(st, i);
+        if constexpr(!is_mixed<S>())
             q = quat_from_basis(R);
-        }
         const V3<S> acc   = mk<S>(F.x / m, F.y / m, F.z / m);
         const V3<S> alpha = angular_acceleration(I, I1, w, T, q);
         V3<S>       trans;
@@ -1020,9 +1026,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
         {
             const S tk[3] = {trans.x, trans.y, trans.z};
             if constexpr(is_mixed<S>())
-                xn[k] = st.pos[k][i] + (double)tk[k];
+                xn[k] = x0[k] + (double)tk[k];
             else
-                xn[k] = to_d(S(st.pos[k][i]) + tk[k]);
+                xn[k] = to_d(S(x0[k]) + tk[k]);
             st.pos[k][i] = xn[k];
         }
         if constexpr(is_mixed<S>())
@@ -1076,6 +1082,10 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 5 : 2)
         st.trq[1][i] = (store_t<S>)to_d(T.y);
         st.trq[2][i] = (store_t<S>)to_d(T.z);
     }
+    if(contacts_out && (sp.phases & PHASE_DETECT))
+        contacts_out[i] = nc;
+    if(i == 0)
+        atomicAdd(done, 1u); // the host counts the launches that completed
 }
 
 } // namespace gb
