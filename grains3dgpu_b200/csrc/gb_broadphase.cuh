@@ -33,6 +33,19 @@ __device__ __forceinline__ bool step_aborted(const int* flags)
     return flags && (*flags & kFlagAbort);
 }
 
+// Programmatic dependent launch: the kernels of a step are launched with the
+// stream-serialization attribute relaxed, so that one is scheduled while the
+// stream's previous kernel drains.  Each of them calls this first: it waits
+// until the previous kernel has completed and its writes are visible (and so
+// all earlier work of the stream), then lets the next kernel launch in turn.
+// It comes before every return path, so that a kernel's completion still
+// implies its predecessor's.  Without the attribute both are no-ops.
+__device__ __forceinline__ void grid_dep_sync()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---- cell hash: LinkedCell::computeCellId / computeLinearCellHash
 //      (Grains/Component/src/LinkedCell.cpp:117-159): floor((p - min)/extent)
 //      in IEEE double, linear hash (z*ny + y)*nx + x.  Out-of-grid centres are
@@ -97,6 +110,7 @@ __global__ void k_hash_count(int n, const double* __restrict__ px, const double*
                              uint32_t* __restrict__ keys, uint32_t* __restrict__ count,
                              int* __restrict__ flags)
 {
+    grid_dep_sync();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n)
         return;
@@ -135,6 +149,7 @@ __global__ void k_cell_scatter(int n, const uint32_t* __restrict__ keys,
                                const uint32_t* __restrict__ cstart, uint32_t* __restrict__ count,
                                uint32_t* __restrict__ unordered)
 {
+    grid_dep_sync();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n)
         return;
@@ -178,6 +193,7 @@ __global__ void k_cell_rank(int n, const uint32_t* __restrict__ unordered,
                             float4* __restrict__ out32, uint32_t* __restrict__ sorted_of,
                             int* __restrict__ flags)
 {
+    grid_dep_sync();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if(t >= n)
         return;
@@ -424,6 +440,7 @@ __global__ void __launch_bounds__(kBlock)
                    uint32_t epoch, uint32_t* __restrict__ grand_total,
                    const int* abort_flags, int* __restrict__ flags)
 {
+    grid_dep_sync();
     __shared__ uint32_t s_tile, s_prefix;
     if(threadIdx.x == 0)
         s_tile = (uint32_t)(atomicAdd(ticket, 1ull) - ticket_base);

@@ -44,6 +44,27 @@ inline int blocks(int64_t n, int b)
     return (int)((n + b - 1) / b);
 }
 
+// Launches kernel k.  With pdl set, the launch is a programmatic dependent
+// one: the GPU may schedule it while the stream's previous kernel drains, and
+// the kernel's grid_dep_sync() holds it until that kernel has completed.
+// Only kernels that call grid_dep_sync() first are launched this way, and only
+// where their other dependencies are stream order (no cross-stream wait).
+template <typename... P, typename... A>
+cudaError_t launch(bool pdl, void (*k)(P...), int grid, int block, cudaStream_t s, A&&... args)
+{
+    cudaLaunchAttribute attr[1];
+    attr[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg                             = {};
+    cfg.gridDim                                        = dim3((unsigned)grid);
+    cfg.blockDim                                       = dim3((unsigned)block);
+    cfg.dynamicSmemBytes                               = 0;
+    cfg.stream                                         = s;
+    cfg.attrs                                          = attr;
+    cfg.numAttrs                                       = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 template <typename T>
 int dalloc(T** p, size_t count)
 {
@@ -129,6 +150,7 @@ struct gb_ctx
     bool      count_zero = false;   // the fill pass leaves the candidate counts at zero
     bool      ccount_zero = false;   // the scatter pass leaves every count at zero
     bool      radix_sort = false;   // a crowded cell was seen: sort with the radix kernels
+    bool      pdl        = true;    // programmatic dependent launches within a step
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
@@ -550,9 +572,8 @@ int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* 
                               c->stream));
         c->scan_epoch = 1;
     }
-    k_scan_onepass<<<nb, kBlock, 0, c->stream>>>(in, out, n, c->d_tile_state, c->d_ticket,
-                                                  c->tickets, c->scan_epoch, d_total,
-                                                  abort_flags, c->d_flags);
+    GB_CK(launch(c->pdl, k_scan_onepass, nb, kBlock, c->stream, in, out, n, c->d_tile_state,
+                 c->d_ticket, c->tickets, c->scan_epoch, d_total, abort_flags, c->d_flags));
     c->tickets += (unsigned long long)nb;
     c->launches += 1;
     GB_CK(cudaGetLastError());
@@ -639,26 +660,26 @@ int broad_phase_counting(gb_ctx* c)
     mark(c, 0);
     if(!c->ccount_zero)
         GB_CK(cudaMemsetAsync(c->d_ccount, 0, ((size_t)c->ncells + 1) * sizeof(uint32_t), s));
-    k_hash_count<<<nb, kBlock, 0, s>>>(n, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
-                                       c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2],
-                                       c->cell, c->dims[0], c->dims[1], c->dims[2], c->d_hash,
-                                       c->d_ccount, c->d_flags);
+    GB_CK(launch(c->pdl, k_hash_count, nb, kBlock, s, n, c->d_pos, c->d_pos + n,
+                 c->d_pos + 2 * (size_t)n, c->cfg.origin[0], c->cfg.origin[1], c->cfg.origin[2],
+                 c->cell, c->dims[0], c->dims[1], c->dims[2], c->d_hash, c->d_ccount,
+                 c->d_flags));
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 1);
     GB_TRY(scan_u32(c, c->d_ccount, c->d_cstart, (int64_t)c->ncells + 1, nullptr));
-    k_cell_scatter<<<nb, kBlock, 0, s>>>(n, c->d_hash, c->d_cstart, c->d_ccount, c->d_i[0]);
+    GB_CK(launch(c->pdl, k_cell_scatter, nb, kBlock, s, n, c->d_hash, c->d_cstart, c->d_ccount,
+                 c->d_i[0]));
     c->ccount_zero = true; // each particle took back the count it added
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 2);
     c->d_skeys = c->d_k[1];
     c->d_sids  = c->d_i[1];
-    k_cell_rank<<<nb, kBlock, 0, s>>>(n, c->d_i[0], c->d_hash, c->d_cstart, c->d_skeys, c->d_sids,
-                                      c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
-                                      c->d_rb_id, c->d_rcirc64, c->d_spos,
-                                      c->prec == GB_MIXED ? c->d_spos32 : nullptr,
-                                      c->d_sorted_of, c->d_flags);
+    GB_CK(launch(c->pdl, k_cell_rank, nb, kBlock, s, n, c->d_i[0], c->d_hash, c->d_cstart,
+                 c->d_skeys, c->d_sids, c->d_pos, c->d_pos + n, c->d_pos + 2 * (size_t)n,
+                 c->d_rb_id, c->d_rcirc64, c->d_spos, c->prec == GB_MIXED ? c->d_spos32 : nullptr,
+                 c->d_sorted_of, c->d_flags));
     c->launches += 1;
     GB_CK(cudaGetLastError());
     mark(c, 3);
@@ -700,26 +721,25 @@ int build_pairs(gb_ctx* c)
     const float4*   spos32 = c->prec == GB_MIXED ? c->d_spos32 : nullptr;
     if(c->nob && !c->mask_valid)
     {
-        k_obstacle_mask<S><<<nb, kBlock, 0, s>>>(n, state_of<St>(c), tables_of<S>(c),
-                                                 c->d_obsmask_id);
+        GB_CK(launch(c->pdl, k_obstacle_mask<S>, nb, kBlock, s, n, state_of<St>(c),
+                     tables_of<S>(c), c->d_obsmask_id));
         c->launches += 1;
         GB_CK(cudaGetLastError());
         c->mask_valid = true;
     }
     if(!c->count_zero)
         GB_CK(cudaMemsetAsync(c->d_count, 0, 2 * ((size_t)n + 1) * sizeof(uint32_t), s));
-    k_pair_count<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_spos, spos32, c->d_cstart,
-                                          c->dims[0], c->dims[1], c->dims[2], c->d_count,
-                                          c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob);
+    GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_spos,
+                 spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                 c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob));
     c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));
     mark(c, 4);
-    k_pair_fill<S><<<nb, kBlock, 0, s>>>(n, c->d_skeys, c->d_sids, c->d_sorted_of, c->d_spos,
-                                         spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
-                                         c->d_count, c->d_slot, c->d_obsmask_id, c->nob, off,
-                                         c->d_pa, c->d_pb[c->cur], c->cap, c->d_flags, c->d_gjkn,
-                                         c->d_count + n + 1);
+    GB_CK(launch(c->pdl, k_pair_fill<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_sorted_of,
+                 c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                 c->d_slot, c->d_obsmask_id, c->nob, off, c->d_pa, c->d_pb[c->cur], c->cap,
+                 c->d_flags, c->d_gjkn, c->d_count + n + 1));
     c->count_zero = true; // the fill pass zeroes each count it reads
     c->launches += 1;
     GB_CK(cudaGetLastError());
@@ -751,18 +771,21 @@ PairOut<store_t<S>> pair_out(gb_ctx* c)
 }
 
 template <typename S>
-void launch_particles(gb_ctx* c, const State<store_t<S>>& st, const Tables<S>& tb,
+int launch_particles(gb_ctx* c, const State<store_t<S>>& st, const Tables<S>& tb,
                       const PairOut<store_t<S>>& po, const StepParams<S>& sp, int* contacts_out)
 {
     const int  nb   = std::max(1, blocks(c->n, kBlock));
     const bool move = (sp.phases & PHASE_MOVE) != 0;
-    k_particles<S><<<nb, kBlock, 0, c->stream>>>(c->n, st, tb, c->d_off[c->cur], po, sp,
-                                                 contacts_out,
-                                                 move && c->nob ? c->d_obsmask_id : nullptr,
-                                                 c->d_flags, c->d_done);
+    // after a detect with obstacles the stream waits on the auxiliary one:
+    // a plain launch there
+    const bool pdl = c->pdl && !(c->nob && (sp.phases & PHASE_DETECT));
+    GB_CK(launch(pdl, k_particles<S>, nb, kBlock, c->stream, c->n, st, tb, c->d_off[c->cur], po,
+                 sp, contacts_out, move && c->nob ? c->d_obsmask_id : nullptr, c->d_flags,
+                 c->d_done));
     c->launches += 1;
     if(move)
         c->mask_valid = c->nob > 0;
+    return GB_OK;
 }
 
 template <typename S>
@@ -810,12 +833,12 @@ int run_detect(gb_ctx* c, int phases)
                 GB_CK(cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
                 so = c->aux_stream;
             }
-            k_narrow<S, VAR><<<one_wave((const void*)k_narrow<S, VAR>), 128, 0, s>>>(
-                total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr, S(c->cfg.dt),
-                c->d_counters, c->d_gjkq, c->d_gjkn);
-            k_narrow_gjk<S, VAR><<<one_wave((const void*)k_narrow_gjk<S, VAR>), 128, 0, s>>>(
-                c->d_gjkn, c->d_flags, c->d_gjkq, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
-                S(c->cfg.dt), c->d_counters);
+            GB_CK(launch(c->pdl, k_narrow<S, VAR>, one_wave((const void*)k_narrow<S, VAR>), 128, s,
+                         total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
+                         S(c->cfg.dt), c->d_counters, c->d_gjkq, c->d_gjkn));
+            GB_CK(launch(c->pdl, k_narrow_gjk<S, VAR>, one_wave((const void*)k_narrow_gjk<S, VAR>),
+                         128, s, c->d_gjkn, c->d_flags, c->d_gjkq, c->d_pa, c->d_pb[c->cur], st,
+                         tb, po, law, kr, S(c->cfg.dt), c->d_counters));
             c->launches += 2;
             if(!c->nob)
                 return GB_OK;
@@ -858,7 +881,7 @@ int run_detect(gb_ctx* c, int phases)
     sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
     sp.rb_identity = c->rb_identity ? 1 : 0;
     // the per-particle contact counts are read only by the detect call
-    launch_particles<S>(c, st, tb, po, sp, phases == PHASE_STEP ? nullptr : c->d_contacts);
+    GB_TRY(launch_particles<S>(c, st, tb, po, sp, phases == PHASE_STEP ? nullptr : c->d_contacts));
     GB_CK(cudaGetLastError());
     mark(c, 7);
     close_event_set(c);
@@ -890,7 +913,7 @@ int run_particles(gb_ctx* c, int phases)
     sp.accumulate = (phases & PHASE_DETECT) && c->torce_dirty ? 1 : 0;
     sp.rb_identity = c->rb_identity ? 1 : 0;
     PairOut<St> po = pair_out<S>(c);
-    launch_particles<S>(c, state_of<St>(c), tables_of<S>(c), po, sp, nullptr);
+    GB_TRY(launch_particles<S>(c, state_of<St>(c), tables_of<S>(c), po, sp, nullptr));
     GB_CK(cudaGetLastError());
     if(phases & PHASE_MOVE)
     {

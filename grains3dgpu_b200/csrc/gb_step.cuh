@@ -260,6 +260,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_obstacle_mask(int n, State<store_t<S>> st, Tables<S> tb, uint32_t* __restrict__ mask)
 {
+    grid_dep_sync();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n)
         return;
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
                  uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
                  uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs)
 {
+    grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
     const int      s      = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= n)
@@ -448,6 +450,7 @@ __global__ void __launch_bounds__(kBlock)
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
                 uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot)
 {
+    grid_dep_sync();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if(a == 0)
         *gjk_count = 0; // the narrow phase's GJK queue of this step starts empty
@@ -820,6 +823,7 @@ __global__ void __launch_bounds__(128)
              S dt, unsigned long long* __restrict__ counters, uint32_t* __restrict__ gjk_queue,
              uint32_t* __restrict__ gjk_count)
 {
+    grid_dep_sync();
     if(step_aborted(flags))
         return;
     for_each_pair(*total, [&](int64_t p) {
@@ -840,6 +844,7 @@ __global__ void __launch_bounds__(128)
                  PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
                  unsigned long long* __restrict__ counters)
 {
+    grid_dep_sync();
     if(step_aborted(flags))
         return;
     const int64_t nq     = *gjk_count;
@@ -925,6 +930,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
                 uint32_t* __restrict__ mask_out, const int* __restrict__ flags,
                 unsigned int* __restrict__ done)
 {
+    grid_dep_sync();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n || step_aborted(flags))
         return;
