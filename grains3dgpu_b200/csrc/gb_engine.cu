@@ -125,6 +125,7 @@ struct gb_ctx
     double4* d_obs_plane = nullptr; // Rectangle planes: normal, normal . origin
     uint32_t obs_rect    = 0u;      // bit o: obstacle o (< 32) is a Rectangle
     double*  d_rcirc64 = nullptr;
+    double   rmax      = 0.0;     // the largest circumscribed radius (the candidate test's radius)
     // FP64 shape tables: aliases of the above in the FP64 modes, separate
     // copies in the mixed mode (read by its FP64 GJK)
     void* d_shape64 = nullptr;
@@ -729,8 +730,13 @@ int build_pairs(gb_ctx* c)
     }
     if(!c->count_zero)
         GB_CK(cudaMemsetAsync(c->d_count, 0, 2 * ((size_t)n + 1) * sizeof(uint32_t), s));
+    CellGeometry geo;
+    for(int k = 0; k < 3; ++k)
+        geo.mn[k] = c->cfg.origin[k];
+    geo.cell = c->cell;
+    geo.rmax = c->rmax;
     GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_spos,
-                 spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
+                 spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], geo, c->d_count,
                  c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob));
     c->launches += 1;
     GB_CK(cudaGetLastError());
@@ -1288,6 +1294,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
     if(coeff < 1.0)
         coeff = 1.0;
     c->cell = coeff * 2.0 * rmax;
+    c->rmax = rmax;
     for(int k = 0; k < 3; ++k)
     {
         c->lc_max[k] = c->cfg.max_coordinate[k] + (c->cfg.pad_grid ? c->cell : 0.0);

@@ -378,15 +378,35 @@ GB_D void for_each_candidate(int s, const uint32_t* __restrict__ skeys,
 // order.  The enumeration order of a particle's candidates is ascending
 // sorted position (rows ascend in (z, y), cells in x, ids within a cell), so
 // the fill pass restores it by sorting the slots.  Obstacle candidates are
-// added to count[id] by the particle itself.  Latency-bound on L1 hits: the
-// mixed instantiation runs at full occupancy (32 registers), which measured
-// 5% faster than 40 registers at six blocks per SM.
+// added to count[id] by the particle itself.
+//
+// Reach: a particle b hashed to a neighbour cell lies beyond the cell faces
+// that separate that cell from a's (a centre clamped into the grid lies
+// further out still), so |a - b| is at least the distance from a to those
+// faces, and a candidate needs |a - b| < rA + rB <= rA + rmax.  The rows and
+// the end cells of a row that are farther than that, with a margin far above
+// the rounding of the hash and of the faces, hold no pair that the exact test
+// accepts and are not walked; the pair set is unchanged.  The FP64 modes
+// prune so (their exact test on every candidate is the costly part); the
+// mixed mode does not, since its FP32 pre-test is cheap and a warp walks the
+// longest range among its lanes anyway: pruning measured slower there.
+//
+// Latency-bound on L1 hits: the mixed instantiation runs at full occupancy
+// (32 registers), which measured 5% faster than 40 registers at six blocks
+// per SM.
+struct CellGeometry
+{
+    double mn[3]; // grid origin
+    double cell;  // cell edge
+    double rmax;  // largest bounding radius of any particle
+};
+
 template <typename S>
 __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
     k_pair_count(int n, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
-                 uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
+                 CellGeometry geo, uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
                  uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs)
 {
     grid_dep_sync();
@@ -413,12 +433,39 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
             slot[(size_t)u * kPairSlots + k] = v;
         atomicAdd(count + sids[u], 1u);
     };
+    // distances from a to the faces of its cell (0 if a lies outside it)
+    constexpr bool PRUNE = !PRE32;
+    double         r2 = 0.0, gxm = 0.0, gxp = 0.0, gym = 0.0, gyp = 0.0, gzp = 0.0;
+    if constexpr(PRUNE)
+    {
+        const double reach = (pa.w + geo.rmax) * (1.0 + 1e-6) + 1e-6 * geo.cell;
+        r2                 = reach * reach;
+        gxm = fmax(pa.x - (geo.mn[0] + cx * geo.cell), 0.0);
+        gxp = fmax(geo.mn[0] + (cx + 1) * geo.cell - pa.x, 0.0);
+        gym = fmax(pa.y - (geo.mn[1] + cy * geo.cell), 0.0);
+        gyp = fmax(geo.mn[1] + (cy + 1) * geo.cell - pa.y, 0.0);
+        gzp = fmax(geo.mn[2] + (cz + 1) * geo.cell - pa.z, 0.0);
+    }
     for(int r = 4; r < 9; ++r)
     {
-        uint32_t t0, t1;
-        neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
-        if(r == 4)
-            t0 = (uint32_t)s + 1;
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        const int z = cz + dz, y = cy + dy;
+        if(z >= (int)nz || y < 0 || y >= (int)ny)
+            continue;
+        bool left = cx > 0, right = cx + 1 < (int)nx;
+        if constexpr(PRUNE)
+        {
+            const double gy = dy < 0 ? gym : (dy > 0 ? gyp : 0.0);
+            const double gz = dz > 0 ? gzp : 0.0;
+            const double d2 = gy * gy + gz * gz;
+            if(d2 > r2)
+                continue;
+            left  = left && !(d2 + gxm * gxm > r2);
+            right = right && !(d2 + gxp * gxp > r2);
+        }
+        const uint32_t row = ((uint32_t)z * ny + (uint32_t)y) * nx;
+        const uint32_t t0 = r == 4 ? (uint32_t)s + 1 : cstart[row + (uint32_t)(left ? cx - 1 : cx)];
+        const uint32_t t1 = cstart[row + (uint32_t)(right ? cx + 2 : cx + 1)];
 #pragma unroll 2
         for(uint32_t t = t0; t < t1; ++t)
         {
