@@ -26,6 +26,7 @@ GB_MAX_POLY_VERTICES = 64
 GB_FP64, GB_MIXED, GB_FP64_STRICT = 0, 1, 2
 GB_FLAG_RECORD_CONTACT_INFO = 1
 GB_FLAG_PHASE_TIMING = 2
+GB_RAW_COORDINATION_NUMBER = 1
 PHASES = ["hash", "sort", "cell_start", "pair_count", "pair_fill", "narrow", "particle"]
 GB_N_PHASES = len(PHASES)
 GB_LAW_HOOKE, GB_LAW_HOOKE_HISTORY = 0, 1
@@ -151,6 +152,9 @@ ENGINE_API = {
     "synchronize": (C.c_int, [_P]),
     "set_stream": (C.c_int, [_P, _P]),
     "get_phase_times": (C.c_int, [_P, _D, _I64, C.c_int32]),
+    "rawdata_open": (C.c_int, [_P, C.c_char_p, C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "rawdata_write": (C.c_int, [C.c_void_p, C.c_double]),
+    "rawdata_close": (C.c_int, [C.c_void_p]),
     "save_state": (C.c_int, [_P, C.c_void_p]),
     "load_state": (C.c_int, [_P, C.c_void_p]),
 }

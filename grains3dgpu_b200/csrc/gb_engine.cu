@@ -12,6 +12,7 @@
 #include "gb_io.cuh"
 #include "gb_adjoint.cuh"
 #include "gb_step.cuh"
+#include "gb_rawdata.cuh"
 
 using namespace gb;
 
@@ -1860,6 +1861,205 @@ int gb_device_pointer(gb_ctx* c, const char* name, void** ptr)
     if(s == "rotation")
         return *ptr = c->d_rot, GB_OK;
     return GB_E_INVALID_ARG;
+}
+
+} // extern "C"
+
+// ---- RawData writer (gb_rawdata.cuh) ----------------------------------------------
+struct gb_rawdata_writer
+{
+    gb_ctx*      c = nullptr;
+    std::string  base;   // directory/root_name
+    int          flags = 0;
+    FILE*        f[10]  = {}; // position x,y,z; translational x,y,z; angular x,y,z; coordination
+    double*      d_snap = nullptr;
+    uint32_t*    d_cn   = nullptr;
+    double*      h_snap = nullptr; // pinned
+    uint32_t*    h_cn   = nullptr; // pinned
+    cudaStream_t copy   = nullptr;
+    cudaEvent_t  ev_snap = nullptr, ev_copied = nullptr;
+    std::thread  worker;
+    int          status = GB_OK; // the last save's write status
+};
+
+namespace
+{
+const char* const kRawFiles[10] = {"_position_x",
+                                   "_position_y",
+                                   "_position_z",
+                                   "_translational_velocity_x",
+                                   "_translational_velocity_y",
+                                   "_translational_velocity_z",
+                                   "_angular_velocity_x",
+                                   "_angular_velocity_y",
+                                   "_angular_velocity_z",
+                                   "_coordinationNumber"};
+
+// one save's lines, formatted from the pinned snapshot: component files in
+// parallel threads, then the coordination number and particleType files
+int raw_write_lines(gb_rawdata_writer* w, int n, double time)
+{
+    cudaSetDevice(w->c->cfg.device);
+    if(cudaEventSynchronize(w->ev_copied) != cudaSuccess)
+        return GB_E_CUDA;
+    const int    nob = w->c->nob;
+    const double* otr = w->c->obs_tr.data();
+    char         tbuf[64];
+    raw_real(tbuf, sizeof tbuf, time);
+    int  bad[9] = {0};
+    auto line   = [&](int k) {
+        std::string out(tbuf);
+        out.reserve((size_t)(n + nob) * 14 + 64);
+        char         b[64];
+        const double* v = w->h_snap + (size_t)k * n;
+        for(int i = 0; i < n; ++i)
+        {
+            out.push_back(' ');
+            out.append(b, (size_t)raw_real(b, sizeof b, v[i]));
+        }
+        for(int o = 0; o < nob; ++o)
+        {
+            // obstacles: the origin of their transform, zero velocities
+            out.push_back(' ');
+            out.append(b, (size_t)raw_real(b, sizeof b, k < 3 ? otr[12 * o + 9 + k] : 0.0));
+        }
+        out.push_back('\n');
+        bad[k] = std::fwrite(out.data(), 1, out.size(), w->f[k]) != out.size()
+                 || std::fflush(w->f[k]) != 0;
+    };
+    std::vector<std::thread> th;
+    for(int k = 1; k < 9; ++k)
+        th.emplace_back(line, k);
+    line(0);
+    for(auto& t : th)
+        t.join();
+    std::string cn;
+    if(w->flags & GB_RAW_COORDINATION_NUMBER)
+    {
+        cn = tbuf;
+        for(int i = 0; i < n; ++i)
+            cn += " " + std::to_string(w->h_cn[i]);
+    }
+    cn.push_back('\n');
+    int err = std::fwrite(cn.data(), 1, cn.size(), w->f[9]) != cn.size() || std::fflush(w->f[9]);
+    // particleType.dat: rewritten at each save with one empty line
+    FILE* pt = std::fopen((w->base + "_particleType.dat").c_str(), "w");
+    err |= !pt || std::fputc('\n', pt) == EOF;
+    if(pt)
+        err |= std::fclose(pt) != 0;
+    for(int k = 0; k < 9; ++k)
+        err |= bad[k];
+    return err ? GB_E_INVALID_ARG : GB_OK;
+}
+
+int raw_join(gb_rawdata_writer* w)
+{
+    if(w->worker.joinable())
+        w->worker.join();
+    return w->status;
+}
+} // namespace
+
+extern "C" {
+
+int gb_rawdata_open(gb_ctx* c, const char* directory, const char* root_name, int32_t flags,
+                    gb_rawdata_writer** out)
+{
+    if(!c || !directory || !root_name || !out || (flags & ~GB_RAW_COORDINATION_NUMBER))
+        return GB_E_INVALID_ARG;
+    *out                 = nullptr;
+    gb_rawdata_writer* w = new gb_rawdata_writer;
+    w->c                 = c;
+    w->flags             = flags;
+    w->base              = std::string(directory) + "/" + root_name;
+    auto fail            = [&](int st) {
+        gb_rawdata_close(w);
+        return st;
+    };
+    // PostProcessing_start: the files are created empty (ios::out)
+    for(int k = 0; k < 10; ++k)
+        if(!(w->f[k] = std::fopen((w->base + kRawFiles[k] + ".dat").c_str(), "w")))
+            return fail(GB_E_INVALID_ARG);
+    const size_t n = (size_t)std::max(c->n, 1);
+    if(dalloc(&w->d_snap, 9 * n) || dalloc(&w->d_cn, n))
+        return fail(GB_E_OUT_OF_MEMORY);
+    if(cudaMallocHost(&w->h_snap, 9 * n * sizeof(double)) != cudaSuccess
+       || cudaMallocHost(&w->h_cn, n * sizeof(uint32_t)) != cudaSuccess)
+        return fail(GB_E_OUT_OF_MEMORY);
+    if(cudaStreamCreateWithFlags(&w->copy, cudaStreamNonBlocking) != cudaSuccess
+       || cudaEventCreateWithFlags(&w->ev_snap, cudaEventDisableTiming) != cudaSuccess
+       || cudaEventCreateWithFlags(&w->ev_copied, cudaEventDisableTiming) != cudaSuccess)
+        return fail(GB_E_CUDA);
+    *out = w;
+    return GB_OK;
+}
+
+int gb_rawdata_write(gb_rawdata_writer* w, double time)
+{
+    if(!w)
+        return GB_E_INVALID_ARG;
+    gb_ctx* c = w->c;
+    GB_TRY(ready(c));
+    GB_TRY(raw_join(w)); // the previous save has left the pinned buffers
+    const int n = c->n;
+    if(n > 0)
+    {
+        const uint32_t* off = c->detect_valid ? c->d_off[c->cur] : nullptr;
+        uint32_t*       cn  = (w->flags & GB_RAW_COORDINATION_NUMBER) ? w->d_cn : nullptr;
+        if(c->prec == GB_MIXED)
+            k_raw_snapshot<float><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+                n, c->d_pos, (const float*)c->d_vel, (const float*)c->d_omg, off, c->d_pc,
+                w->d_snap, cn);
+        else
+            k_raw_snapshot<double><<<blocks(n, kBlock), kBlock, 0, c->stream>>>(
+                n, c->d_pos, (const double*)c->d_vel, (const double*)c->d_omg, off, c->d_pc,
+                w->d_snap, cn);
+        c->launches += 1;
+        GB_CK(cudaGetLastError());
+    }
+    GB_CK(cudaEventRecord(w->ev_snap, c->stream));
+    GB_CK(cudaStreamWaitEvent(w->copy, w->ev_snap, 0));
+    if(n > 0)
+    {
+        GB_CK(cudaMemcpyAsync(w->h_snap, w->d_snap, 9 * (size_t)n * sizeof(double),
+                              cudaMemcpyDeviceToHost, w->copy));
+        if(w->flags & GB_RAW_COORDINATION_NUMBER)
+            GB_CK(cudaMemcpyAsync(w->h_cn, w->d_cn, (size_t)n * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToHost, w->copy));
+    }
+    GB_CK(cudaEventRecord(w->ev_copied, w->copy));
+    w->worker = std::thread([w, n, time] { w->status = raw_write_lines(w, n, time); });
+    return GB_OK;
+}
+
+int gb_rawdata_close(gb_rawdata_writer* w)
+{
+    if(!w)
+        return GB_E_INVALID_ARG;
+    int st = raw_join(w);
+    for(FILE*& f : w->f)
+        if(f)
+        {
+            if(std::fclose(f) != 0 && st == GB_OK)
+                st = GB_E_INVALID_ARG;
+            f = nullptr;
+        }
+    if(w->copy)
+        cudaStreamSynchronize(w->copy);
+    dfree(w->d_snap);
+    dfree(w->d_cn);
+    if(w->h_snap)
+        cudaFreeHost(w->h_snap);
+    if(w->h_cn)
+        cudaFreeHost(w->h_cn);
+    if(w->ev_snap)
+        cudaEventDestroy(w->ev_snap);
+    if(w->ev_copied)
+        cudaEventDestroy(w->ev_copied);
+    if(w->copy)
+        cudaStreamDestroy(w->copy);
+    delete w;
+    return st;
 }
 
 } // extern "C"

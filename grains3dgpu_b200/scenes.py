@@ -11,6 +11,8 @@ fixed order: shapes, centres, jitter, orientations, velocities.
 """
 import dataclasses
 
+import os
+
 import numpy as np
 
 from . import abi
@@ -456,6 +458,10 @@ class System:
             out = out.reshape(-1, 7)
         return out
 
+    def rawdata(self, directory, root_name, coordination=False):
+        """A RawData post-processing writer on this system (gb_rawdata_open)."""
+        return RawDataWriter(self, directory, root_name, coordination)
+
     def close(self):
         if self.ctx:
             self.lib.destroy(self.ctx)
@@ -466,3 +472,26 @@ class System:
             self.close()
         except Exception:
             pass
+
+
+class RawDataWriter:
+    """RawDataPostProcessingWriter's start / PostProcessing / end as
+    open / write(time) / close (gb_rawdata_open, gb_rawdata_write,
+    gb_rawdata_close)."""
+
+    def __init__(self, system, directory, root_name, coordination=False):
+        self.system = system
+        h = abi.C.c_void_p()
+        flags = abi.GB_RAW_COORDINATION_NUMBER if coordination else 0
+        system._check(system.lib.rawdata_open(system.ctx, os.fsencode(directory),
+                                              os.fsencode(root_name), flags, abi.C.byref(h)),
+                      "rawdata_open")
+        self.h = h
+
+    def write(self, time):
+        return self.system._check(self.system.lib.rawdata_write(self.h, time), "rawdata_write")
+
+    def close(self):
+        if self.h:
+            h, self.h = self.h, None
+            return self.system._check(self.system.lib.rawdata_close(h), "rawdata_close")

@@ -285,6 +285,27 @@ int gb_linked_cell_sort_static(const double* pos, int32_t n, const double origin
                                double cell_size, const int32_t dims[3], uint32_t* sorted_ids,
                                uint32_t* cell_start, void* stream);
 
+/* ---- RawData post-processing output ------------------------------------------------
+ * RawDataPostProcessingWriter (PostProcessing/src/RawDataPostProcessingWriter.cpp:
+ * PostProcessing_start :63-71, PostProcessing :75-212, PostProcessing_end :218-231),
+ * called where Grains drives its writers (Grains.cpp:52, :66, :82).  Files
+ * <directory>/<root_name>_{position,translational_velocity,angular_velocity}_{x,y,z}.dat
+ * get one line per save: the time, every particle's value, then every obstacle's
+ * (origin; zero velocities), each printed as realToString(ios::scientific, 6, v)
+ * ("%.6e"; a zero as "0").  _coordinationNumber.dat gets an empty line per save, as
+ * the reference writes it, or with GB_RAW_COORDINATION_NUMBER the time and each
+ * particle's particle-contact count of the last detect.  _particleType.dat holds one
+ * empty line.  gb_rawdata_write snapshots the state on the context's stream after
+ * the work launched before it and returns; the files are written by a host thread
+ * while later steps run, and the next write or the close waits for it (and returns
+ * its status). */
+#define GB_RAW_COORDINATION_NUMBER 1
+typedef struct gb_rawdata_writer gb_rawdata_writer;
+int gb_rawdata_open(gb_ctx* ctx, const char* directory, const char* root_name, int32_t flags,
+                    gb_rawdata_writer** out);
+int gb_rawdata_write(gb_rawdata_writer* writer, double time);
+int gb_rawdata_close(gb_rawdata_writer* writer);
+
 /* ---- host set-up helpers (no context needed) ------------------------------------- */
 /* Volume, mass, circumscribed radius, bounding box and inertia of a rigid
  * body as RigidBody::RigidBody computes them; polyhedra use their convex
