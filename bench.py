@@ -570,14 +570,15 @@ def main():
 # (profiles/k_pair_count_k_narrow_gjk_k_particles_superquadrics_1M.md); their
 # traffic scales with the particle count.  The narrow phase's scales with the
 # pairs that reach GJK and is not extrapolated.
-TRAFFIC_PER_PARTICLE = {"integration": (132.09e6 + 28.99e6) / 1_000_000,
-                        "pair_count": (62.03e6 + 1.48e6) / 1_000_000}
+TRAFFIC_PER_PARTICLE = {"integration": (132.12e6 + 24.71e6) / 1_000_000,
+                        "pair_count": (62.00e6 + 1.13e6) / 1_000_000}
 
 
 # what bounds each stage, from the ncu capture named above
-LIMITER = {"pair_count": "issue slots: 71% active, 26 of 32 lanes per instruction; "
+LIMITER = {"pair_count": "issue slots: 67% active, 26 of 32 lanes per instruction; "
                          "~48 L1-resident neighbour tests per particle",
-           "integration": "memory latency: 55% warps active, 34% of DRAM peak",
+           "integration": "memory latency and issue: 44% warps active, 52% issue slots, "
+                          "38% of DRAM peak",
            "broad_phase": "launch and tail latency of short kernels"}
 
 
