@@ -509,7 +509,13 @@ def main():
     s64.close()
     t64 = max_over_ranks(el64, torch, world, "cuda")
     value64 = aggregate(world, scene.n, args.fp64_steps, t64)
-    ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch) if rank == 0 else None
+    ferr = None
+    if rank == 0:
+        # from one identical state: a block of the workload (a loose packing,
+        # few contacts) and the same grains packed densely (2.2 mm lattice)
+        ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch)
+        ferr["dense"] = force_error(scenes.polydisperse_superquadrics(
+            seed=5, n=min(scene.n, 200_000), pitch=2.2e-3), torch)
 
     shapes = None
     if world == 1 and not args.no_shapes:
