@@ -292,23 +292,36 @@ def measure_shapes(args, torch):
 
 
 def force_error(scene, torch):
-    """Single-step force error of the mixed mode against the FP64 mode from
-    one identical state: max |F_mixed - F_fp64| over particles divided by
-    max |F_fp64|, and the same for torques."""
+    """Single-step force error of the mixed mode against the FP64 mode: max
+    |F_mixed - F_fp64| over particles divided by max |F_fp64|, and the same
+    for torques.  `*_rel_err` gives both modes the scene's FP64 pose; the
+    mixed state rounds its orientation to an FP32 quaternion on the way in, so
+    `identical_state` also runs the FP64 mode from the mixed mode's (rounded)
+    pose: one identical state for both."""
     from grains3dgpu_b200 import engine
     lib = engine.load()
-    out = {}
-    for prec in (abi.GB_MIXED, abi.GB_FP64):
+
+    def run(prec, tr=None):
         s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device(),
                           contact_law=LAW)
+        if tr is not None:
+            s.set_transforms(tr)
         s.detect()
-        out[prec] = (s.torces(), s.stats().contacts)
+        out = (s.torces(), s.stats().contacts, s.transforms().copy())
         s.close()
-    a, b = out[abi.GB_MIXED][0], out[abi.GB_FP64][0]
-    ef = np.abs(a[:, :3] - b[:, :3]).max() / max(np.abs(b[:, :3]).max(), 1e-300)
-    et = np.abs(a[:, 3:] - b[:, 3:]).max() / max(np.abs(b[:, 3:]).max(), 1e-300)
-    return {"force_rel_err": float(ef), "torque_rel_err": float(et),
-            "contacts": int(out[abi.GB_FP64][1])}
+        return out
+
+    def err(a, b):
+        return (float(np.abs(a[:, :3] - b[:, :3]).max() / max(np.abs(b[:, :3]).max(), 1e-300)),
+                float(np.abs(a[:, 3:] - b[:, 3:]).max() / max(np.abs(b[:, 3:]).max(), 1e-300)))
+
+    mixed, fp64 = run(abi.GB_MIXED), run(abi.GB_FP64)
+    same = run(abi.GB_FP64, mixed[2])
+    ef, et = err(mixed[0], fp64[0])
+    sf, st = err(mixed[0], same[0])
+    return {"force_rel_err": ef, "torque_rel_err": et, "contacts": int(fp64[1]),
+            "identical_state": {"force_rel_err": sf, "torque_rel_err": st,
+                                "contacts": int(same[1])}}
 
 
 # ---------------------------------------------------------------------------
