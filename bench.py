@@ -2,18 +2,22 @@
 
 Workload: the mixed-precision configuration -- 1,000,000 polydisperse
 superquadrics (equivalent radius lognormal, median 1 mm, sigma 0.25, clipped
-to 0.5-2 mm; b/a, c/a ~ U(0.5, 2); n1, n2 ~ U(2, 10)) on a jittered lattice in a
-closed 0.3 x 0.3 x 1.2 m box, dt = 1e-6 s, linear spring-dashpot kn=1e4 N/m,
-en=0.7, tangential stiffness 0.8 kn with per-pair tangential history, Coulomb
-mu=0.5, gravity -z.  One step = one GrainsCPU::simulate loop iteration
-(collide + force, gravity, move) over all particles.
+to 0.5-2 mm; b/a, c/a ~ U(0.5, 2); n1, n2 ~ U(2, 10)) as a bed in a closed
+0.3 x 0.3 x 1.2 m box: a 2.2 mm jittered lattice from the floor up, ~0.12 m
+deep, ~6 bounding-sphere candidates per grain.  dt = 1e-6 s, linear
+spring-dashpot kn=1e4 N/m, en=0.7, tangential stiffness 0.8 kn with per-pair
+tangential history, Coulomb mu=0.5, gravity -z.  One step = one
+GrainsCPU::simulate loop iteration (collide + force, gravity, move) over all
+particles.  The same grains spread over the whole box (a ~4.7 mm lattice,
+~0.01 candidates per grain) are reported as the secondary `dilute` line.
 
 The engine arm runs the tangential-history law (GB_LAW_HOOKE_HISTORY), the
 workload's law.  The reference has only its Hooke law, whose relative
 velocity takes the absolute contact point as lever arm: in this 1.2 m tall box
 a spinning grain's damping force grows with its height, and the packing blows
 up within ~100 steps.  The reference CPU path (cpu_baseline, --impl reference)
-is timed with that Hooke law, a little less work per contact.
+is timed with that Hooke law on blocks of the same bed, a little less work per
+contact.
 
   python bench.py [--gpus N --steps K --warmup W]          the engine (mixed)
   python bench.py --impl reference [...]                   the reference CPU path
@@ -119,7 +123,12 @@ def replica_seed(rank):
     return 2 + 1000 * rank
 
 
-def make_scene(args, rank):
+BED_PITCH = 2.2e-3  # lattice pitch of the bed
+
+
+def make_scene(args, rank, workload="bed"):
+    if workload == "bed":
+        return scenes.polydisperse_bed(seed=replica_seed(rank), n=args.n, pitch=BED_PITCH)
     return scenes.polydisperse_superquadrics(seed=replica_seed(rank), n=args.n)
 
 
@@ -292,36 +301,27 @@ def measure_shapes(args, torch):
 
 
 def force_error(scene, torch):
-    """Single-step force error of the mixed mode against the FP64 mode: max
-    |F_mixed - F_fp64| over particles divided by max |F_fp64|, and the same
-    for torques.  `*_rel_err` gives both modes the scene's FP64 pose; the
-    mixed state rounds its orientation to an FP32 quaternion on the way in, so
-    `identical_state` also runs the FP64 mode from the mixed mode's (rounded)
-    pose: one identical state for both."""
-    from grains3dgpu_b200 import engine
+    """Single-step error of the mixed mode against the FP64 mode, both given
+    the scene's FP64 pose: per contact (metrics.contact_force_errors: the
+    force and torque each contact pair puts on its first particle, |x_mixed -
+    x_fp64| / |x_fp64|), and per particle (max |F_mixed - F_fp64| over
+    particles divided by max |F_fp64|)."""
+    from grains3dgpu_b200 import engine, metrics
     lib = engine.load()
-
-    def run(prec, tr=None):
-        s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device(),
-                          contact_law=LAW)
-        if tr is not None:
-            s.set_transforms(tr)
-        s.detect()
-        out = (s.torces(), s.stats().contacts, s.transforms().copy())
-        s.close()
-        return out
-
-    def err(a, b):
-        return (float(np.abs(a[:, :3] - b[:, :3]).max() / max(np.abs(b[:, :3]).max(), 1e-300)),
-                float(np.abs(a[:, 3:] - b[:, 3:]).max() / max(np.abs(b[:, 3:]).max(), 1e-300)))
-
-    mixed, fp64 = run(abi.GB_MIXED), run(abi.GB_FP64)
-    same = run(abi.GB_FP64, mixed[2])
-    ef, et = err(mixed[0], fp64[0])
-    sf, st = err(mixed[0], same[0])
-    return {"force_rel_err": ef, "torque_rel_err": et, "contacts": int(fp64[1]),
-            "identical_state": {"force_rel_err": sf, "torque_rel_err": st,
-                                "contacts": int(same[1])}}
+    dev = torch.cuda.current_device()
+    m = scenes.System(lib, scene, precision=abi.GB_MIXED, device=dev, contact_law=LAW)
+    f = scenes.System(lib, scene, precision=abi.GB_FP64, device=dev, contact_law=LAW)
+    m.detect()
+    f.detect()
+    per_contact = metrics.contact_force_errors(m, f)
+    a, b = m.torces(), f.torces()
+    m.close()
+    f.close()
+    return {"per_contact": per_contact,
+            "per_particle_force": float(np.abs(a[:, :3] - b[:, :3]).max()
+                                        / max(np.abs(b[:, :3]).max(), 1e-300)),
+            "per_particle_torque": float(np.abs(a[:, 3:] - b[:, 3:]).max()
+                                         / max(np.abs(b[:, 3:]).max(), 1e-300))}
 
 
 # ---------------------------------------------------------------------------
@@ -403,7 +403,7 @@ def reference_arm(args):
         nthreads = len(os.sched_getaffinity(0))
     except Exception:
         nthreads = os.cpu_count() or 1
-    scene = scenes.polydisperse_superquadrics(seed=2, n=args.n)
+    scene = make_scene(args, 0)
     cell = full_cell_size(scene)
     blocks = [b for b in sample_blocks(scene, args.ref_sample, nthreads) if b.size]
     nthreads = len(blocks)
@@ -428,7 +428,9 @@ def reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": "sample of 1,000,000 polydisperse superquadrics in a 0.3x0.3x1.2 m box",
+        "config": {"workload": f"sample of {args.n:,} polydisperse superquadrics as a bed "
+                               f"(a {BED_PITCH*1e3:.1f} mm jittered lattice from the floor of a "
+                               "0.3x0.3x1.2 m box)",
                    "sample_particles_per_thread": m, "threads": nthreads},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": nthreads, "kind": kind,
                          "sample": f"{nthreads} threads, each stepping its own lattice block of "
@@ -459,6 +461,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--shape-steps", type=int, default=10)
     ap.add_argument("--no-shapes", action="store_true")
+    ap.add_argument("--no-dilute", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -524,11 +527,27 @@ def main():
     value64 = aggregate(world, scene.n, args.fp64_steps, t64)
     ferr = None
     if rank == 0:
-        # from one identical state: a block of the workload (a loose packing,
-        # few contacts) and the same grains packed densely (2.2 mm lattice)
-        ferr = force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch)
-        ferr["dense"] = force_error(scenes.polydisperse_superquadrics(
-            seed=5, n=min(scene.n, 200_000), pitch=2.2e-3), torch)
+        # both modes from the same FP64 pose: the bottom 200,000 grains of the
+        # bed, and 200,000 grains of the spread-out lattice
+        ferr = {"bed_200k": force_error(scene.subset(np.arange(min(scene.n, 200_000))), torch),
+                "dilute_200k": force_error(make_scene(args, rank, "dilute").subset(
+                    np.arange(min(scene.n, 200_000))), torch)}
+
+    dilute = None
+    if world == 1 and not args.no_dilute:
+        dscene = make_scene(args, rank, "dilute")
+        dres = {}
+        for prec, key, k in ((abi.GB_MIXED, "mixed", args.steps),
+                             (abi.GB_FP64, "fp64", args.fp64_steps)):
+            ds, del_, _, _, _, dst = run_engine(args, dscene, prec, k, args.warmup, torch, 0, 1,
+                                                timing=False)
+            ds.close()
+            dres[key] = {"value": dscene.n * k / del_, "ms_per_step": del_ / k * 1e3}
+        dres["mixed_over_fp64"] = dres["mixed"]["value"] / dres["fp64"]["value"]
+        dres["workload"] = (f"the same {dscene.n:,} grains spread over the whole box "
+                            f"({dscene.notes})")
+        dres["candidate_pairs_last_step"] = int(dst.candidate_pairs)
+        dilute = dres
 
     shapes = None
     if world == 1 and not args.no_shapes:
@@ -549,12 +568,17 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (f64 positions, f64 GJK)",
             "data": "synthetic (seeded jittered-lattice packing)",
-            "config": {"workload": f"{scene.n:,} polydisperse superquadrics in a "
-                                   "0.3x0.3x1.2 m box, dt=1e-6 s, mixed precision",
+            "config": {"workload": f"{scene.n:,} polydisperse superquadrics as a bed (a "
+                                   f"{BED_PITCH*1e3:.1f} mm jittered lattice from the floor of "
+                                   "a 0.3x0.3x1.2 m box), dt=1e-6 s, mixed precision",
                        "n_particles": scene.n, "precision": "mixed",
                        "contact_law": "linear spring-dashpot, kt = 0.8 kn, Coulomb mu = 0.5, "
                                       "per-pair tangential history",
+                       "gjk": "GJK with Johnson's sub-algorithm (the reference's)",
                        "n_cells": st.n_cells, "candidate_pairs_last_step": st.candidate_pairs,
+                       "candidate_pairs_per_particle": st.candidate_pairs / scene.n,
+                       "gjk_pairs_last_step": st.gjk_calls,
+                       "contacts_last_step": st.contacts,
                        "l2": "per-step working set > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline,
@@ -572,6 +596,7 @@ def main():
                      "stages": stage_report(ms64 / max(n64, 1), scene.n, st.n_cells, 8, hbm)},
             "mixed_over_fp64": value / value64,
             "mixed_vs_fp64_single_step": ferr,
+            "dilute": dilute,
             "adjoint": adj,
             "other_shapes": shapes,
             "gpu_launches": int(launches),
@@ -586,7 +611,7 @@ def main():
 
 # DRAM bytes (read + write) per particle of the dominant kernels, from one
 # ncu capture of this workload with 1,000,000 particles
-# (profiles/k_pair_count_k_narrow_gjk_k_particles_superquadrics_1M.md); their
+# (the summary of that capture is committed beside the other profiles); their
 # traffic scales with the particle count.  The narrow phase's scales with the
 # pairs that reach GJK and is not extrapolated.
 TRAFFIC_PER_PARTICLE = {"integration": (132.12e6 + 24.71e6) / 1_000_000,

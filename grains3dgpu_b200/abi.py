@@ -40,6 +40,7 @@ GB_DUMP_CANDIDATE_PAIRS = 3
 GB_DUMP_CONTACT_PAIRS = 4
 GB_DUMP_CONTACT_INFO = 5
 GB_DUMP_NEIGHBORS = 6
+GB_DUMP_CONTACT_FORCES = 7
 
 
 class Convex(C.Structure):

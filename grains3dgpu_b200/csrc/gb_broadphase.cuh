@@ -546,6 +546,9 @@ __global__ void __launch_bounds__(kBlock)
 //      it locates its key range with two binary searches, stages those sorted
 //      keys in shared memory, and answers each cell from there.
 constexpr int kCellsPerBlock = 1024;
+// Largest cell count of a grid: cell keys and k_cell_start's cell indices
+// (up to ncells + kCellsPerBlock) stay below 2^32.
+constexpr uint64_t kMaxCells = 0xFFFFFFFFull - 2 * kCellsPerBlock;
 constexpr int kStageCap      = 4096;
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t n, uint32_t key)
@@ -570,7 +573,13 @@ __global__ void __launch_bounds__(kBlock) k_cell_start(const uint32_t* __restric
     __shared__ uint32_t sk[kStageCap];
     const uint32_t      c0 = blockIdx.x * kCellsPerBlock;
     if(threadIdx.x < 2)
-        range[threadIdx.x] = lower_bound_u32(skeys, n, c0 + threadIdx.x * kCellsPerBlock);
+    {
+        // the block's key range in 64 bits: the upper bound of the last block
+        // may lie past 2^32 - 1, beyond every key (callers keep ncells below
+        // kMaxCells, so c0 + kCellsPerBlock does not wrap either)
+        const uint64_t b = (uint64_t)c0 + (uint64_t)threadIdx.x * kCellsPerBlock;
+        range[threadIdx.x] = lower_bound_u32(skeys, n, b > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)b);
+    }
     __syncthreads();
     const uint32_t lo = range[0], hi = range[1];
     const uint32_t m  = hi - lo;

@@ -135,7 +135,7 @@ struct gb_ctx
 
     // state
     double*   d_pos = nullptr; // 3n
-    void*     d_rot = nullptr; // 9n (FP64) or 4n (mixed)
+    void*     d_rot = nullptr; // 9n (FP64) or 8n (mixed: quaternion hi, lo)
     void*     d_vel = nullptr; // 3n
     void*     d_omg = nullptr;
     void*     d_frc = nullptr;
@@ -265,7 +265,7 @@ size_t store_size(int prec)
 
 int rot_count(int prec)
 {
-    return prec == GB_MIXED ? 4 : 9;
+    return prec == GB_MIXED ? 8 : 9; // mixed: quaternion hi (4) and lo (4)
 }
 
 template <typename St>
@@ -1307,7 +1307,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
         c->dims[k] = (uint32_t)t;
     }
     const uint64_t nc = (uint64_t)c->dims[0] * c->dims[1] * c->dims[2];
-    if(nc == 0 || nc >= 0xFFFFFFF0ull)
+    if(nc == 0 || nc > kMaxCells)
         return GB_E_INVALID_ARG;
     c->ncells   = (uint32_t)nc;
     c->key_bits = 0;
@@ -1698,6 +1698,13 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
     o->candidate_pairs   = c->npairs;
     o->obstacle_contacts = (int64_t)cnt[0];
     o->gjk_iterations    = (int64_t)cnt[1];
+    if(c->d_gjkn)
+    {
+        // particle pairs queued for GJK by the last detect (past the bounding tests)
+        uint32_t q = 0;
+        GB_CK(cudaMemcpy(&q, c->d_gjkn, sizeof(q), cudaMemcpyDeviceToHost));
+        o->gjk_calls = c->detect_valid ? (int64_t)q : 0;
+    }
     if(c->detect_valid && c->npairs > 0)
     {
         // particle pairs only: obstacle candidates share the list
@@ -1787,6 +1794,7 @@ int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
         case GB_DUMP_CANDIDATE_PAIRS:
         case GB_DUMP_CONTACT_PAIRS:
         case GB_DUMP_CONTACT_INFO:
+        case GB_DUMP_CONTACT_FORCES:
         {
             if(!c->detect_valid)
                 return GB_E_NOT_READY;
@@ -1807,6 +1815,21 @@ int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
                 info.resize(7 * P);
                 GB_CK(cudaMemcpy(info.data(), c->d_info, 7 * P * sizeof(double), cudaMemcpyDeviceToHost));
             }
+            // force and torque of each pair (the storage type of the mode)
+            std::vector<double> ft;
+            if(kind == GB_DUMP_CONTACT_FORCES && P)
+            {
+                const size_t        ss = store_size(c->prec);
+                std::vector<char> raw(6 * P * ss);
+                for(int k = 0; k < 6; ++k)
+                    GB_CK(cudaMemcpy(raw.data() + k * P * ss, (const char*)c->d_pf + k * c->cap * ss,
+                                     P * ss, cudaMemcpyDeviceToHost));
+                ft.resize(6 * P);
+                for(int k = 0; k < 6; ++k)
+                    for(int64_t p = 0; p < P; ++p)
+                        ft[6 * p + k] = ss == 4 ? (double)((const float*)raw.data())[k * P + p]
+                                                : ((const double*)raw.data())[k * P + p];
+            }
             int64_t w = 0;
             for(int64_t p = 0; p < P; ++p)
             {
@@ -1819,6 +1842,11 @@ int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
                     if(out && 7 * w + 7 <= capacity)
                         std::memcpy((double*)out + 7 * w, &info[7 * p], 7 * sizeof(double));
                 }
+                else if(kind == GB_DUMP_CONTACT_FORCES)
+                {
+                    if(out && 6 * w + 6 <= capacity)
+                        std::memcpy((double*)out + 6 * w, &ft[6 * p], 6 * sizeof(double));
+                }
                 else if(out && 2 * w + 2 <= capacity)
                 {
                     ((uint32_t*)out)[2 * w]     = a[p];
@@ -1826,7 +1854,7 @@ int gb_debug_dump(gb_ctx* c, int32_t kind, void* out, int64_t capacity, int64_t*
                 }
                 ++w;
             }
-            *count = kind == GB_DUMP_CONTACT_INFO ? 7 * w : 2 * w;
+            *count = kind == GB_DUMP_CONTACT_INFO ? 7 * w : kind == GB_DUMP_CONTACT_FORCES ? 6 * w : 2 * w;
             return GB_OK;
         }
         default:

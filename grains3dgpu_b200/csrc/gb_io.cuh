@@ -10,7 +10,8 @@ namespace gb
 {
 
 // 12 doubles per particle -> positions + basis (FP64 modes) or unit
-// quaternion (mixed mode, Quaternion::setQuaternion(Matrix3) then normalised)
+// quaternion (mixed mode, Quaternion::setQuaternion(Matrix3) then normalised,
+// kept as a compensated FP32 pair)
 template <typename St>
 __global__ void k_set_transforms(int n, const double* __restrict__ tr, double* __restrict__ pos,
                                  St* __restrict__ rot, int quat)
@@ -35,10 +36,16 @@ __global__ void k_set_transforms(int n, const double* __restrict__ tr, double* _
         R.m[k] = t[k];
     Quat<double> q  = quat_from_basis(R);
     const double nq = sqrt(q.w * q.w + q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z);
-    rot[i]                 = (St)(q.w / nq);
-    rot[(size_t)n + i]     = (St)(q.v.x / nq);
-    rot[2 * (size_t)n + i] = (St)(q.v.y / nq);
-    rot[3 * (size_t)n + i] = (St)(q.v.z / nq);
+    const double c[4] = {q.w / nq, q.v.x / nq, q.v.y / nq, q.v.z / nq};
+    // a compensated pair: the FP32 value in rot[0..3] and its FP32 remainder
+    // in rot[4..7], so that hi + lo carries the FP64 orientation
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+    {
+        const St hi                  = (St)c[k];
+        rot[(size_t)k * n + i]       = hi;
+        rot[(size_t)(4 + k) * n + i] = (St)(c[k] - (double)hi);
+    }
 }
 
 template <typename St>
@@ -59,9 +66,11 @@ __global__ void k_get_transforms(int n, double* __restrict__ tr, const double* _
             t[k] = (double)rot[(size_t)k * n + i];
         return;
     }
-    const M3<double> R = quat_to_matrix<double>((double)rot[i], (double)rot[(size_t)n + i],
-                                                (double)rot[2 * (size_t)n + i],
-                                                (double)rot[3 * (size_t)n + i]);
+    double q[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+        q[k] = (double)rot[(size_t)k * n + i] + (double)rot[(size_t)(4 + k) * n + i];
+    const M3<double> R = quat_to_matrix<double>(q[0], q[1], q[2], q[3]);
 #pragma unroll
     for(int k = 0; k < 9; ++k)
         t[k] = R.m[k];

@@ -12,12 +12,16 @@ namespace gb
 // every mode.  Orientation: in the FP64 modes the 3x3 basis of Grains'
 // Transform3 (9 arrays, row-major), updated exactly as
 // Transform3::composeLeftByRotation; in the mixed mode a unit quaternion
-// (w, x, y, z) in FP32.
+// (w, x, y, z) as a compensated FP32 pair: rot[0..3] hold the FP32 value,
+// read by the FP32 bounding tests, and rot[4..7] the FP32 remainder, so that
+// hi + lo (read by the FP64 contact geometry) keeps the orientation to FP64
+// accuracy (an FP32 quaternion alone rounds a pose by ~6e-8 rad, which moves
+// GJK's stopping point on resting contacts).
 template <typename St>
 struct State
 {
     double*   pos[3];
-    St*       rot[9]; // basis (FP64 modes) or quaternion in rot[0..3] (mixed)
+    St*       rot[9]; // basis (FP64 modes) or quaternion hi in rot[0..3], lo in rot[4..7] (mixed)
     St*       vel[3];
     St*       omg[3];
     St*       frc[3];
@@ -48,16 +52,26 @@ struct Tables
 // The bounding-sphere and OBB tests run in FP32 on FP32 poses (their margins
 // are absolute: LOWEPS on the OBB axes, the crust-free bounding box), and every
 // pair that survives them is solved by the FP64 GJK of the FP64 mode, with
-// FP64 shape tables and the FP32 quaternion widened: FP32 support points on
+// FP64 shape tables and the compensated quaternion: FP32 support points on
 // mm-size grains carry ~1e-10 m of rounding, the order of a resting contact's
 // overlap (m g / kn ~ 1e-8 m), so contact points and overlaps come from FP64.
 // (An FP32 GJK as a rejection stage before the FP64 solve measured slower than
 // the FP64 solve alone once its supports took the log-domain form.)
 
+GB_D Quat<double> load_quat64(const State<float>& st, uint32_t i)
+{
+    Quat<double> q;
+    q.w = (double)st.rot[0][i] + (double)st.rot[4][i];
+    q.v = mk<double>((double)st.rot[1][i] + (double)st.rot[5][i],
+                     (double)st.rot[2][i] + (double)st.rot[6][i],
+                     (double)st.rot[3][i] + (double)st.rot[7][i]);
+    return q;
+}
+
 GB_D M3<double> load_rot64(const State<float>& st, uint32_t i)
 {
-    return quat_to_matrix<double>((double)st.rot[0][i], (double)st.rot[1][i],
-                                  (double)st.rot[2][i], (double)st.rot[3][i]);
+    const Quat<double> q = load_quat64(st, i);
+    return quat_to_matrix<double>(q.w, q.v.x, q.v.y, q.v.z);
 }
 
 GB_D Contact<float> to_f(const Contact<double>& c)
@@ -991,10 +1005,11 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     // loaded before it, and every store comes after all loads, so that these
     // loads and the loop's gathers are in flight together.
     const bool move = (sp.phases & PHASE_MOVE) != 0;
-    S          I[6], I1[6];
-    Quat<S>    q;
-    M3<S>      R;
-    double     x0[3];
+    S            I[6], I1[6];
+    Quat<S>      q;
+    Quat<double> q64; // mixed: the compensated orientation
+    M3<S>        R;
+    double       x0[3];
     if(move)
     {
 #pragma unroll
@@ -1007,6 +1022,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
         {
             q.w = S(st.rot[0][i]);
             q.v = mk<S>(S(st.rot[1][i]), S(st.rot[2][i]), S(st.rot[3][i]));
+            q64 = load_quat64(st, i);
         }
         else
             R = load_rot<S>(st, i);
@@ -1086,18 +1102,24 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
         }
         if constexpr(is_mixed<S>())
         {
-            Quat<S> qn = qmul(dq, q);
-            const S nq = s_sqrt(qn.w * qn.w + norm2(qn.v));
-            qn.w /= nq;
-            qn.v.x /= nq;
-            qn.v.y /= nq;
-            qn.v.z /= nq;
-            st.rot[0][i] = qn.w;
-            st.rot[1][i] = qn.v.x;
-            st.rot[2][i] = qn.v.y;
-            st.rot[3][i] = qn.v.z;
+            // the increment from the FP32 angular velocity, composed with the
+            // compensated orientation and renormalised in FP64
+            Quat<double> dq64;
+            dq64.w          = (double)dq.w;
+            dq64.v          = cvt3<double>(dq.v);
+            Quat<double> qn = qmul(dq64, q64);
+            const double nq = sqrt(qn.w * qn.w + norm2(qn.v));
+            const double c[4] = {qn.w / nq, qn.v.x / nq, qn.v.y / nq, qn.v.z / nq};
+            float        hi[4];
+#pragma unroll
+            for(int k = 0; k < 4; ++k)
+            {
+                hi[k]            = (float)c[k];
+                st.rot[k][i]     = hi[k];
+                st.rot[4 + k][i] = (float)(c[k] - (double)hi[k]);
+            }
             if(mask_out)
-                R = quat_to_matrix<S>(qn.w, qn.v.x, qn.v.y, qn.v.z);
+                R = quat_to_matrix<S>(hi[0], hi[1], hi[2], hi[3]);
         }
         else
         {

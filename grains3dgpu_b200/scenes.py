@@ -283,6 +283,17 @@ def polydisperse_superquadrics(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=N
                  notes=f"lattice pitch {pitch*1e3:.3f} mm", lattice_counts=tuple(counts))
 
 
+def polydisperse_bed(seed=2, n=1_000_000, box=(0.3, 0.3, 1.2), pitch=2.2e-3):
+    """The grains of :func:`polydisperse_superquadrics` as a bed: a 2.2 mm
+    jittered lattice filling the box from the floor up (about 0.12 m deep for
+    1,000,000 grains), a solid fraction of ~0.5 and ~6 bounding-sphere
+    candidates per grain -- the contact density of a settled packing, where
+    the spread-out lattice has ~0.01."""
+    s = polydisperse_superquadrics(seed=seed, n=n, box=box, pitch=pitch)
+    s.name = "polydisperse_bed"
+    return s
+
+
 def _sq_axes_vec(r_eq, ba, ca, n1, n2):
     from scipy.special import gamma
     e1, e2 = 2.0 / n1, 2.0 / n2
@@ -447,7 +458,8 @@ class System:
     def dump(self, kind):
         cnt = abi.C.c_int64(0)
         self._check(self.lib.debug_dump(self.ctx, kind, None, 0, abi.C.byref(cnt)), "debug_dump")
-        dt = np.float64 if kind == abi.GB_DUMP_CONTACT_INFO else np.uint32
+        dt = (np.float64 if kind in (abi.GB_DUMP_CONTACT_INFO, abi.GB_DUMP_CONTACT_FORCES)
+              else np.uint32)
         out = np.zeros(max(1, cnt.value), dt)
         self._check(self.lib.debug_dump(self.ctx, kind, out.ctypes.data_as(abi.C.c_void_p),
                                         cnt.value, abi.C.byref(cnt)), "debug_dump")
@@ -456,6 +468,8 @@ class System:
             out = out.reshape(-1, 2)
         elif kind == abi.GB_DUMP_CONTACT_INFO:
             out = out.reshape(-1, 7)
+        elif kind == abi.GB_DUMP_CONTACT_FORCES:
+            out = out.reshape(-1, 6)
         return out
 
     def rawdata(self, directory, root_name, coordination=False):

@@ -158,7 +158,7 @@ typedef struct gb_stats {
     int64_t candidate_pairs;  /* ordered pairs passing the bounding-sphere test */
     int64_t contacts;         /* ordered particle pairs with overlap < 0         */
     int64_t obstacle_contacts;
-    int64_t gjk_calls;
+    int64_t gjk_calls;        /* particle pairs past the bounding tests (GJK) */
     int64_t gjk_iterations;
     int32_t status_flags; /* bit i set: device-side error (1 << -GB_E_x)    */
     int32_t n_cells;
@@ -177,6 +177,8 @@ typedef struct gb_stats {
 #define GB_DUMP_CONTACT_PAIRS 4   /* uint32[2K]: (A,B) pairs with overlap < 0      */
 #define GB_DUMP_CONTACT_INFO 5    /* double[7K]: contact point, vector, overlap    */
 #define GB_DUMP_NEIGHBORS 6       /* uint32[27C]: neighbour table (UINT32_MAX out) */
+#define GB_DUMP_CONTACT_FORCES 7  /* double[6K]: force, torque on A of each contact
+                                     pair, in GB_DUMP_CONTACT_PAIRS order           */
 
 typedef struct gb_ctx gb_ctx;
 
@@ -247,9 +249,11 @@ int gb_get_stats(gb_ctx* ctx, gb_stats* out);
 int gb_debug_dump(gb_ctx* ctx, int32_t kind, void* out, int64_t capacity,
                   int64_t* count);
 /* Device pointers of the SoA state for zero-copy consumers (torch, CUDA code).
- * names: "pos_x" "pos_y" "pos_z" (double), "quat_w" "quat_x" "quat_y"
- * "quat_z" "vel_x" ... "omega_z" "force_x" ... "torque_z" (double in GB_FP64,
- * float in GB_MIXED), "rb_id" (uint32). */
+ * names: "pos_x" "pos_y" "pos_z" (double), "vel_x" ... "omega_z" "force_x" ...
+ * "torque_z" (double in the FP64 modes, float in GB_MIXED), "rotation" (the
+ * FP64 modes: 9 rows of n doubles, the Transform3 basis row-major; GB_MIXED:
+ * 8 rows of n floats, the unit quaternion w x y z followed by its FP32
+ * remainder, whose sum is the orientation), "rb_id" (uint32). */
 int gb_device_pointer(gb_ctx* ctx, const char* name, void** ptr);
 /* Synchronises the context stream and returns the device-side status flags. */
 int gb_synchronize(gb_ctx* ctx);

@@ -10,7 +10,7 @@ superquadrics (CUDA's pow and the host libm's differ in the last ulp).
 import numpy as np
 import pytest
 
-from grains3dgpu_b200 import abi, engine, scenes
+from grains3dgpu_b200 import abi, engine, metrics, scenes
 
 from conftest import rel_err, share_props
 
@@ -217,7 +217,7 @@ def test_torce_accumulation(gb, oracle, precision):
         assert d.max() < 1e-12
         assert rel_err(g.velocities(), o.velocities()) < 1e-12
     else:
-        # FP32 quaternion: basis entries to ~1e-7, FP64 centres
+        # FP32 angular velocity and torques: basis entries to ~1e-7, FP64 centres
         assert d[:, 9:].max() < 1e-9 and d[:, :9].max() < 1e-6
         assert rel_err(g.velocities(), o.velocities()) < 1e-4
 
@@ -247,15 +247,33 @@ def test_rerun_is_bitwise_deterministic(gb):
 
 @pytest.mark.parametrize("kind", ["superquadric", "polyhedron", "box-on-walls"])
 def test_mixed_precision_single_step(gb, kind):
-    """Mixed mode (FP32 bulk, FP64 positions, FP64 GJK past the bounding tests)
-    against the FP64 mode from one identical state: same contact pairs, and
-    force error <= 1e-5 of the largest force."""
+    """Mixed mode (FP32 bulk, FP64 positions, compensated FP32 quaternion,
+    FP64 GJK past the bounding tests) against the FP64 mode, both given the
+    same FP64 pose: the same contact pairs, and per contact a force and a
+    torque within 1e-5 relative of the FP64 mode's."""
     scene = make_scene(kind)
     m = scenes.System(gb, scene, precision=abi.GB_MIXED)
     f = scenes.System(gb, scene, precision=abi.GB_FP64)
     m.detect()
     f.detect()
     assert np.array_equal(m.dump(abi.GB_DUMP_CONTACT_PAIRS), f.dump(abi.GB_DUMP_CONTACT_PAIRS))
-    a, b = m.torces(), f.torces()
-    assert np.abs(a[:, :3] - b[:, :3]).max() <= 1e-5 * np.abs(b[:, :3]).max()
-    assert np.abs(a[:, 3:] - b[:, 3:]).max() <= 1e-5 * np.abs(b[:, 3:]).max()
+    e = metrics.contact_force_errors(m, f)
+    assert e["matched"] == e["contacts_ref"] > 0
+    assert e["force"]["max"] <= 1e-5 and e["torque"]["max"] <= 1e-5, e
+
+
+def test_mixed_precision_single_step_dense_polydisperse(gb):
+    """The polydisperse superquadrics of the 1,000,000-grain workload,
+    200,000 of them packed on a 2.2 mm lattice (a dense bed), with the
+    workload's tangential-history law: mixed against FP64 from the same FP64
+    pose, per contact, within 1e-5 relative."""
+    scene = scenes.polydisperse_superquadrics(seed=5, n=200_000, pitch=2.2e-3)
+    law = abi.GB_LAW_HOOKE_HISTORY
+    m = scenes.System(gb, scene, precision=abi.GB_MIXED, contact_law=law)
+    f = scenes.System(gb, scene, precision=abi.GB_FP64, contact_law=law)
+    m.detect()
+    f.detect()
+    e = metrics.contact_force_errors(m, f)
+    assert e["contacts_ref"] > 1000
+    assert e["matched"] == e["contacts_ref"] == e["contacts_run"], e
+    assert e["force"]["max"] <= 1e-5 and e["torque"]["max"] <= 1e-5, e

@@ -27,15 +27,26 @@ def static_sort_fn():
     return fn
 
 
-def test_static_sort_matches_update_links(gb):
+def static_sort_scene(kind):
+    if kind == "one-tile":
+        return scenes.superquadric_column(n=1500, pitch=2.05e-3)
+    # the size limit: 128 tiles of the radix sort and, on the workload's
+    # 0.3 x 0.3 x 1.2 m grid (~2.8e5 cells, 19 key bits), three radix passes
+    return scenes.polydisperse_superquadrics(seed=7, n=MAX_PARTICLES)
+
+
+@pytest.mark.parametrize("kind", ["one-tile", "max-size"])
+def test_static_sort_matches_update_links(gb, kind):
     import torch
     fn = static_sort_fn()
-    scene = scenes.superquadric_column(n=1500, pitch=2.05e-3)
+    scene = static_sort_scene(kind)
     s = scenes.System(gb, scene, precision=abi.GB_FP64)
     assert gb.update_links(s.ctx) == abi.GB_OK
     ref_ids = s.dump(abi.GB_DUMP_SORTED_IDS)
     ref_start = s.dump(abi.GB_DUMP_CELL_START)
     st = s.stats()
+    if kind == "max-size":
+        assert s.n == MAX_PARTICLES and st.key_bits > 16
     origin = (C.c_double * 3)(*scene.config["origin"])
     dims = (C.c_int32 * 3)(*st.cells_per_dir)
     pos = C.c_void_p()
