@@ -5,6 +5,8 @@ C ABI returns.
   another from an identical state, per contact: for every particle-particle
   contact pair (A, B) found by both, |F_run - F_ref| / |F_ref| of the force
   that the pair puts on A, and the same for its torque.
+* :func:`particle_torce_errors` -- the same per particle, on the torces
+  accumulated over all of a particle's contacts (walls included).
 * :func:`kinetic_energy`, :func:`coordination_number`,
   :func:`packing_fraction` -- the long-run statistics that compare chaotic
   trajectories: translational and rotational kinetic energy, mean number of
@@ -43,6 +45,21 @@ def contact_force_errors(run, ref):
         out[name] = ({"max": float(e.max()), "p99": float(np.percentile(e, 99)),
                       "median": float(np.median(e))} if e.size else
                      {"max": 0.0, "p99": 0.0, "median": 0.0})
+    return out
+
+
+def particle_torce_errors(run, ref):
+    """Per-particle relative error of the accumulated torces (force and
+    torque) of System `run` against System `ref`, over the particles whose
+    reference force is non-zero: max of |x_run - x_ref| / |x_ref|."""
+    a, b = run.torces(), ref.torces()
+    out = {}
+    for name, sl in (("force", slice(0, 3)), ("torque", slice(3, 6))):
+        nb = np.linalg.norm(b[:, sl], axis=1)
+        sel = nb > 0
+        e = np.linalg.norm(a[sel, sl] - b[sel, sl], axis=1) / nb[sel]
+        out[name] = float(e.max()) if e.size else 0.0
+    out["particles"] = int((np.linalg.norm(b[:, :3], axis=1) > 0).sum())
     return out
 
 

@@ -257,9 +257,14 @@ def test_mixed_precision_single_step(gb, kind):
     m.detect()
     f.detect()
     assert np.array_equal(m.dump(abi.GB_DUMP_CONTACT_PAIRS), f.dump(abi.GB_DUMP_CONTACT_PAIRS))
-    e = metrics.contact_force_errors(m, f)
-    assert e["matched"] == e["contacts_ref"] > 0
-    assert e["force"]["max"] <= 1e-5 and e["torque"]["max"] <= 1e-5, e
+    if kind != "box-on-walls":  # boxes touch only the walls (the exact-box OBB test)
+        e = metrics.contact_force_errors(m, f)
+        assert e["matched"] == e["contacts_ref"] > 0
+        assert e["force"]["max"] <= 1e-5 and e["torque"]["max"] <= 1e-5, e
+    # and per particle, walls included
+    e = metrics.particle_torce_errors(m, f)
+    assert e["particles"] > 0
+    assert e["force"] <= 1e-5 and e["torque"] <= 1e-5, e
 
 
 def test_mixed_precision_single_step_dense_polydisperse(gb):
