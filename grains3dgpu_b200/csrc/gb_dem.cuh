@@ -35,26 +35,32 @@ GB_D Contact<S> no_contact()
 // working coordinates (xA, xB absolute; or 0, xB-xA relative); d = xB - xA.
 // VAR selects the GJK (GB_GJK_JH, the reference's choice, or GB_GJK_SV /
 // GB_GJK_NESTEROV).
+// closestPointsSpheres (CollisionDetection.cpp:26-48)
+template <typename S>
+GB_D Contact<S> closest_spheres(const Body<S>& A, const Body<S>& B, const V3<S>& oA,
+                                const V3<S>& oB)
+{
+    V3<S>   vba     = oB - oA;
+    const S overlap = norm(vba) - A.rcirc - B.rcirc;
+    vba             = vba / norm(vba);
+    if(overlap < S(0.0))
+    {
+        Contact<S> c;
+        c.pt      = oA + (A.rcirc + S(0.5) * overlap) * vba;
+        c.vec     = overlap * vba;
+        c.overlap = overlap;
+        return c;
+    }
+    return no_contact<S>();
+}
+
 template <int VAR = GB_GJK_JH, typename S>
 GB_D Contact<S> closest_points(const Body<S>& A, const Body<S>& B, const M3<S>& RA,
                                const M3<S>& RB, const V3<S>& oA, const V3<S>& oB,
                                const V3<S>& d, int* gjk_iters)
 {
     if(A.type == GB_SPHERE && B.type == GB_SPHERE)
-    {
-        V3<S>   vba     = oB - oA;
-        const S overlap = norm(vba) - A.rcirc - B.rcirc;
-        vba             = vba / norm(vba);
-        if(overlap < S(0.0))
-        {
-            Contact<S> c;
-            c.pt      = oA + (A.rcirc + S(0.5) * overlap) * vba;
-            c.vec     = overlap * vba;
-            c.overlap = overlap;
-            return c;
-        }
-        return no_contact<S>();
-    }
+        return closest_spheres(A, B, oA, oB);
     const S overlap = norm(d) - (A.rcirc + B.rcirc);
     if(!(overlap < S(0.0)))
         return no_contact<S>();

@@ -100,7 +100,7 @@ extern "C" int gb_linked_cell_sort_static(const double* pos, int32_t n, const do
     if(dims[0] < 1 || dims[1] < 1 || dims[2] < 1)
         return GB_E_INVALID_ARG;
     const uint64_t ncells = (uint64_t)dims[0] * dims[1] * dims[2];
-    if(ncells > kMaxCells)
+    if(ncells > gb::kMaxCells)
         return GB_E_INVALID_ARG;
     uint32_t* sc = nullptr;
     int       st = scratch_on_current_device(&sc);

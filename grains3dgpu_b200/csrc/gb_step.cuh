@@ -83,6 +83,24 @@ GB_D Contact<float> to_f(const Contact<double>& c)
     return r;
 }
 
+// closestPointsSpheres (CollisionDetection.cpp:26-48) for the mixed mode:
+// the closed form directly in FP64, the point relative to A's centre.
+GB_D Contact<float> closest_spheres_mixed(const Tables<float>& tb, uint32_t ra, uint32_t rb,
+                                          const double xa[3], const double xb[3])
+{
+    const V3<double> d64 = mk<double>(xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]);
+    const double     rA = tb.shape64[ra].rcirc, rB = tb.shape64[rb].rcirc;
+    const double     nd = norm(d64), overlap = nd - rA - rB;
+    if(!(overlap < 0.0))
+        return no_contact<float>();
+    const V3<double> u = d64 / nd;
+    Contact<double>  c;
+    c.pt      = (rA + 0.5 * overlap) * u;
+    c.vec     = overlap * u;
+    c.overlap = overlap;
+    return to_f(c);
+}
+
 // closestPointsRigidBodies for the mixed mode; points relative to A's centre.
 // VAR: the GJK variant of the FP64 solve.
 template <int VAR>
@@ -93,19 +111,7 @@ GB_D Contact<float> closest_mixed(const Tables<float>& tb, const State<float>& s
 {
     const V3<double> d64 = mk<double>(xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]);
     if(A.type == GB_SPHERE && B.type == GB_SPHERE)
-    {
-        // closed form (CollisionDetection.cpp:26-48) directly in FP64
-        const double rA = tb.shape64[ra].rcirc, rB = tb.shape64[rb].rcirc;
-        const double nd = norm(d64), overlap = nd - rA - rB;
-        if(!(overlap < 0.0))
-            return no_contact<float>();
-        const V3<double> u = d64 / nd;
-        Contact<double>  c;
-        c.pt      = (rA + 0.5 * overlap) * u;
-        c.vec     = overlap * u;
-        c.overlap = overlap;
-        return to_f(c);
-    }
+        return closest_spheres_mixed(tb, ra, rb, xa, xb);
     const V3<float> d = cvt3<float>(d64);
     if(!(norm(d) - (A.rcirc + B.rcirc) < 0.0f))
         return no_contact<float>();
@@ -749,7 +755,55 @@ GB_D bool needs_gjk(const Body<S>& A, const Body<S>& B, const M3<S>& RA, const M
     }
 }
 
-template <typename S, int VAR>
+// The first iteration of GJK-JH (gjk_jh, GJK_JH.cpp:332-371), where it
+// decides the pair on its own.  From v = sA(0) - b2a(sB(0)) and the first
+// Minkowski support w = sA(-v) - b2a(sB(R^T v)), g = v.w / |v| is a lower
+// bound on the distance of the cores, and GJK returns a distance of at
+// least g wherever it stops (|v| of a point of the Minkowski difference).
+// So:
+//   g > crustA + crustB + margin: GJK's distance exceeds the crusts: no
+//     contact;
+//   g < -margin: mu stays 0 < the absolute tolerance, GJK stops at this
+//     iteration and returns |v|; if that exceeds the crusts: no contact.
+// Every other pair (in particular every contact) takes the full GJK.  The
+// FP64 modes evaluate exactly GJK's first iteration, with a margin far
+// above FP64 rounding; the mixed mode evaluates it in FP32 (supports,
+// frames and dot products), with a margin of 1e-4 of the bounding radii,
+// some 20 times a bound on the FP32 error of g (support values are
+// Lipschitz in the direction with constant |x| <= R_circ, so the FP32
+// direction error of ~3e-7 moves them by < 1e-9 m; the FP32 supports and
+// frames add a few 1e-9 m): a pair decided here is one that the FP64 GJK
+// also finds out of contact, so the mixed mode's contact set and contact
+// geometry stay those of its FP64 GJK.
+template <typename S>
+GB_D bool gjk_first_iteration_separates(const Body<S>& A, const Body<S>& B, const M3<S>& RA,
+                                        const M3<S>& RB, const V3<S>& d)
+{
+    Tr<S>       b2a;
+    const M3<S> RAt = transpose(RA);
+    b2a.R           = mul(RAt, RB);
+    b2a.o           = mul(RAt, d);
+    const V3<S> s0A = support(A, zero3<S>()), s0B = support(B, zero3<S>());
+    const V3<S> v   = s0A - apply(b2a, s0B);
+    const S     dist = norm(v);
+    const V3<S> pa = support_first(A, -v), qb = support_first(B, mul_t(b2a.R, v));
+    const V3<S> w  = pa - apply(b2a, qb);
+    const S     g  = dot(v, w) / dist;
+    const S     ct = A.crust + B.crust;
+    const S     margin = is_mixed<S>() ? S(1e-4) * (A.rcirc + B.rcirc) + S(1e-9)
+                                       : S(1e-9) * (A.rcirc + B.rcirc) + S(1e-15);
+    if(g > ct + margin)
+        return true;
+    return g < -margin && dist - ct > margin;
+}
+
+// Pair record p: contact detection, contact law, outputs.  QUEUE (the cull
+// pass, k_narrow): the pair is finished here when it is two spheres (closed
+// form) or out of contact by the bounding tests or GJK-JH's first iteration,
+// and queued for the GJK pass otherwise -- no GJK is compiled into this
+// pass, which keeps its registers low.  Without QUEUE (k_narrow_gjk): the
+// full closestPointsRigidBodies.
+template <typename S, int VAR, bool QUEUE = false>
 GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
                       const uint32_t* __restrict__ pair_b, const State<store_t<S>>& st,
                       const Tables<S>& tb, const PairOut<store_t<S>>& po, int law_kind, int has_kr,
@@ -779,15 +833,29 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
         oB = mk<S>(S(xb[0]), S(xb[1]), S(xb[2]));
         d  = oB - oA;
     }
-    if(gjk_queue && needs_gjk<S>(A, B, RA, RB, xa, xb, d))
-    {
-        // the GJK pass (k_narrow_gjk) takes this pair and stores its outputs
-        gjk_queue[atomicAdd(gjk_count, 1u)] = (uint32_t)p;
-        return;
-    }
     int        iters = 0;
     Contact<S> ci;
-    if constexpr(is_mixed<S>())
+    if constexpr(QUEUE)
+    {
+        constexpr bool JH = (VAR & ~kGjkPaired) == GB_GJK_JH;
+        if(A.type == GB_SPHERE && B.type == GB_SPHERE)
+        {
+            if constexpr(is_mixed<S>())
+                ci = closest_spheres_mixed(tb, ra, rb, xa, xb);
+            else
+                ci = closest_spheres(A, B, oA, oB);
+        }
+        else if(!needs_gjk<S>(A, B, RA, RB, xa, xb, d)
+                || (JH && gjk_first_iteration_separates<S>(A, B, RA, RB, d)))
+            ci = no_contact<S>();
+        else
+        {
+            // the GJK pass (k_narrow_gjk) takes this pair and stores its outputs
+            gjk_queue[atomicAdd(gjk_count, 1u)] = (uint32_t)p;
+            return;
+        }
+    }
+    else if constexpr(is_mixed<S>())
         ci = closest_mixed<VAR>(tb, st, a, b, ra, rb, A, B, RA, RB, xa, xb, &iters);
     else
         ci = closest_points<VAR>(A, B, RA, RB, oA, oB, d, &iters);
@@ -888,7 +956,7 @@ __global__ void __launch_bounds__(128)
     if(step_aborted(flags))
         return;
     for_each_pair(*total, [&](int64_t p) {
-        narrow_pair<S, VAR>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters,
+        narrow_pair<S, VAR, true>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters,
                             gjk_queue, gjk_count);
     });
 }
