@@ -526,7 +526,9 @@ def main():
                               "ms_per_step": elapsed / args.steps * 1e3,
                               "gpu_launches": int(launches),
                               "candidate_pairs": int(st.candidate_pairs),
-                              "gjk_pairs": int(st.gjk_calls), "contacts": int(st.contacts)}))
+                              "gjk_pairs": int(st.gjk_calls),
+                              "gjk_fp64_pairs": int(st.gjk_fp64_calls),
+                              "contacts": int(st.contacts)}))
         if world > 1:
             torch.distributed.destroy_process_group()
         return 0
@@ -633,6 +635,7 @@ def main():
                        "n_cells": st.n_cells, "candidate_pairs_last_step": st.candidate_pairs,
                        "candidate_pairs_per_particle": st.candidate_pairs / scene.n,
                        "gjk_pairs_last_step": st.gjk_calls,
+                       "gjk_fp64_pairs_last_step": st.gjk_fp64_calls,
                        "contacts_last_step": st.contacts,
                        "l2": "per-step working set > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world}"},

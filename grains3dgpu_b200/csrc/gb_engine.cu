@@ -156,8 +156,9 @@ struct gb_ctx
     double4*  d_spos = nullptr;
     float4*   d_spos32 = nullptr; // FP32 copy for the candidate pre-test
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
-    uint32_t* d_gjkq   = nullptr; // the step's pairs that need GJK (pair capacity)
-    uint32_t* d_gjkn   = nullptr; // their number (reset by the fill pass)
+    uint32_t* d_gjkq   = nullptr; // the step's pairs that need GJK (pair capacity; the
+                                  // mixed mode: a second queue for its FP64 GJK after it)
+    uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
     uint32_t* d_obsmask_id = nullptr; // the same per particle id, from the last move
     bool      mask_valid   = false;   // d_obsmask_id matches the current poses
@@ -479,8 +480,8 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
     GB_TRY(dalloc(&c->d_counters, 4));
-    GB_TRY(dalloc(&c->d_gjkn, 1));
-    GB_CK(cudaMemset(c->d_gjkn, 0, sizeof(uint32_t)));
+    GB_TRY(dalloc(&c->d_gjkn, 2));
+    GB_CK(cudaMemset(c->d_gjkn, 0, 2 * sizeof(uint32_t)));
     if(!c->d_ticket)
     {
         GB_TRY(dalloc(&c->d_ticket, 1));
@@ -538,7 +539,7 @@ int ensure_pairs(gb_ctx* c, int64_t need)
     dfree(c->d_pc);
     dfree(c->d_info);
     dfree(c->d_gjkq);
-    GB_TRY(dalloc(&c->d_gjkq, ncap));
+    GB_TRY(dalloc(&c->d_gjkq, (c->prec == GB_MIXED ? 2 : 1) * ncap));
     GB_TRY(dalloc(&c->d_pa, ncap));
     GB_CK(cudaMalloc(&c->d_pf, 9 * ncap * ss));
     GB_TRY(dalloc(&c->d_pc, ncap));
@@ -843,8 +844,23 @@ int run_detect(gb_ctx* c, int phases)
             GB_CK(launch(c->pdl, k_narrow<S, VAR>, one_wave((const void*)k_narrow<S, VAR>), 128, s,
                          total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
                          S(c->cfg.dt), c->d_counters, c->d_gjkq, c->d_gjkn));
+            // the FP64 GJK's queue: the cull pass's, or in the mixed mode
+            // (GJK-JH) what the FP32 stage leaves of it
+            const uint32_t* q64 = c->d_gjkq;
+            const uint32_t* n64 = c->d_gjkn;
+            if constexpr(is_mixed<S>() && VAR == GB_GJK_JH)
+            {
+                GB_CK(launch(c->pdl, k_narrow_gjk32, one_wave((const void*)k_narrow_gjk32), 128, s,
+                             (const uint32_t*)c->d_gjkn, (const int*)c->d_flags,
+                             (const uint32_t*)c->d_gjkq, (const uint32_t*)c->d_pa,
+                             (const uint32_t*)c->d_pb[c->cur], st, tb, po, law, kr,
+                             c->d_gjkq + c->cap, c->d_gjkn + 1));
+                c->launches += 1;
+                q64 = c->d_gjkq + c->cap;
+                n64 = c->d_gjkn + 1;
+            }
             GB_CK(launch(c->pdl, k_narrow_gjk<S, VAR>, one_wave((const void*)k_narrow_gjk<S, VAR>),
-                         128, s, c->d_gjkn, c->d_flags, c->d_gjkq, c->d_pa, c->d_pb[c->cur], st,
+                         128, s, n64, c->d_flags, q64, c->d_pa, c->d_pb[c->cur], st,
                          tb, po, law, kr, S(c->cfg.dt), c->d_counters));
             c->launches += 2;
             if(!c->nob)
@@ -1700,10 +1716,13 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
     o->gjk_iterations    = (int64_t)cnt[1];
     if(c->d_gjkn)
     {
-        // particle pairs queued for GJK by the last detect (past the bounding tests)
-        uint32_t q = 0;
-        GB_CK(cudaMemcpy(&q, c->d_gjkn, sizeof(q), cudaMemcpyDeviceToHost));
-        o->gjk_calls = c->detect_valid ? (int64_t)q : 0;
+        // particle pairs queued for GJK by the last detect (past the bounding
+        // tests and GJK's first iteration), and those solved by the FP64 GJK
+        uint32_t q[2] = {0, 0};
+        GB_CK(cudaMemcpy(q, c->d_gjkn, sizeof(q), cudaMemcpyDeviceToHost));
+        const bool stage32 = c->prec == GB_MIXED && c->cfg.gjk_variant == GB_GJK_JH;
+        o->gjk_calls       = c->detect_valid ? (int64_t)q[0] : 0;
+        o->gjk_fp64_calls  = c->detect_valid ? (int64_t)q[stage32 ? 1 : 0] : 0;
     }
     if(c->detect_valid && c->npairs > 0)
     {

@@ -520,7 +520,12 @@ __global__ void __launch_bounds__(kBlock)
     grid_dep_sync();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if(a == 0)
-        *gjk_count = 0; // the narrow phase's GJK queue of this step starts empty
+    {
+        // the narrow phase's GJK queues of this step start empty: [0] the
+        // cull pass's, [1] the mixed mode's FP32 stage's
+        gjk_count[0] = 0;
+        gjk_count[1] = 0;
+    }
     if(a >= n || step_aborted(flags))
         return;
     const uint32_t c = count[a];
@@ -797,6 +802,176 @@ GB_D bool gjk_first_iteration_separates(const Body<S>& A, const Body<S>& B, cons
     return g < -margin && dist - ct > margin;
 }
 
+// ---- the mixed mode's FP32 GJK stage ------------------------------------------
+// Closest point to the origin of the segment (a, b) or the triangle (a, b, c)
+// (Ericson, Real-Time Collision Detection, 5.1.2 and 5.1.5, by Voronoi
+// regions), with the vertices of the feature it lies on put in y0..y(n-1).
+GB_D V3<float> closest_on_segment(const V3<float>& a, const V3<float>& b, V3<float>& y0,
+                                  V3<float>& y1, int& n)
+{
+    const V3<float> ab = b - a;
+    const float     t  = -dot(a, ab);
+    if(t <= 0.0f)
+    {
+        y0 = a;
+        n  = 1;
+        return a;
+    }
+    const float den = dot(ab, ab);
+    if(t >= den)
+    {
+        y0 = b;
+        n  = 1;
+        return b;
+    }
+    y0 = a;
+    y1 = b;
+    n  = 2;
+    return a + (t / den) * ab;
+}
+
+GB_D V3<float> closest_on_triangle(const V3<float>& a, const V3<float>& b, const V3<float>& c,
+                                   V3<float>& y0, V3<float>& y1, V3<float>& y2, int& n)
+{
+    const V3<float> ab = b - a, ac = c - a;
+    const float     d1 = -dot(ab, a), d2 = -dot(ac, a);
+    if(d1 <= 0.0f && d2 <= 0.0f)
+    {
+        y0 = a;
+        n  = 1;
+        return a;
+    }
+    const float d3 = -dot(ab, b), d4 = -dot(ac, b);
+    if(d3 >= 0.0f && d4 <= d3)
+    {
+        y0 = b;
+        n  = 1;
+        return b;
+    }
+    const float vc = d1 * d4 - d3 * d2;
+    if(vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f)
+    {
+        y0 = a;
+        y1 = b;
+        n  = 2;
+        return a + (d1 / (d1 - d3)) * ab;
+    }
+    const float d5 = -dot(ab, c), d6 = -dot(ac, c);
+    if(d6 >= 0.0f && d5 <= d6)
+    {
+        y0 = c;
+        n  = 1;
+        return c;
+    }
+    const float vb = d5 * d2 - d1 * d6;
+    if(vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f)
+    {
+        y0 = a;
+        y1 = c;
+        n  = 2;
+        return a + (d2 / (d2 - d6)) * ac;
+    }
+    const float va = d3 * d6 - d5 * d4;
+    if(va <= 0.0f && d4 - d3 >= 0.0f && d5 - d6 >= 0.0f)
+    {
+        y0 = b;
+        y1 = c;
+        n  = 2;
+        return b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b);
+    }
+    const float den = 1.0f / (va + vb + vc);
+    y0              = a;
+    y1              = b;
+    y2              = c;
+    n               = 3;
+    return a + (vb * den) * ab + (vc * den) * ac;
+}
+
+constexpr int kGjk32MaxIter = 24;
+
+// For a pair that GJK's first iteration leaves open: GJK iterations in
+// FP32 on at most a triangle (a new point added to a triangle keeps the
+// nearest of the three faces through it), kept only for their support
+// planes.  Any direction v and the Minkowski support w along -v give the
+// lower bound v.w/|v| on the distance of the cores, whatever the simplex
+// arithmetic did, with the FP32 error bound of gjk_first_iteration_separates.
+// True: the largest bound exceeds the crusts by that margin, so the FP64 GJK
+// finds no contact either.  False (the FP64 GJK decides): the iterates
+// converged below the crusts (a contact or a near miss), reached the
+// origin, left the finite range, or ran out of iterations.
+GB_D bool gjk_fp32_separates(const Body<float>& A, const Body<float>& B, const M3<float>& RA,
+                             const M3<float>& RB, const V3<float>& d)
+{
+    Tr<float>       b2a;
+    const M3<float> RAt = transpose(RA);
+    b2a.R               = mul(RAt, RB);
+    b2a.o               = mul(RAt, d);
+    const float ct      = A.crust + B.crust;
+    const float margin  = 1e-4f * (A.rcirc + B.rcirc) + 1e-9f;
+    V3<float>   y0 = support(A, zero3<float>()) - apply(b2a, support(B, zero3<float>()));
+    V3<float>   y1 = y0, y2 = y0;
+    int         n  = 1;
+    V3<float>   v  = y0;
+    float       mu = -INFINITY;
+    for(int k = 0; k < kGjk32MaxIter; ++k)
+    {
+        const float vv = dot(v, v);
+        if(!(vv > 1e-30f))
+            return false;
+        const V3<float> w = support_first(A, -v)
+                            - apply(b2a, support_first(B, mul_t(b2a.R, v)));
+        const float vw = dot(v, w);
+        const float nv = sqrtf(vv);
+        const float g  = vw / nv;
+        if(!(g == g))
+            return false;
+        mu = fmaxf(mu, g);
+        if(mu > ct + margin)
+            return true;
+        if(nv - mu <= margin || vv - vw <= 1e-6f * vv)
+            return false;
+        if(n == 1)
+            v = closest_on_segment(y0, w, y0, y1, n);
+        else if(n == 2)
+            v = closest_on_triangle(y0, y1, w, y0, y1, y2, n);
+        else
+        {
+            // the faces of the tetrahedron through w: the nearest one
+            V3<float>       a0, a1, a2, b0, b1, b2, c0, c1, c2;
+            int             na, nb, nc;
+            const V3<float> pa = closest_on_triangle(w, y0, y1, a0, a1, a2, na);
+            const V3<float> pb = closest_on_triangle(w, y1, y2, b0, b1, b2, nb);
+            const V3<float> pc = closest_on_triangle(w, y0, y2, c0, c1, c2, nc);
+            const float     da = dot(pa, pa), db = dot(pb, pb), dc = dot(pc, pc);
+            if(da <= db && da <= dc)
+            {
+                v  = pa;
+                y0 = a0;
+                y1 = a1;
+                y2 = a2;
+                n  = na;
+            }
+            else if(db <= dc)
+            {
+                v  = pb;
+                y0 = b0;
+                y1 = b1;
+                y2 = b2;
+                n  = nb;
+            }
+            else
+            {
+                v  = pc;
+                y0 = c0;
+                y1 = c1;
+                y2 = c2;
+                n  = nc;
+            }
+        }
+    }
+    return false;
+}
+
 // Pair record p: contact detection, contact law, outputs.  QUEUE (the cull
 // pass, k_narrow): the pair is finished here when it is two spheres (closed
 // form) or out of contact by the bounding tests or GJK-JH's first iteration,
@@ -958,6 +1133,42 @@ __global__ void __launch_bounds__(128)
     for_each_pair(*total, [&](int64_t p) {
         narrow_pair<S, VAR, true>(p, pair_a, pair_b, st, tb, po, law_kind, has_kr, dt, counters,
                             gjk_queue, gjk_count);
+    });
+}
+
+// The mixed mode's FP32 stage over the cull pass's queue: a pair that
+// gjk_fp32_separates decides is finished here (no contact, the outputs the
+// FP64 GJK would store), the others go to the FP64 GJK's queue.
+__global__ void __launch_bounds__(128)
+    k_narrow_gjk32(const uint32_t* __restrict__ gjk_count, const int* __restrict__ flags,
+                   const uint32_t* __restrict__ gjk_queue, const uint32_t* __restrict__ pair_a,
+                   const uint32_t* __restrict__ pair_b, State<float> st, Tables<float> tb,
+                   PairOut<float> po, int law_kind, int has_kr, uint32_t* __restrict__ queue64,
+                   uint32_t* __restrict__ count64)
+{
+    grid_dep_sync();
+    if(step_aborted(flags))
+        return;
+    for_each_pair(*gjk_count, [&](int64_t q) {
+        const uint32_t    p = gjk_queue[q];
+        const uint32_t    a = pair_a[p], b = pair_b[p];
+        const uint32_t    ra = st.rb_id[a], rb = st.rb_id[b];
+        const Body<float> A  = load_body<float>(tb.shape, ra, tb.verts);
+        const Body<float> B  = load_body<float>(tb.shape, rb, tb.verts);
+        const M3<float>   RA = load_rot<float>(st, a), RB = load_rot<float>(st, b);
+        const V3<float>   d  = mk<float>(float(st.pos[0][b] - st.pos[0][a]),
+                                         float(st.pos[1][b] - st.pos[1][a]),
+                                         float(st.pos[2][b] - st.pos[2][a]));
+        if(gjk_fp32_separates(A, B, RA, RB, d))
+        {
+            const double xa[3] = {st.pos[0][a], st.pos[1][a], st.pos[2][a]};
+            Force<float> F;
+            F.f = F.t = F.m = zero3<float>();
+            store_pair<float>(po, p, F, zero3<float>(), uint8_t(0), law_kind, has_kr,
+                              no_contact<float>(), xa);
+        }
+        else
+            queue64[atomicAdd(count64, 1u)] = p;
     });
 }
 

@@ -158,7 +158,8 @@ typedef struct gb_stats {
     int64_t candidate_pairs;  /* ordered pairs passing the bounding-sphere test */
     int64_t contacts;         /* ordered particle pairs with overlap < 0         */
     int64_t obstacle_contacts;
-    int64_t gjk_calls;        /* particle pairs past the bounding tests (GJK) */
+    int64_t gjk_calls;        /* particle pairs past the bounding tests and GJK's first
+                                 iteration (queued for the GJK pass)           */
     int64_t gjk_iterations;
     int32_t status_flags; /* bit i set: device-side error (1 << -GB_E_x)    */
     int32_t n_cells;
@@ -167,6 +168,8 @@ typedef struct gb_stats {
     double cell_size;
     double grid_max[3];      /* linked-cell max corner actually used */
     int64_t kernel_launches; /* kernels launched by this context so far */
+    int64_t gjk_fp64_calls;  /* particle pairs solved by the FP64 GJK (GB_MIXED: those its
+                                FP32 stage leaves open; otherwise gjk_calls) */
 } gb_stats;
 
 /* ---- debug dump kinds -------------------------------------------------------- */
