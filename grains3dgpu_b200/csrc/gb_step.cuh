@@ -199,7 +199,10 @@ GB_D Law<S> load_law(const Law<store_t<S>>* t, int ma, int mb)
 // inflates its radii by a bound on the FP32 rounding, so an FP32 rejection
 // implies an FP64 rejection) skips most non-candidates before the FP64 test:
 // the candidate set is the FP64 test's.  The FP64 modes test in FP64 only.
-constexpr int kPairSlots = 16; // candidates kept per particle by the count pass
+// Candidates kept per particle by the count pass: 32 covers all but ~1e-4 of
+// the particles of a dense polydisperse bed (mean ~7, 99.9th percentile ~25);
+// the fill pass enumerates the rest again.
+constexpr int kPairSlots = 32;
 
 // Particle-obstacle pairs (ComponentManagerCPU.cpp:301-351) share the pair
 // list: after the particle pairs of A come A's obstacle candidates in obstacle
@@ -546,22 +549,33 @@ __global__ void __launch_bounds__(kBlock)
     const uint32_t cp   = c - (uint32_t)obstacle_candidates(mask, n_obs);
     if(cp <= kPairSlots)
     {
-        const uint32_t* mine = slot + (size_t)s * kPairSlots;
-        uint32_t        t[kPairSlots];
-        for(uint32_t k = 0; k < cp; ++k)
+        // the slots in registers (unused ones as 0xffffffff, above every
+        // sorted position), each written at its rank among them: a sort with
+        // static indices only, so nothing goes to local memory
+        const uint4* mine = reinterpret_cast<const uint4*>(slot + (size_t)s * kPairSlots);
+        uint32_t     t[kPairSlots];
+#pragma unroll
+        for(int q = 0; q < kPairSlots / 4; ++q)
         {
-            // insertion sort: a particle has a handful of candidates
-            const uint32_t v = mine[k];
-            uint32_t       j = k;
-            for(; j > 0 && t[j - 1] > v; --j)
-                t[j] = t[j - 1];
-            t[j] = v;
+            uint4 x = make_uint4(~0u, ~0u, ~0u, ~0u);
+            if((uint32_t)(4 * q) < cp)
+                x = mine[q];
+            t[4 * q]     = (uint32_t)(4 * q) < cp ? x.x : ~0u;
+            t[4 * q + 1] = (uint32_t)(4 * q + 1) < cp ? x.y : ~0u;
+            t[4 * q + 2] = (uint32_t)(4 * q + 2) < cp ? x.z : ~0u;
+            t[4 * q + 3] = (uint32_t)(4 * q + 3) < cp ? x.w : ~0u;
         }
-        for(uint32_t k = 0; k < cp; ++k)
-        {
-            pair_a[out + k] = a;
-            pair_b[out + k] = sids[t[k]];
-        }
+#pragma unroll
+        for(int k = 0; k < kPairSlots; ++k)
+            if((uint32_t)k < cp)
+            {
+                uint32_t r = 0;
+#pragma unroll
+                for(int j = 0; j < kPairSlots; ++j)
+                    r += t[j] < t[k];
+                pair_a[out + r] = a;
+                pair_b[out + r] = sids[t[k]];
+            }
         out += cp;
     }
     else
