@@ -667,20 +667,21 @@ def main():
     return 0
 
 
-# DRAM bytes (read + write) per particle of the dominant kernels, from one
-# ncu capture of this workload with 1,000,000 particles
-# (the summary of that capture is committed beside the other profiles); their
-# traffic scales with the particle count.  The narrow phase's scales with the
-# pairs that reach GJK and is not extrapolated.
-TRAFFIC_PER_PARTICLE = {"integration": (132.12e6 + 24.71e6) / 1_000_000,
-                        "pair_count": (62.00e6 + 1.13e6) / 1_000_000}
+# DRAM bytes (read + write) per particle of the HBM-rated kernels, from one
+# ncu capture of each on the bed with 200,000 grains (the summary of those
+# captures is committed beside the other profiles); their traffic scales with
+# the particle count at the bed's density.  The narrow phase's scales with
+# the pairs and is not extrapolated.
+TRAFFIC_PER_PARTICLE = {"integration": (32.71e6 + 0.13e6) / 200_000,
+                        "pair_count": (17.37e6 + 3.74e6) / 200_000}
 
 
-# what bounds each stage, from the ncu capture named above
-LIMITER = {"pair_count": "issue slots: 67% active, 26 of 32 lanes per instruction; "
-                         "~48 L1-resident neighbour tests per particle",
-           "integration": "memory latency and issue: 44% warps active, 52% issue slots, "
-                          "38% of DRAM peak",
+# what bounds each stage, from the captures named above
+LIMITER = {"pair_count": "memory latency of the neighbour walk: 11 long-scoreboard stalls per "
+                         "issue at 42% warps active, 43% issue slots; ~480 FP32 pre-tests per "
+                         "particle in 27 cells of 7.2 mm",
+           "integration": "memory latency: 38% warps active, 4.9 long-scoreboard stalls per "
+                          "issue, 164 B per particle moved",
            "broad_phase": "launch and tail latency of short kernels"}
 
 
