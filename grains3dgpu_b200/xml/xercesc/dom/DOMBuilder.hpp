@@ -1,0 +1,3 @@
+// Xerces-free stand-in: the DOM of gb_dom.hh (see there).
+#pragma once
+#include "../../gb_dom.hh"

@@ -59,6 +59,10 @@ public:
         T          ktOverKn   = T(0.8);    // tangential spring of GB_LAW_HOOKE_HISTORY
         int        device     = 0;
         int        flags      = 0;
+        // material id of each particle / obstacle rigid body; empty: the
+        // rigid body's own (RigidBody::getMaterial)
+        std::vector<int32_t> particleMaterials;
+        std::vector<int32_t> obstacleMaterials;
     };
 
     /** particleRB[nRigidBodies], obstacleRB[nObstacles] (one rigid body per
@@ -105,7 +109,11 @@ public:
         {
             std::vector<gb_rigid_body_desc> rbs(nRigidBodies);
             for(uint i = 0; i < nRigidBodies; ++i)
+            {
                 rbs[i] = describe(*particleRB[i]);
+                if(i < setup.particleMaterials.size())
+                    rbs[i].material = setup.particleMaterials[i];
+            }
             check(gb_set_rigid_bodies(m_ctx, rbs.data(), nullptr, 0), "gb_set_rigid_bodies");
             const uint nLaws = nMaterials * (nMaterials + 1) / 2;
             std::vector<gb_contact_model> laws(nLaws);
@@ -114,7 +122,11 @@ public:
             check(gb_set_contact_models(m_ctx, laws.data()), "gb_set_contact_models");
             m_obsRB.resize(nObstacles);
             for(uint i = 0; i < nObstacles; ++i)
+            {
                 m_obsRB[i] = describe(*obstacleRB[i]);
+                if(i < setup.obstacleMaterials.size())
+                    m_obsRB[i].material = setup.obstacleMaterials[i];
+            }
             m_obsId.resize(nObstacles);
             for(uint i = 0; i < nObstacles; ++i)
                 m_obsId[i] = i;

@@ -9,6 +9,8 @@
 // (Grains/Base/src/GrainsCPU.cpp:55-66).
 #include <cstdint>
 #include <cstring>
+#include <memory>
+#include <string>
 #include <vector>
 
 #include "ComponentManagerCPU.hh"
@@ -21,6 +23,7 @@
 #include "HookeContactForceModel.hh"
 #include "LinkedCell.hh"
 #include "OBB.hh"
+#include "RawDataPostProcessingWriter.hh"
 #include "Rectangle.hh"
 #include "RigidBody.hh"
 #include "Sphere.hh"
@@ -257,6 +260,9 @@ struct ref_ctx
     uint32_t                       ncells = 0;
     int64_t                        steps  = 0;
     bool                           detected = false;
+    // the reference's RawData writer (ref_rawdata_write) and its XML node
+    std::unique_ptr<DOMElement>                          raw_node;
+    std::unique_ptr<RawDataPostProcessingWriter<T>>      raw;
 };
 
 ref_ctx* ref_create(const gb_config* cfg, int* status)
@@ -282,10 +288,56 @@ ref_ctx* ref_create(const gb_config* cfg, int* status)
     return c;
 }
 
+// The reference's RawDataPostProcessingWriter (RawDataPostProcessingWriter.cpp:
+// 13-22 from an XML node, PostProcessing_start :63-71, PostProcessing :75-212,
+// PostProcessing_end :218-231) on the harness's particles and obstacles.  The
+// first call (`first` != 0) builds the writer from <RawData Directory=...
+// RootName=...> (through the Xerces-free ReaderXML) and starts it, which
+// removes earlier files of that root name in the directory; each call writes
+// one save at `time`.
+int ref_rawdata_write(ref_ctx* c, const char* directory, const char* root_name, double time,
+                      int32_t first)
+{
+    if(!c || !c->cm || !directory || !root_name)
+        return GB_E_INVALID_ARG;
+    if(first || !c->raw)
+    {
+        auto quote = [](std::string v) {
+            std::string o;
+            for(char ch : v)
+                o += ch == '"' ? std::string("&quot;") : ch == '&' ? std::string("&amp;")
+                     : ch == '<' ? std::string("&lt;") : std::string(1, ch);
+            return o;
+        };
+        std::string err;
+        c->raw.reset();
+        c->raw_node = gb::xml::parse("<RawData Directory=\"" + quote(directory) + "\" RootName=\""
+                                         + quote(root_name) + "\"/>",
+                                     &err);
+        if(!c->raw_node)
+            return GB_E_INVALID_ARG;
+        c->raw.reset(new RawDataPostProcessingWriter<T>(c->raw_node.get()));
+        c->raw->PostProcessing_start();
+    }
+    c->raw->PostProcessing(c->prb.data(), c->orb.data(), c->cm, T(time));
+    return GB_OK;
+}
+
+int ref_rawdata_close(ref_ctx* c)
+{
+    if(!c)
+        return GB_E_INVALID_ARG;
+    if(c->raw)
+        c->raw->PostProcessing_end();
+    c->raw.reset();
+    return GB_OK;
+}
+
 int ref_destroy(ref_ctx* c)
 {
     if(!c)
         return GB_E_INVALID_ARG;
+    c->raw.reset();
     delete c->cm;
     delete c->lc;
     delete c->ti;

@@ -1,8 +1,13 @@
-"""RawData post-processing output against the reference writer's format
-(RawDataPostProcessingWriter.cpp:75-212, realToString in GrainsUtils.hh:33-44),
-restated here: per component file one line per save, the time then every
-particle's value then every obstacle's (origin, zero velocities), "%.6e" with
-a zero printed as "0"."""
+"""RawData post-processing output of the engine (gb_rawdata_*):
+
+* byte for byte against the reference's own RawDataPostProcessingWriter
+  (RawDataPostProcessingWriter.cpp:63-231, compiled into oracle/_ref and run
+  by the harness on the same state);
+* against the format restated here (realToString, GrainsUtils.hh:33-44): per
+  component file one line per save, the time then every particle's value
+  then every obstacle's (origin, zero velocities), "%.6e" with a zero
+  printed as "0"; and the coordination-number option."""
+import ctypes as C
 import math
 
 import numpy as np
@@ -74,3 +79,44 @@ def test_rawdata_files(gb, tmp_path, precision, coordination):
     if coordination:
         assert any(int(x) > 0 for x in cn_want[-1].split()[1:])  # the column has contacts
     s.close()
+
+
+def test_rawdata_files_equal_the_reference_writer(gb, reference, tmp_path):
+    """The engine (FP64) and the reference harness hold the same states (the
+    harness's, set into the engine before each save); each writes its three
+    saves with its own writer; every file is byte-identical."""
+    from conftest import share_props
+    scene = scenes.superquadric_column(n=90, pitch=2.05e-3)
+    r = scenes.System(reference, scene)
+    g = scenes.System(gb, scene, precision=abi.GB_FP64)
+    share_props(g, r, reference)
+    write = reference.lib.ref_rawdata_write
+    write.restype = C.c_int
+    write.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_int32]
+    close = reference.lib.ref_rawdata_close
+    close.restype = C.c_int
+    close.argtypes = [C.c_void_p]
+    (tmp_path / "ref").mkdir()
+    (tmp_path / "gb").mkdir()
+    w = g.rawdata(str(tmp_path / "gb"), "run")
+    dt = scene.config["dt"]
+    for k, nsteps in enumerate((0, 7, 7)):
+        if nsteps:
+            r.step(nsteps)
+        g.set_transforms(r.transforms())
+        g.set_velocities(r.velocities())
+        t = dt * 7 * k
+        assert write(r.ctx, str(tmp_path / "ref").encode(), b"run", t, int(k == 0)) == 0
+        w.write(t)
+    assert close(r.ctx) == 0
+    w.close()
+    names = sorted(p.name for p in (tmp_path / "ref").iterdir())
+    assert names == sorted(p.name for p in (tmp_path / "gb").iterdir())
+    assert len(names) == 11
+    for name in names:
+        a = (tmp_path / "ref" / name).read_bytes()
+        b = (tmp_path / "gb" / name).read_bytes()
+        assert a == b, name
+    assert len((tmp_path / "ref" / "run_position_z.dat").read_bytes()) > 90 * 3 * 12
+    g.close()
+    r.close()
