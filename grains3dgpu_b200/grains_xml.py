@@ -139,14 +139,18 @@ def write_grains_xml(scene, directory, name="grains", steps=10, linked_cell_max=
     org = cfg["origin"]
     g = cfg["gravity"]
     end = (steps - 0.5) * dt  # the loop runs while t <= End + 1e-15, from t = 0
-    post = ""
+    # Grains::postProcess reads the front of the save-time queue every step
+    # (Grains.cpp:60-73), also once it is empty; the save times therefore run
+    # on past the end of the run.
+    every = save_every or steps
+    writers = ""
     if raw_data_root is not None:
-        every = save_every or steps
-        post = (f'    <PostProcessing>\n'
-                f'      <TimeSave Start="0" End="{_fmt((steps - 1) * dt)}" dt="{_fmt(every * dt)}"/>\n'
-                f'      <Writers>\n'
-                f'        <RawData Directory="{directory}" RootName="{raw_data_root}"/>\n'
-                f'      </Writers>\n    </PostProcessing>\n')
+        writers = (f'      <Writers>\n'
+                   f'        <RawData Directory="{directory}" RootName="{raw_data_root}"/>\n'
+                   f'      </Writers>\n')
+    post = (f'    <PostProcessing>\n'
+            f'      <TimeSave Start="0" End="{_fmt((2 * steps + every) * dt)}" dt="{_fmt(every * dt)}"/>\n'
+            f'{writers}    </PostProcessing>\n')
     xml = f'''<?xml version="1.0" encoding="iso-8859-1"?>
 <Grains3D Type="Standard" Precision="Double">
   <Construction>

@@ -197,7 +197,10 @@ public:
             b200->addExternalForces(Grains<T>::m_particleRigidBodyList, GP::m_gravity);
             b200->moveParticles(Grains<T>::m_particleRigidBodyList,
                                 Grains<T>::m_timeIntegrator);
-            Grains<T>::postProcess(b200);
+            // Grains::postProcess reads the next save time even when none is
+            // left (Grains.cpp:60-73); it runs only while one is
+            if(!GP::m_tSave.empty())
+                Grains<T>::postProcess(b200);
         }
         m_contacts = 0;
         for(int r : result)

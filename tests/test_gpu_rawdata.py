@@ -85,11 +85,9 @@ def test_rawdata_files_equal_the_reference_writer(gb, reference, tmp_path):
     """The engine (FP64) and the reference harness hold the same states (the
     harness's, set into the engine before each save); each writes its three
     saves with its own writer; every file is byte-identical."""
-    from conftest import share_props
     scene = scenes.superquadric_column(n=90, pitch=2.05e-3)
     r = scenes.System(reference, scene)
     g = scenes.System(gb, scene, precision=abi.GB_FP64)
-    share_props(g, r, reference)
     write = reference.lib.ref_rawdata_write
     write.restype = C.c_int
     write.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_int32]
