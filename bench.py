@@ -300,6 +300,31 @@ def measure_shapes(args, torch):
     return out
 
 
+def measure_drum(args, torch):
+    """The rotating-drum configuration (scenes.rotating_drum): 2,000,000 grains
+    (40% spheres, 30% cubes as polyhedra, 30% n = 6 superquadrics) in a drum
+    of radius 0.1 m turning at 30 rpm, its length scaled for the grains to
+    fill 40% of it, the tangential-history law, grain-wall friction 0.6:
+    `drum_steps` mixed steps in one gb_step call, and a shorter FP64 run of
+    the same drum for the ratio."""
+    scene = scenes.rotating_drum(n=args.drum_n)
+    out = {"workload": f"{scene.n:,} grains (40% spheres r=1 mm, 30% cubes 1.6 mm as "
+                       "polyhedra, 30% superquadrics n=6 1x1x0.7 mm) in a drum of radius "
+                       f"0.1 m turning at 30 rpm, {scene.notes}, wall mu 0.6, dt 1e-6 s",
+           "n_particles": scene.n}
+    for prec, key, k in ((abi.GB_MIXED, "mixed", args.drum_steps),
+                         (abi.GB_FP64, "fp64", max(1, args.drum_steps // 10))):
+        s, el, _, _, _, st = run_engine(args, scene, prec, k, 3, torch, 0, 1, timing=False)
+        tr = s.transforms()
+        out[key] = {"steps": k, "value": scene.n * k / el, "ms_per_step": el / k * 1e3,
+                    "contacts_last_step": int(st.contacts),
+                    "wall_contacts_last_step": int(st.obstacle_contacts),
+                    "finite": bool(np.isfinite(tr).all())}
+        s.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def force_error(scene, torch):
     """Single-step error of the mixed mode against the FP64 mode, both given
     the scene's FP64 pose: per contact (metrics.contact_force_errors: the
@@ -493,6 +518,8 @@ def main():
     ap.add_argument("--shape-steps", type=int, default=10)
     ap.add_argument("--no-shapes", action="store_true")
     ap.add_argument("--no-dilute", action="store_true")
+    ap.add_argument("--drum-n", type=int, default=2_000_000)
+    ap.add_argument("--drum-steps", type=int, default=5000)
     ap.add_argument("--timed-only", action="store_true",
                     help="run the headline's warm-up and timed steps only (for profilers)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
@@ -610,6 +637,10 @@ def main():
     if world == 1 and not args.no_shapes:
         shapes = measure_shapes(args, torch)
 
+    drum = None
+    if world == 1 and args.drum_steps > 0:
+        drum = measure_drum(args, torch)
+
     adj = None
     if world == 1 and not args.no_adjoint:
         adj = measure_adjoint(torch, args.adjoint_n, args.adjoint_steps)
@@ -657,6 +688,7 @@ def main():
             "dilute": dilute,
             "adjoint": adj,
             "other_shapes": shapes,
+            "drum": drum,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

@@ -20,7 +20,7 @@ GB_E_CAPACITY = -8
 GB_E_UNSUPPORTED = -9
 
 GB_SPHERE, GB_BOX, GB_CYLINDER, GB_CONE = 0, 1, 2, 3
-GB_SUPERQUADRIC, GB_POLYHEDRON, GB_RECTANGLE = 4, 5, 6
+GB_SUPERQUADRIC, GB_POLYHEDRON, GB_RECTANGLE, GB_DRUM = 4, 5, 6, 7
 GB_MAX_POLY_VERTICES = 64
 
 GB_FP64, GB_MIXED, GB_FP64_STRICT = 0, 1, 2
@@ -108,6 +108,7 @@ SYSTEM_API = {
     "get_rigid_body_props": (C.c_int, [_P, C.c_int32, C.POINTER(RigidBodyProps)]),
     "set_contact_models": (C.c_int, [_P, C.POINTER(ContactModel)]),
     "set_obstacles": (C.c_int, [_P, C.POINTER(RigidBodyDesc), _D]),
+    "set_obstacle_velocities": (C.c_int, [_P, _D]),
     "set_rigid_body_ids": (C.c_int, [_P, _U32]),
     "set_transforms": (C.c_int, [_P, _D]),
     "set_velocities": (C.c_int, [_P, _D]),

@@ -108,6 +108,27 @@ GB_D Contact<S> closest_rectangle(const Body<S>& A, const M3<S>& RA, const V3<S>
     return no_contact<S>();
 }
 
+// NEW (no reference shape): the inner wall of a drum of radius R about the
+// axis `ax` through oO.  The wall point nearest A's centre, w = oO + t + R e
+// (t the axial part of oA - oO, e the unit radial direction), and the inward
+// normal -e give the tangent plane that closest_rectangle meets.  A centre on
+// the axis has no nearest point: no contact.
+template <typename S>
+GB_D Contact<S> closest_drum(const Body<S>& A, const M3<S>& RA, const V3<S>& oA, const V3<S>& oO,
+                             const V3<S>& ax, S R)
+{
+    const V3<S> d  = oA - oO;
+    const V3<S> t  = dot(ax, d) * ax;
+    const V3<S> r  = d - t;
+    const S     nr = norm(r);
+    if(!(nr > S(1e-12) * R))
+        return no_contact<S>();
+    const V3<S> e = (S(1.0) / nr) * r;
+    V3<S>       w = oO + t;
+    w             = w + R * e;
+    return closest_rectangle(A, RA, oA, w, -e);
+}
+
 // ---------------------------------------------------------------------------
 // Contact laws.  Output: force on A, its torque about A's centre, and the
 // rolling moment (kr != 0).

@@ -125,6 +125,9 @@ struct gb_ctx
     double*  d_obs_mass = nullptr;
     double4* d_obs_plane = nullptr; // Rectangle planes: normal, normal . origin
     uint32_t obs_rect    = 0u;      // bit o: obstacle o (< 32) is a Rectangle
+    bool     obs_gjk     = false;   // some obstacle is neither a Rectangle nor a drum
+    std::vector<double> obs_vel;    // 6 per obstacle: velocity, angular velocity
+    double*  d_obs_vel   = nullptr;
     double*  d_rcirc64 = nullptr;
     double   rmax      = 0.0;     // the largest circumscribed radius (the candidate test's radius)
     // FP64 shape tables: aliases of the above in the FP64 modes, separate
@@ -301,6 +304,7 @@ Tables<S> tables_of(gb_ctx* c)
     t.obs_tr      = c->d_obs_tr;
     t.obs_mass    = c->d_obs_mass;
     t.obs_plane   = c->d_obs_plane;
+    t.obs_vel     = c->d_obs_vel;
     t.obs_rect    = c->obs_rect;
     t.n_obs       = c->nob;
     t.shape64     = (const RBShape<double>*)c->d_shape64;
@@ -429,13 +433,24 @@ int upload_obstacles(gb_ctx* c)
     // planes of the Rectangle obstacles (normal = the frame's z axis, n . origin)
     std::vector<double4> plane(std::max(c->nob, 1), make_double4(0, 0, 0, 0));
     c->obs_rect = 0u;
+    c->obs_gjk  = false;
     for(int i = 0; i < c->nob; ++i)
     {
         const double* t = c->obs_tr.data() + 12 * i;
         plane[i]        = make_double4(t[2], t[5], t[8], t[2] * t[9] + t[5] * t[10] + t[8] * t[11]);
         if(i < kMaskObstacles && c->obs[i].convex.type == GB_RECTANGLE)
             c->obs_rect |= 1u << i;
+        c->obs_gjk = c->obs_gjk || (c->obs[i].convex.type != GB_RECTANGLE
+                                    && c->obs[i].convex.type != GB_DRUM);
     }
+    // wall velocities (zero until gb_set_obstacle_velocities)
+    c->obs_vel.resize(6 * (size_t)c->nob, 0.0);
+    dfree(c->d_obs_vel);
+    GB_TRY(dalloc(&c->d_obs_vel, std::max<size_t>(c->obs_vel.size(), 6)));
+    GB_CK(cudaMemset(c->d_obs_vel, 0, std::max<size_t>(c->obs_vel.size(), 6) * sizeof(double)));
+    if(!c->obs_vel.empty())
+        GB_CK(cudaMemcpy(c->d_obs_vel, c->obs_vel.data(), c->obs_vel.size() * sizeof(double),
+                         cudaMemcpyHostToDevice));
     dfree(c->d_obs_plane);
     GB_TRY(dalloc(&c->d_obs_plane, plane.size()));
     GB_CK(cudaMemcpy(c->d_obs_plane, plane.data(), plane.size() * sizeof(double4),
@@ -865,9 +880,9 @@ int run_detect(gb_ctx* c, int phases)
             c->launches += 2;
             if(!c->nob)
                 return GB_OK;
-            const bool all_rect = c->nob <= kMaskObstacles
-                                  && c->obs_rect == ((c->nob == 32) ? ~0u : ((1u << c->nob) - 1u));
-            if(all_rect)
+            // Rectangles and drums are met by their own closed forms; any
+            // other obstacle needs the general GJK compiled in
+            if(!c->obs_gjk)
                 k_narrow_obstacles<S, false, GB_GJK_JH>
                     <<<one_wave((const void*)k_narrow_obstacles<S, false, GB_GJK_JH>), 128, 0, so>>>(
                     total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
@@ -1220,7 +1235,7 @@ int gb_destroy(gb_ctx* c)
     if(c->stream)
         cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->d_shape, c->d_inertia, c->d_verts, c->d_law, c->d_obs_shape, c->d_obs_tr,
-                    c->d_obs_mass, c->d_obs_plane, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
+                    c->d_obs_mass, c->d_obs_plane, c->d_obs_vel, c->d_rcirc64, c->d_pos, c->d_rot, c->d_vel, c->d_omg, c->d_frc,
                     c->d_trq, c->d_rb_id, c->d_hash, c->d_iota, c->d_k[0], c->d_k[1], c->d_i[0],
                     c->d_i[1], c->d_hist, c->d_part, c->d_cstart, c->d_ccount, c->d_spos, c->d_spos32, c->d_slot, c->d_sorted_of, c->d_obsmask_id, c->d_count,
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
@@ -1390,6 +1405,8 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
         if(obst[i].convex.type == GB_POLYHEDRON || obst[i].convex.type == GB_CYLINDER
            || obst[i].convex.type == GB_CONE)
             return GB_E_UNSUPPORTED;
+        if(obst[i].convex.type == GB_DRUM && !(obst[i].convex.p[0] > 0.0))
+            return GB_E_INVALID_ARG;
         if(obst[i].material < 0 || obst[i].material >= c->nmat)
             return GB_E_INVALID_ARG;
         GB_TRY(gb_rigid_body_properties(&obst[i], nullptr, &c->obs_props[i]));
@@ -1408,6 +1425,26 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
         return st;
     c->obs_set    = true;
     c->mask_valid = false;
+    return GB_OK;
+}
+
+int gb_set_obstacle_velocities(gb_ctx* c, const double* kin)
+{
+    if(!c || (c->nob && !kin))
+        return GB_E_INVALID_ARG;
+    if(!c->obs_set)
+        return GB_E_NOT_READY;
+    for(size_t k = 0; k < 6 * (size_t)c->nob; ++k)
+        if(!std::isfinite(kin[k]))
+            return GB_E_INVALID_ARG;
+    c->obs_vel.assign(kin, kin + 6 * (size_t)c->nob);
+    if(c->nob)
+    {
+        // ordered after the steps already launched, as every state update
+        GB_CK(cudaStreamSynchronize(c->stream));
+        GB_CK(cudaMemcpy(c->d_obs_vel, c->obs_vel.data(), c->obs_vel.size() * sizeof(double),
+                         cudaMemcpyHostToDevice));
+    }
     return GB_OK;
 }
 
@@ -1642,6 +1679,9 @@ int gb_adjoint_step(gb_ctx* c, const double* adj_next, double* adj_prev, double*
             return GB_E_UNSUPPORTED;
     for(const auto& ob : c->obs)
         if(ob.convex.type != GB_RECTANGLE)
+            return GB_E_UNSUPPORTED;
+    for(double v : c->obs_vel) // walls at rest only
+        if(v != 0.0)
             return GB_E_UNSUPPORTED;
     AdjLaws laws{};
     laws.n = nl;

@@ -318,6 +318,18 @@ int convex_props(const gb_convex& cv, const double* verts, double& volume, doubl
             bb[0] = lx, bb[1] = ly, bb[2] = 0.0;
             return GB_OK;
         }
+        case GB_DRUM:
+        {
+            // NEW: a wall (surface) only -- no volume, mass or inertia; the
+            // bounding sphere and box of the cylinder R, half-length L
+            const double R = p[0], L = p[1];
+            if(!(R > 0.0) || L < 0.0)
+                return GB_E_INVALID_ARG;
+            volume = 0.0;
+            rc     = std::sqrt(R * R + L * L);
+            bb[0] = R, bb[1] = R, bb[2] = L;
+            return GB_OK;
+        }
         case GB_POLYHEDRON:
         {
             if(!verts || cv.n_vertices < 4 || cv.n_vertices > GB_MAX_POLY_VERTICES)

@@ -40,6 +40,7 @@ struct Tables
     const double*                obs_tr; // 12 per obstacle (basis, origin)
     const double*                obs_mass;
     const double4*               obs_plane; // Rectangle planes: normal, normal . origin
+    const double*                obs_vel;   // 6 per obstacle: velocity, angular velocity
     uint32_t                     obs_rect;  // bit o: obstacle o (< 32) is a Rectangle
     int                          n_obs;
     // FP64 copies of the shape tables (read by the mixed mode's FP64 GJK)
@@ -682,7 +683,30 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
     Contact<S> ci    = no_contact<S>();
     if constexpr(is_mixed<S>())
     {
-        if(O.type == GB_RECTANGLE)
+        if(O.type == GB_DRUM)
+        {
+            // the wall point nearest A's centre and its tangent plane, in FP64
+            // relative to the centre; the FP32 pre-test, then the FP64 plane
+            // contact as for Rectangles
+            const V3<double> ax = mk<double>(ot[2], ot[5], ot[8]);
+            const V3<double> d  = mk<double>(xa[0] - ot[9], xa[1] - ot[10], xa[2] - ot[11]);
+            const V3<double> r  = d - dot(ax, d) * ax;
+            const double     nr = norm(r), R = tb.obs_shape64[o].p[0];
+            if(nr > 1e-12 * R)
+            {
+                const V3<double> e  = (1.0 / nr) * r;
+                const V3<double> w  = (R - nr) * e; // the wall point, from A's centre
+                const V3<S>      e32 = cvt3<S>(e);
+                const V3<S>      pA  = mul(RA, support(A, mul_t(RA, e32)));
+                if(S(R - nr) - dot(e32, pA) < S(1e-6))
+                {
+                    const Body<double> A64  = load_body<double>(tb.shape64, ra, tb.verts64);
+                    const M3<double>   RA64 = load_rot64(st, a);
+                    ci = to_f(closest_rectangle(A64, RA64, zero3<double>(), w, -e));
+                }
+            }
+        }
+        else if(O.type == GB_RECTANGLE)
         {
             // FP32 first; a contact (or a near miss within the rounding
             // margin) is recomputed in FP64 relative to the particle centre
@@ -704,6 +728,8 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
     }
     else if(O.type == GB_RECTANGLE)
         ci = closest_rectangle(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]));
+    else if(O.type == GB_DRUM)
+        ci = closest_drum(A, RA, oA, oO, mk<S>(RO.m[2], RO.m[5], RO.m[8]), O.p[0]);
     else if constexpr(GEN)
         ci = closest_points<VAR>(A, O, RA, RO, oA, oO, oO - oA, &iters);
     const bool hit = ci.overlap < S(0.0);
@@ -715,28 +741,34 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
         const S      m1 = S(tb.inertia[ra].mass);
         const S      m2 = S(tb.obs_mass[o]);
         const V3<S>  vA = load3<S>(st.vel, a), wA = load3<S>(st.omg, a);
-        V3<S>        arm, ptw;
+        V3<S>        arm, ptw, armO;
         if constexpr(is_mixed<S>())
         {
-            arm = ci.pt;
-            ptw = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)), S(xa[2] + to_d(ci.pt.z)));
+            arm  = ci.pt;
+            ptw  = mk<S>(S(xa[0] + to_d(ci.pt.x)), S(xa[1] + to_d(ci.pt.y)), S(xa[2] + to_d(ci.pt.z)));
+            armO = mk<S>(S(xa[0] - ot[9]), S(xa[1] - ot[10]), S(xa[2] - ot[11])) + ci.pt;
         }
         else
         {
-            arm = ci.pt - oA;
-            ptw = ci.pt;
+            arm  = ci.pt - oA;
+            ptw  = ci.pt;
+            armO = ci.pt - oO;
         }
+        // the wall's velocity at the contact point, v + w x (p - origin): zero
+        // for the reference's walls at rest (ComponentManagerCPU.cpp:330-340)
+        const double* ov  = tb.obs_vel + 6 * o;
+        const V3<S>   wO  = mk<S>(S(ov[3]), S(ov[4]), S(ov[5]));
+        const V3<S>   vOp = mk<S>(S(ov[0]), S(ov[1]), S(ov[2])) + cross(wO, armO);
         if(law_kind == GB_LAW_HOOKE)
         {
-            // obstacles have zero velocity (ComponentManagerCPU.cpp:330-340)
-            const V3<S> zero = zero3<S>();
-            const V3<S> rel  = (vA + cross(wA, ptw)) - (zero + cross(zero, ptw));
-            F                = hooke(L, ci, rel, wA - zero, m1, m2, arm);
+            const V3<S> rel = (vA + cross(wA, ptw)) - vOp;
+            F               = hooke(L, ci, rel, wA - wO, m1, m2, arm);
         }
         else
         {
             V3<S> xi;
-            F = hooke_history(L, ci, vA + cross(wA, arm), m1, m2, dt, zero3<S>(), xi, arm);
+            F = hooke_history(L, ci, (vA + cross(wA, arm)) - vOp, m1, m2, dt, zero3<S>(), xi,
+                              arm);
         }
         atomicAdd(&counters[0], 1ull);
     }

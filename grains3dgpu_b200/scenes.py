@@ -38,6 +38,7 @@ class Scene:
     contact_models: list     # dicts, l(l+1)/2+s indexed
     notes: str = ""
     lattice_counts: tuple = None  # sites per axis of the jittered lattice (site k = particle k)
+    obstacle_velocities: np.ndarray = None  # float64 [n_obstacles, 6] (moving walls) or None
 
     @property
     def n(self):
@@ -362,6 +363,98 @@ def sphere_bed(seed=1, n=60, box=(0.009, 0.009, 0.016), pitch=2.05e-3, sink=0.55
     return scene
 
 
+def drum_obstacles(radius, length, centre, material=1):
+    """A drum about the world y axis through `centre`: the cylindrical wall
+    (GB_DRUM, radius, half-length; frame z = world y) and the two end caps
+    (Rectangles at y = centre_y -+ length/2, normals pointing inwards)."""
+    descs = np.zeros(3, RB_DTYPE)
+    descs["density"] = 0.0
+    descs["material"] = material
+    descs[0]["type"] = abi.GB_DRUM
+    descs[0]["p"][:2] = [radius, 0.5 * length]
+    for k in (1, 2):
+        descs[k]["type"] = abi.GB_RECTANGLE
+        descs[k]["p"][:2] = [radius, radius]
+    tr = np.zeros((3, 12))
+    # frame axes as columns of the row-major basis: x -> x, y -> -z, z -> y
+    tr[0, :9] = [1, 0, 0, 0, 0, 1, 0, -1, 0]
+    tr[0, 9:] = centre
+    # cap at the low end: normal +y (frame z = y); high end: normal -y
+    tr[1, :9] = [1, 0, 0, 0, 0, 1, 0, -1, 0]
+    tr[1, 9:] = [centre[0], centre[1] - 0.5 * length, centre[2]]
+    tr[2, :9] = [1, 0, 0, 0, 0, -1, 0, 1, 0]
+    tr[2, 9:] = [centre[0], centre[1] + 0.5 * length, centre[2]]
+    return descs, tr
+
+
+def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=2.8e-3,
+                  length=None, wall_mu=0.6, margin=2.0e-3):
+    """The rotating-drum configuration: a seeded mix of 40% spheres (r = 1 mm),
+    30% cubes (edge 1.6 mm, as 8-vertex polyhedra) and 30% superquadrics
+    (n1 = n2 = 6, semi-axes 1, 1, 0.7 mm), randomly oriented on a jittered
+    `pitch` lattice filling the lowest `fill` of a drum of radius 0.1 m whose
+    axis is horizontal (world y), turning at 30 rpm (its wall and end caps
+    carry that surface velocity), grain-wall friction 0.6.  The drum's length
+    is scaled so that the n grains fit: 2,000,000 grains need ~3.5 m at 40%
+    of a 0.1 m cross-section (the nominal 0.05 m holds ~30,000)."""
+    rng = np.random.default_rng(seed)
+    kind = rng.choice(3, size=n, p=[0.4, 0.3, 0.3]).astype(np.uint32)
+    rbs = np.zeros(3, RB_DTYPE)
+    rbs["density"] = 2500.0
+    rbs[0]["type"] = abi.GB_SPHERE
+    rbs[0]["p"][0] = 1e-3
+    rbs[0]["crust"] = 5e-5
+    rbs[1]["type"] = abi.GB_POLYHEDRON
+    rbs[1]["n_vertices"] = 8
+    rbs[1]["first_vertex"] = 0
+    rbs[1]["crust"] = 0.04e-3
+    rbs[2]["type"] = abi.GB_SUPERQUADRIC
+    rbs[2]["p"] = [1e-3, 1e-3, 0.7e-3, 6.0, 6.0]
+    rbs[2]["crust"] = 0.035e-3
+    h = 0.8e-3
+    verts = np.array([[sx * h, sy * h, sz * h] for sx in (-1, 1) for sy in (-1, 1)
+                      for sz in (-1, 1)], float)
+    # lattice sites of a cross-section below the fill level, `margin` inside the wall
+    rin = radius - margin
+    # the fill level y0 (from the centre) whose circular segment holds `fill`
+    lo, hi = -rin, rin
+    for _ in range(60):
+        y0 = 0.5 * (lo + hi)
+        area = rin * rin * np.arccos(-y0 / rin) + y0 * np.sqrt(rin * rin - y0 * y0)
+        lo, hi = (y0, hi) if area < fill * np.pi * rin * rin else (lo, y0)
+    g = np.arange(-rin, rin + 1e-12, pitch)
+    X, Z = np.meshgrid(g, g, indexing="ij")
+    inside = (X * X + Z * Z <= rin * rin) & (Z <= y0)
+    sec = np.stack([X[inside], Z[inside]], 1)
+    layers = int(np.ceil(n / sec.shape[0]))
+    ends = max(margin, 2e-3)  # clearance from the end caps
+    if length is None:
+        length = 2 * ends + layers * pitch
+    ny = int(np.floor((length - 2 * ends) / pitch)) + 1
+    if sec.shape[0] * ny < n:
+        raise ValueError("the drum holds fewer lattice sites than grains")
+    k = np.arange(n)
+    c = k % sec.shape[0]
+    yl = k // sec.shape[0]
+    centre = np.array([radius + 1e-3, 0.5 * length, radius + 1e-3])
+    pos = np.stack([centre[0] + sec[c, 0], max(margin, 2e-3) + yl * pitch, centre[2] + sec[c, 1]],
+                   1)
+    pos += rng.uniform(-0.05 * pitch, 0.05 * pitch, size=pos.shape)
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = pos
+    walls, wtr = drum_obstacles(radius, length, centre)
+    box = (2 * radius + 2e-3, length, 2 * radius + 2e-3)
+    cfg = dict(n_particles=n, n_rigid_bodies=3, n_obstacles=3, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
+    laws = [law(), law(muc=wall_mu), law(muc=wall_mu)]
+    scene = Scene("rotating_drum", cfg, rbs, verts, kind, tr, np.zeros((n, 6)), walls, wtr,
+                  laws, notes=f"drum length {length:.3f} m, {sec.shape[0]} sites per layer")
+    omega = 2.0 * np.pi * rpm / 60.0
+    scene.obstacle_velocities = np.tile([0.0, 0.0, 0.0, 0.0, omega, 0.0], (3, 1))
+    return scene
+
+
 # ---------------------------------------------------------------------------
 class System:
     """Applies a Scene to one engine library bound by abi.Bound (gb_, or_ or
@@ -391,6 +484,10 @@ class System:
             self._check(lib.set_obstacles(
                 self.ctx, ob.ctypes.data_as(abi.C.POINTER(abi.RigidBodyDesc)),
                 abi.dptr(np.ascontiguousarray(scene.obstacle_transforms))), "set_obstacles")
+        if scene.obstacle_velocities is not None:
+            self._check(lib.set_obstacle_velocities(
+                self.ctx, abi.dptr(np.ascontiguousarray(scene.obstacle_velocities, np.float64))),
+                "set_obstacle_velocities")
         self._check(lib.set_rigid_body_ids(self.ctx, abi.u32ptr(np.ascontiguousarray(scene.rb_ids))),
                     "set_rigid_body_ids")
         self.set_transforms(scene.transforms)

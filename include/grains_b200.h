@@ -51,6 +51,7 @@ extern "C" {
  *   GB_SUPERQUADRIC  a b c n1 n2                  (Superquadric.cpp:10-17)
  *   GB_POLYHEDRON    (unused) vertices come from the vertex pool
  *   GB_RECTANGLE     half edge lengths LX/2 LY/2  (plane z=0 of its frame)
+ *   GB_DRUM          radius, half-length           (obstacles only; see below)
  */
 #define GB_SPHERE 0
 #define GB_BOX 1
@@ -59,6 +60,12 @@ extern "C" {
 #define GB_SUPERQUADRIC 4
 #define GB_POLYHEDRON 5
 #define GB_RECTANGLE 6
+/* NEW (no reference shape): an obstacle only -- the inner surface of a
+ * circular cylinder (a rotating drum's wall) of radius p[0] and half-length
+ * p[1] about its frame's z axis, the particles inside it.  A particle meets
+ * it at the tangent plane of the wall point nearest its centre, evaluated as
+ * closestPointsRectangle evaluates a plane (CollisionDetection.cpp:53-90). */
+#define GB_DRUM 7
 
 #define GB_MAX_POLY_VERTICES 64
 
@@ -201,6 +208,14 @@ int gb_set_contact_models(gb_ctx* ctx, const gb_contact_model* table);
 /* Obstacles: n_obstacles rigid bodies (density 0) and their transforms. */
 int gb_set_obstacles(gb_ctx* ctx, const gb_rigid_body_desc* obstacles,
                      const double* transforms);
+/* Moving walls (no counterpart in the reference, whose obstacles are at rest,
+ * ComponentManagerCPU.cpp:326-336): 6 doubles per obstacle, the velocity of
+ * its origin and its angular velocity (world axes).  They enter the contact
+ * laws as the wall's velocity at the contact point, v + w x (p - origin);
+ * the wall's geometry stays where gb_set_obstacles put it (a surface velocity:
+ * a drum turning about its own axis, a conveyor), and a caller that moves a
+ * wall calls gb_set_obstacles again between steps.  Zero until set. */
+int gb_set_obstacle_velocities(gb_ctx* ctx, const double* kin);
 
 /* ---- particle state (ComponentManager set/get, ComponentManager.hh:37-104) ------ */
 int gb_set_rigid_body_ids(gb_ctx* ctx, const uint32_t* ids);

@@ -491,6 +491,19 @@ static int convex_props(const gb_convex* cv, const double* verts, double* volume
             bb[2] = c;
             return 0;
         }
+        case GB_DRUM:
+        {
+            /* NEW: a wall only (no volume, mass or inertia); bounding sphere and
+               box of the cylinder of radius p[0] and half-length p[1] */
+            if(!(p[0] > 0.0) || p[1] < 0.0)
+                return GB_E_INVALID_ARG;
+            *volume = 0.0;
+            *rc     = sqrt(p[0] * p[0] + p[1] * p[1]);
+            bb[0]   = p[0];
+            bb[1]   = p[0];
+            bb[2]   = p[1];
+            return 0;
+        }
         case GB_RECTANGLE:
         {
             /* Rectangle.cpp:68-109 */
@@ -1300,15 +1313,13 @@ static void closest_spheres(const body_view* A, const body_view* B,
         no_contact(o);
 }
 
-static void closest_rectangle(const body_view* A, const double a2w[12],
-                              const double b2w[12], or_contact* o)
+/* closestPointsRectangle (CollisionDetection.cpp:53-90) against the plane
+   through rpt with normal rn_in (turned towards A's centre) */
+static void closest_plane(const body_view* A, const double a2w[12], const double rpt[3],
+                          const double rn_in[3], or_contact* o)
 {
-    /* closestPointsRectangle (CollisionDetection.cpp:53-90) */
-    double rpt[3], rn[3], d[3];
-    copy3(b2w + 9, rpt);
-    rn[0] = b2w[2];
-    rn[1] = b2w[5];
-    rn[2] = b2w[8];
+    double rn[3], d[3];
+    copy3(rn_in, rn);
     sub3(a2w + 9, rpt, d);
     scal3(copysign(1.0, dot3(rn, d)), rn, rn);
     double nrn[3] = {-rn[0], -rn[1], -rn[2]}, dir[3], sa[3], pA[3];
@@ -1331,6 +1342,43 @@ static void closest_rectangle(const body_view* A, const double a2w[12],
         no_contact(o);
 }
 
+static void closest_rectangle(const body_view* A, const double a2w[12],
+                              const double b2w[12], or_contact* o)
+{
+    /* the plane of the rectangle's frame: its origin, its z axis */
+    const double rn[3] = {b2w[2], b2w[5], b2w[8]};
+    closest_plane(A, a2w, b2w + 9, rn, o);
+}
+
+static void closest_drum(const body_view* A, const double a2w[12], const double b2w[12],
+                         double R, or_contact* o)
+{
+    /* NEW: the inner wall of a drum of radius R about its frame's z axis.  The
+       wall point nearest A's centre, w = origin + t + R e (t the axial part of
+       the centre's offset, e the unit radial direction), and the inward normal
+       -e give the tangent plane met as closest_plane meets a plane; a centre
+       on the axis has no nearest point: no contact. */
+    const double ax[3] = {b2w[2], b2w[5], b2w[8]};
+    double       d[3], t[3], r[3], e[3], w[3], rn[3];
+    sub3(a2w + 9, b2w + 9, d);
+    scal3(dot3(ax, d), ax, t);
+    sub3(d, t, r);
+    const double nr = norm3(r);
+    if(!(nr > 1e-12 * R))
+    {
+        no_contact(o);
+        return;
+    }
+    scal3(1.0 / nr, r, e);
+    add3(b2w + 9, t, w);
+    scal3(R, e, t);
+    add3(w, t, w);
+    rn[0] = -e[0];
+    rn[1] = -e[1];
+    rn[2] = -e[2];
+    closest_plane(A, a2w, w, rn, o);
+}
+
 static void closest_points(const body_view* A, const body_view* B,
                            const double a2w[12], const double b2w[12], int variant,
                            or_contact* o)
@@ -1344,6 +1392,11 @@ static void closest_points(const body_view* A, const body_view* B,
     else if(B->cv->type == GB_RECTANGLE)
     {
         closest_rectangle(A, a2w, b2w, o);
+        return;
+    }
+    else if(B->cv->type == GB_DRUM)
+    {
+        closest_drum(A, a2w, b2w, B->cv->p[0], o);
         return;
     }
     double d[3];
@@ -1816,6 +1869,7 @@ struct or_ctx
     gb_rigid_body_desc* obs;
     gb_rigid_body_props* obp;
     double*             obs_tr;
+    double*             obs_vel; /* 6 per obstacle: velocity, angular velocity */
     gb_contact_model*   cm;
     uint32_t*           rb_id;
     double*             tr;    /* 12 per particle */
@@ -1878,6 +1932,7 @@ or_ctx* or_create(const gb_config* cfg, int* status)
         c->obs     = xcalloc(c->nob, sizeof(gb_rigid_body_desc));
         c->obp     = xcalloc(c->nob, sizeof(gb_rigid_body_props));
         c->obs_tr  = xcalloc((size_t)c->nob * 12, sizeof(double));
+        c->obs_vel = xcalloc((size_t)c->nob * 6 + 1, sizeof(double));
         c->cm      = xcalloc((size_t)c->nmat * (c->nmat + 1) / 2, sizeof(gb_contact_model));
         c->rb_id   = xcalloc(n, sizeof(uint32_t));
         c->tr      = xcalloc(n * 12, sizeof(double));
@@ -1908,6 +1963,7 @@ int or_destroy(or_ctx* c)
     free(c->obs);
     free(c->obp);
     free(c->obs_tr);
+    free(c->obs_vel);
     free(c->cm);
     free(c->rb_id);
     free(c->tr);
@@ -2047,6 +2103,15 @@ int or_set_obstacles(or_ctx* c, const gb_rigid_body_desc* obst, const double* tr
             return st;
     }
     memcpy(c->obs_tr, tr, (size_t)c->nob * 12 * sizeof(double));
+    return GB_OK;
+}
+
+int or_set_obstacle_velocities(or_ctx* c, const double* kin)
+{
+    /* NEW (gb_set_obstacle_velocities): the walls' surface velocities */
+    if(!c || (c->nob && !kin))
+        return GB_E_INVALID_ARG;
+    memcpy(c->obs_vel, kin, (size_t)c->nob * 6 * sizeof(double));
     return GB_OK;
 }
 
@@ -2323,17 +2388,18 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
             {
                 const gb_contact_model* cm = model_for(c, rbA->material, c->obs[o].material);
                 const double*           v1 = c->kin + 6 * a;
-                double                  k1[3], rv[3], rw[3];
+                const double*           vo = c->obs_vel + 6 * o;
+                double                  k1[3], k2[3], rv[3], rw[3], ro[3];
+                /* the wall's velocity at the contact point, v + w ^ (p - origin):
+                   zero for the reference's walls at rest (ComponentManagerCPU.cpp:
+                   326-336; NEW for moving walls) */
+                sub3(ci.pt, trO + 9, ro);
+                kin_at_point(vo, ro, k2);
                 if(!hist)
                 {
-                    double zk[6] = {0, 0, 0, 0, 0, 0}, k2[3];
                     kin_at_point(v1, ci.pt, k1);
-                    kin_at_point(zk, ci.pt, k2);
                     sub3(k1, k2, rv);
-                    copy3(v1 + 3, rw);
-                    rw[0] -= 0.0;
-                    rw[1] -= 0.0;
-                    rw[2] -= 0.0;
+                    sub3(v1 + 3, vo + 3, rw);
                     hooke_forces(cm, &ci, rv, rw, prA->mass, c->obp[o].mass, trA + 9, F, Tq);
                 }
                 else
@@ -2341,7 +2407,8 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
                     /* wall history is not kept: walls use a fresh spring each step */
                     double ra[3], z[3] = {0, 0, 0}, xi[3];
                     sub3(ci.pt, trA + 9, ra);
-                    kin_at_point(v1, ra, rv);
+                    kin_at_point(v1, ra, k1);
+                    sub3(k1, k2, rv);
                     history_forces(cm, &ci, rv, prA->mass, c->obp[o].mass, c->cfg.dt, z,
                                    xi, trA + 9, F, Tq);
                 }

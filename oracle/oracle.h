@@ -73,6 +73,7 @@ int or_set_contact_models(or_ctx* ctx, const gb_contact_model* table);
 int or_set_rigid_body_props(or_ctx* ctx, int32_t rb, const gb_rigid_body_props* props);
 int or_set_obstacles(or_ctx* ctx, const gb_rigid_body_desc* obstacles,
                      const double* transforms);
+int or_set_obstacle_velocities(or_ctx* ctx, const double* kin);
 int or_set_rigid_body_ids(or_ctx* ctx, const uint32_t* ids);
 int or_set_transforms(or_ctx* ctx, const double* transforms);
 int or_set_velocities(or_ctx* ctx, const double* kin);
