@@ -387,7 +387,7 @@ def drum_obstacles(radius, length, centre, material=1):
     return descs, tr
 
 
-def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=2.8e-3,
+def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=3.3e-3,
                   length=None, wall_mu=0.6, margin=2.0e-3):
     """The rotating-drum configuration: a seeded mix of 40% spheres (r = 1 mm),
     30% cubes (edge 1.6 mm, as 8-vertex polyhedra) and 30% superquadrics
@@ -395,8 +395,12 @@ def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=2.8
     `pitch` lattice filling the lowest `fill` of a drum of radius 0.1 m whose
     axis is horizontal (world y), turning at 30 rpm (its wall and end caps
     carry that surface velocity), grain-wall friction 0.6.  The drum's length
-    is scaled so that the n grains fit: 2,000,000 grains need ~3.5 m at 40%
-    of a 0.1 m cross-section (the nominal 0.05 m holds ~30,000)."""
+    is scaled so that the n grains fit: 2,000,000 grains need ~6 m at 40% of
+    a 0.1 m cross-section (the nominal 0.05 m holds ~17,000).  The default
+    pitch, 3.3 mm with +-2% jitter, keeps every pair of bounding spheres apart
+    (2 x 1.58 mm, the superquadric's box half-diagonal, is the largest reach):
+    randomly oriented cores that start intersecting meet GJK at a zero
+    distance, whose contact normal is 0/0 in the reference's algorithm."""
     rng = np.random.default_rng(seed)
     kind = rng.choice(3, size=n, p=[0.4, 0.3, 0.3]).astype(np.uint32)
     rbs = np.zeros(3, RB_DTYPE)
@@ -439,7 +443,7 @@ def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=2.8
     centre = np.array([radius + 1e-3, 0.5 * length, radius + 1e-3])
     pos = np.stack([centre[0] + sec[c, 0], max(margin, 2e-3) + yl * pitch, centre[2] + sec[c, 1]],
                    1)
-    pos += rng.uniform(-0.05 * pitch, 0.05 * pitch, size=pos.shape)
+    pos += rng.uniform(-0.02 * pitch, 0.02 * pitch, size=pos.shape)
     tr = np.zeros((n, 12))
     tr[:, :9] = random_rotations(rng, n)
     tr[:, 9:] = pos
