@@ -307,10 +307,12 @@ def measure_drum(args, torch):
     fill 40% of it, the tangential-history law, grain-wall friction 0.6:
     `drum_steps` mixed steps in one gb_step call, and a shorter FP64 run of
     the same drum for the ratio."""
-    scene = scenes.rotating_drum(n=args.drum_n)
+    scene = scenes.rotating_drum(n=args.drum_n, margin=1.7e-3, v_sigma=0.1)
     out = {"workload": f"{scene.n:,} grains (40% spheres r=1 mm, 30% cubes 1.6 mm as "
                        "polyhedra, 30% superquadrics n=6 1x1x0.7 mm) in a drum of radius "
-                       f"0.1 m turning at 30 rpm, {scene.notes}, wall mu 0.6, dt 1e-6 s",
+                       f"0.1 m turning at 30 rpm, {scene.notes}, wall mu 0.6, dt 1e-6 s; "
+                       "initial velocities N(0, 0.1 m/s) per component so that neighbours "
+                       "0.13 mm apart on the lattice collide within the run",
            "n_particles": scene.n}
     for prec, key, k in ((abi.GB_MIXED, "mixed", args.drum_steps),
                          (abi.GB_FP64, "fp64", max(1, args.drum_steps // 10))):

@@ -388,7 +388,7 @@ def drum_obstacles(radius, length, centre, material=1):
 
 
 def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=3.3e-3,
-                  length=None, wall_mu=0.6, margin=2.0e-3):
+                  length=None, wall_mu=0.6, margin=2.0e-3, v_sigma=0.0):
     """The rotating-drum configuration: a seeded mix of 40% spheres (r = 1 mm),
     30% cubes (edge 1.6 mm, as 8-vertex polyhedra) and 30% superquadrics
     (n1 = n2 = 6, semi-axes 1, 1, 0.7 mm), randomly oriented on a jittered
@@ -400,7 +400,9 @@ def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=3.3
     pitch, 3.3 mm with +-2% jitter, keeps every pair of bounding spheres apart
     (2 x 1.58 mm, the superquadric's box half-diagonal, is the largest reach):
     randomly oriented cores that start intersecting meet GJK at a zero
-    distance, whose contact normal is 0/0 in the reference's algorithm."""
+    distance, whose contact normal is 0/0 in the reference's algorithm.
+    `v_sigma` > 0 draws initial velocities N(0, v_sigma) per component (last
+    in the draw order), so that neighbours meet within a short run."""
     rng = np.random.default_rng(seed)
     kind = rng.choice(3, size=n, p=[0.4, 0.3, 0.3]).astype(np.uint32)
     rbs = np.zeros(3, RB_DTYPE)
@@ -452,7 +454,10 @@ def rotating_drum(seed=4, n=2_000_000, radius=0.1, rpm=30.0, fill=0.4, pitch=3.3
     cfg = dict(n_particles=n, n_rigid_bodies=3, n_obstacles=3, n_materials=2,
                origin=(0, 0, 0), max_coordinate=box, dt=1e-6, gravity=(0, 0, -9.81))
     laws = [law(), law(muc=wall_mu), law(muc=wall_mu)]
-    scene = Scene("rotating_drum", cfg, rbs, verts, kind, tr, np.zeros((n, 6)), walls, wtr,
+    vel = np.zeros((n, 6))
+    if v_sigma > 0.0:
+        vel[:, :3] = rng.normal(0.0, v_sigma, size=(n, 3))
+    scene = Scene("rotating_drum", cfg, rbs, verts, kind, tr, vel, walls, wtr,
                   laws, notes=f"drum length {length:.3f} m, {sec.shape[0]} sites per layer")
     omega = 2.0 * np.pi * rpm / 60.0
     scene.obstacle_velocities = np.tile([0.0, 0.0, 0.0, 0.0, omega, 0.0], (3, 1))
