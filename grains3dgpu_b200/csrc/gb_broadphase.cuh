@@ -23,7 +23,9 @@ constexpr int kFlagCellCrowded = 1 << 9; // a cell too full for the counting sor
 // Either one aborts the step: the kernels that write pair lists or state
 // return at entry once it is set, and the host replays the step.
 constexpr int kFlagScanStall   = 1 << 10; // a one-pass scan gave up waiting (never expected)
-constexpr int kFlagAbort = kFlagCapacity | kFlagCellCrowded;
+// a step with any of these leaves the state untouched: every later kernel of
+// the step returns at entry (a stalled scan's offsets are not to be used)
+constexpr int kFlagAbort = kFlagCapacity | kFlagCellCrowded | kFlagScanStall;
 
 // The flags a kernel checks at entry were set by earlier kernels, so a plain
 // (L1-cached) load sees them; a volatile load from every thread of a
@@ -147,11 +149,11 @@ __global__ void k_hash_count(int n, const double* __restrict__ px, const double*
 // one of its cell's slots by decrementing it
 __global__ void k_cell_scatter(int n, const uint32_t* __restrict__ keys,
                                const uint32_t* __restrict__ cstart, uint32_t* __restrict__ count,
-                               uint32_t* __restrict__ unordered)
+                               uint32_t* __restrict__ unordered, const int* abort_flags)
 {
     grid_dep_sync();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if(i >= n)
+    if(i >= n || step_aborted(abort_flags))
         return;
     const uint32_t key  = keys[i];
     const uint32_t slot = cstart[key] + atomicSub(&count[key], 1u) - 1u;
@@ -195,7 +197,7 @@ __global__ void k_cell_rank(int n, const uint32_t* __restrict__ unordered,
 {
     grid_dep_sync();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if(t >= n)
+    if(t >= n || step_aborted(flags))
         return;
     const uint32_t e   = unordered[t];
     const uint32_t key = keys[e];
@@ -431,14 +433,15 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply(const uint32_t* __restric
 // In place (in == out) is allowed.  abort_flags as for k_scan_apply.
 constexpr unsigned long long kScanAggregate = 1ull, kScanPrefix = 2ull;
 constexpr uint32_t           kScanEpochMask = (1u << 30) - 1u;
-constexpr uint32_t           kScanSpinLimit = 1u << 20;
+constexpr uint32_t           kScanSpinLimit = 1u << 20; // the default bound of the wait
 
 __global__ void __launch_bounds__(kBlock)
     k_scan_onepass(const uint32_t* in, uint32_t* out, int64_t n,
                    unsigned long long* __restrict__ tile_state,
                    unsigned long long* __restrict__ ticket, unsigned long long ticket_base,
                    uint32_t epoch, uint32_t* __restrict__ grand_total,
-                   const int* abort_flags, int* __restrict__ flags)
+                   const int* abort_flags, int* __restrict__ flags,
+                   uint32_t spin_limit = kScanSpinLimit)
 {
     grid_dep_sync();
     __shared__ uint32_t s_tile, s_prefix;
@@ -497,10 +500,10 @@ __global__ void __launch_bounds__(kBlock)
                     }
                     if(!__any_sync(0xffffffffu, st == 0ull))
                         break;
-                    if(++spins > kScanSpinLimit)
+                    if(++spins > spin_limit)
                         break;
                 }
-                if(spins > kScanSpinLimit)
+                if(spins > spin_limit)
                 {
                     if(lane == 0)
                         atomicOr(flags, kFlagScanStall);

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -173,6 +174,7 @@ struct gb_ctx
     size_t              tile_cap     = 0;
     unsigned long long  tickets      = 0;
     uint32_t            scan_epoch   = 0;
+    uint32_t            scan_spin_limit = kScanSpinLimit; // GB_DEBUG_SCAN_SPIN_LIMIT
 
     // pairs (double-buffered for the tangential history)
     uint32_t* d_count = nullptr;
@@ -591,7 +593,8 @@ int scan_u32(gb_ctx* c, const uint32_t* in, uint32_t* out, int64_t n, uint32_t* 
         c->scan_epoch = 1;
     }
     GB_CK(launch(c->pdl, k_scan_onepass, nb, kBlock, c->stream, in, out, n, c->d_tile_state,
-                 c->d_ticket, c->tickets, c->scan_epoch, d_total, abort_flags, c->d_flags));
+                 c->d_ticket, c->tickets, c->scan_epoch, d_total, abort_flags, c->d_flags,
+                 c->scan_spin_limit));
     c->tickets += (unsigned long long)nb;
     c->launches += 1;
     GB_CK(cudaGetLastError());
@@ -687,7 +690,7 @@ int broad_phase_counting(gb_ctx* c)
     mark(c, 1);
     GB_TRY(scan_u32(c, c->d_ccount, c->d_cstart, (int64_t)c->ncells + 1, nullptr));
     GB_CK(launch(c->pdl, k_cell_scatter, nb, kBlock, s, n, c->d_hash, c->d_cstart, c->d_ccount,
-                 c->d_i[0]));
+                 c->d_i[0], (const int*)c->d_flags));
     c->ccount_zero = true; // each particle took back the count it added
     c->launches += 1;
     GB_CK(cudaGetLastError());
@@ -754,7 +757,8 @@ int build_pairs(gb_ctx* c)
     geo.rmax = c->rmax;
     GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_spos,
                  spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], geo, c->d_count,
-                 c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob));
+                 c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob,
+                 (const int*)c->d_flags));
     c->launches += 1;
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));
@@ -1032,6 +1036,7 @@ void restore(gb_ctx* c, const StepSnap& s)
     c->links_valid    = s.links_valid;
     c->steps_done     = s.steps_done;
     c->count_zero     = false; // an aborted fill pass may have left counts behind
+    c->ccount_zero    = false; // ... and an aborted scatter pass cell counts
 }
 
 // Launches n_steps detects (PHASE_DETECT) or fused steps (PHASE_STEP) with no
@@ -1086,6 +1091,14 @@ int run_steps(gb_ctx* c, int32_t n_steps, int phases, int32_t* result)
             return GB_E_CUDA; // an abort flag with every launch completed: inconsistent
         c->ev_npending = 0;   // the aborted launches' phase times mean nothing
         restore(c, snaps[ok]);
+        if(flags & kFlagScanStall)
+        {
+            // a scan gave up waiting: the step is not replayed; the state is
+            // that before the aborted step, the flags are cleared
+            c->last.status_flags |= flags;
+            GB_CK(cudaMemset(c->d_flags, 0, sizeof(int)));
+            return GB_E_CUDA;
+        }
         if(flags & kFlagCellCrowded)
             c->radix_sort = true;
         if(flags & kFlagCapacity)
@@ -1186,6 +1199,10 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
         return fail(GB_E_NO_DEVICE);
     gb_ctx* c = new gb_ctx;
     c->cfg    = *cfg;
+    // test knob: a lower bound on the one-pass scans' look-back wait makes it
+    // run out, which a step reports as GB_E_CUDA with the state untouched
+    if(const char* lim = std::getenv("GB_DEBUG_SCAN_SPIN_LIMIT"))
+        c->scan_spin_limit = (uint32_t)std::strtoul(lim, nullptr, 10);
     c->prec   = cfg->precision;
     c->n      = cfg->n_particles;
     c->nrb    = cfg->n_rigid_bodies;

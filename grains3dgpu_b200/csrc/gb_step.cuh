@@ -431,12 +431,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
                  CellGeometry geo, uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
-                 uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs)
+                 uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs,
+                 const int* abort_flags)
 {
     grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
     const int      s      = blockIdx.x * blockDim.x + threadIdx.x;
-    if(s >= n)
+    if(s >= n || step_aborted(abort_flags))
         return;
     if(n_obs)
     {
