@@ -1314,7 +1314,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
-                uint32_t* __restrict__ mask_out, const int* __restrict__ flags,
+                uint32_t* __restrict__ mask_out, int* __restrict__ flags,
                 unsigned int* __restrict__ done)
 {
     grid_dep_sync();
@@ -1463,6 +1463,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
         st.omg[0][i] = (store_t<S>)to_d(w.x);
         st.omg[1][i] = (store_t<S>)to_d(w.y);
         st.omg[2][i] = (store_t<S>)to_d(w.z);
+        // a move that leaves a non-finite state is reported by its own step
+        // (the next step's hash would report it one step late)
+        if(!(isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]) && isfinite(to_d(v.x))
+             && isfinite(to_d(v.y)) && isfinite(to_d(v.z)) && isfinite(to_d(w.x))
+             && isfinite(to_d(w.y)) && isfinite(to_d(w.z))))
+            atomicOr(flags, kFlagNonFinite);
         if(sp.phases != PHASE_STEP || sp.accumulate)
         {
             // Torce::reset
