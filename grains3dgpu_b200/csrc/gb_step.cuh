@@ -506,6 +506,31 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
     }
 }
 
+// Ascending sort of t[0, N) in registers by a bitonic network (Batcher, 1968):
+// every index is a compile-time constant once unrolled.
+template <int N, int M>
+GB_D void bitonic_sort(uint32_t (&t)[M])
+{
+    static_assert(N <= M && (N & (N - 1)) == 0, "a power of two within the array");
+#pragma unroll
+    for(int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for(int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for(int i = 0; i < N; ++i)
+            {
+                const int l = i ^ j;
+                if(l > i)
+                {
+                    const uint32_t x = t[i], y = t[l];
+                    const uint32_t lo = min(x, y), hi = max(x, y);
+                    const bool     up = (i & k) == 0;
+                    t[i]              = up ? lo : hi;
+                    t[l]              = up ? hi : lo;
+                }
+            }
+}
+
 // Fill pass, one thread per particle id a (most have no candidate and read
 // only count[a]): the pair records of a at offset[a] -- its particle
 // candidates from the slots of its sorted position s = sorted_of[a], sorted
@@ -552,8 +577,8 @@ __global__ void __launch_bounds__(kBlock)
     if(cp <= kPairSlots)
     {
         // the slots in registers (unused ones as 0xffffffff, above every
-        // sorted position), each written at its rank among them: a sort with
-        // static indices only, so nothing goes to local memory
+        // sorted position), sorted with static indices only, so nothing goes
+        // to local memory
         const uint4* mine = reinterpret_cast<const uint4*>(slot + (size_t)s * kPairSlots);
         uint32_t     t[kPairSlots];
 #pragma unroll
@@ -567,16 +592,22 @@ __global__ void __launch_bounds__(kBlock)
             t[4 * q + 2] = (uint32_t)(4 * q + 2) < cp ? x.z : ~0u;
             t[4 * q + 3] = (uint32_t)(4 * q + 3) < cp ? x.w : ~0u;
         }
+        // a bitonic network over the warp's largest count (rounded up to 8,
+        // 16 or 32 slots): one code path per warp, ~80 compare-exchanges for
+        // the common 16 instead of 32 x 32 rank comparisons
+        const uint32_t wmax = __reduce_max_sync(__activemask(), cp);
+        if(wmax <= 8)
+            bitonic_sort<8>(t);
+        else if(wmax <= 16)
+            bitonic_sort<16>(t);
+        else
+            bitonic_sort<kPairSlots>(t);
 #pragma unroll
         for(int k = 0; k < kPairSlots; ++k)
             if((uint32_t)k < cp)
             {
-                uint32_t r = 0;
-#pragma unroll
-                for(int j = 0; j < kPairSlots; ++j)
-                    r += t[j] < t[k];
-                pair_a[out + r] = a;
-                pair_b[out + r] = sids[t[k]];
+                pair_a[out + k] = a;
+                pair_b[out + k] = sids[t[k]];
             }
         out += cp;
     }
@@ -1167,7 +1198,7 @@ GB_D void for_each_pair(int64_t npairs, F&& f)
 // resident warps, so that a warp holds one or two GJK chains rather than
 // every GJK pair among 32 consecutive records of the list.
 template <typename S, int VAR>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, sizeof(store_t<S>) == 4 ? 5 : 1)
     k_narrow(const uint32_t* __restrict__ total, const int* __restrict__ flags,
              const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
              State<store_t<S>> st, Tables<S> tb, PairOut<store_t<S>> po, int law_kind, int has_kr,

@@ -90,6 +90,28 @@ def test_broad_phase_and_pairs_bit_exact_large(gb, oracle, precision):
     o.close()
 
 
+def test_broad_phase_and_pairs_bit_exact_polyhedra_200k(gb, oracle):
+    """The polyhedra configuration at its full size: 200,000 convex hulls of
+    8-32 points on ellipsoids, seeded on the 2.6 mm jittered lattice of a
+    100 x 100 x 400 mm box.  Cell hashes, sorted ids, cell starts, neighbour
+    table, candidate pairs and contact pairs equal the oracle's (FP64 strict),
+    and the mixed mode's candidate and contact pairs equal them too."""
+    scene = scenes.polyhedra_box(n=200_000, hull_centroid=hull_centroid)
+    systems = [scenes.System(gb, scene, precision=p) for p in (abi.GB_FP64_STRICT, abi.GB_MIXED)]
+    o = scenes.System(oracle, scene)
+    share_props(systems[0], o, oracle)  # the same hull volumes and radii
+    o.detect()
+    want = {k: o.dump(k) for k in BROAD_DUMPS + [abi.GB_DUMP_CONTACT_PAIRS]}
+    assert want[abi.GB_DUMP_CANDIDATE_PAIRS].shape[0] > 100_000
+    for g in systems:
+        g.detect()
+        for kind_, b in want.items():
+            a = g.dump(kind_)
+            assert a.shape == b.shape and np.array_equal(a, b), f"dump {kind_} differs"
+        g.close()
+    o.close()
+
+
 @pytest.mark.parametrize("kind", ["sphere", "box-on-walls", "polyhedron"])
 def test_single_step_torce_bit_exact(gb, oracle, kind):
     scene = make_scene(kind)
