@@ -164,6 +164,15 @@ struct gb_ctx
                                   // mixed mode: a second queue for its FP64 GJK after it)
     uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
+    // the finer candidate grid of polydisperse packings (k_pair_count_fine)
+    bool      fine_planned = false, fine = false, fcount_zero = false;
+    FineGrid  fine_g{};
+    uint32_t  fine_nf = 0, fine_nlarge = 0;
+    std::vector<uint32_t> h_rb_id; // the rigid-body ids as last set from the host
+    uint32_t *d_fkey = nullptr, *d_fcount = nullptr, *d_fstart = nullptr, *d_fskey = nullptr,
+             *d_fids = nullptr, *d_fref = nullptr;
+    double4*  d_fpos   = nullptr;
+    float4*   d_fpos32 = nullptr;
     uint32_t* d_obsmask_id = nullptr; // the same per particle id, from the last move
     bool      mask_valid   = false;   // d_obsmask_id matches the current poses
     size_t    part_cap = 0, hist_cap = 0;
@@ -725,6 +734,73 @@ int redo_with_radix(gb_ctx* c)
     return broad_phase(c);
 }
 
+// The finer candidate grid (k_pair_count_fine): r_s is the bounding radius
+// that 95% of the particles do not exceed; the grid is used where that is
+// below 0.7 of the largest radius (a polydisperse packing), the rigid-body
+// ids are known on the host, and its cell count stays moderate.  The split
+// only decides which kernel tests a pair, never whether it is tested, so a
+// stale plan costs time, not results.
+int fine_plan(gb_ctx* c)
+{
+    c->fine_planned = true;
+    c->fine         = false;
+    const int n     = c->n;
+    if(n < 1024 || (int)c->h_rb_id.size() != n || c->props.empty())
+        return GB_OK;
+    std::vector<double> r(n);
+    for(int i = 0; i < n; ++i)
+        r[i] = c->props[c->h_rb_id[i]].circumscribed_radius;
+    std::vector<double> q(r);
+    const size_t k = (size_t)(0.95 * (n - 1));
+    std::nth_element(q.begin(), q.begin() + k, q.end());
+    const double rs = q[k];
+    if(!(rs > 0.0) || !(rs < 0.7 * c->rmax))
+        return GB_OK;
+    FineGrid g{};
+    g.rs = rs;
+    g.h  = 2.0 * rs * (1.0 + 1e-9);
+    uint64_t nf = 1;
+    uint32_t dim[3];
+    for(int a = 0; a < 3; ++a)
+    {
+        g.mn[a]      = c->cfg.origin[a];
+        const double e = std::ceil((c->lc_max[a] - c->cfg.origin[a]) / g.h);
+        if(!(e >= 1.0) || e > 4.0e9)
+            return GB_OK;
+        dim[a] = (uint32_t)e;
+        nf *= dim[a];
+    }
+    if(nf + 1 > kMaxCells || nf > 16ull * (uint64_t)n + 4096)
+        return GB_OK;
+    g.nx = dim[0], g.ny = dim[1], g.nz = dim[2];
+    uint32_t nlarge = 0;
+    for(int i = 0; i < n; ++i)
+        nlarge += r[i] > rs;
+    if(nf + 1 > c->fine_nf + 1 || !c->d_fcount)
+    {
+        dfree(c->d_fcount);
+        dfree(c->d_fstart);
+        GB_TRY(dalloc(&c->d_fcount, (size_t)nf + 1));
+        GB_TRY(dalloc(&c->d_fstart, (size_t)nf + 1));
+    }
+    if(!c->d_fkey)
+    {
+        GB_TRY(dalloc(&c->d_fkey, n));
+        GB_TRY(dalloc(&c->d_fskey, n));
+        GB_TRY(dalloc(&c->d_fids, n));
+        GB_TRY(dalloc(&c->d_fref, n));
+        GB_TRY(dalloc(&c->d_fpos, n));
+        GB_TRY(dalloc(&c->d_fpos32, n));
+    }
+    GB_CK(cudaMemsetAsync(c->d_fcount, 0, ((size_t)nf + 1) * sizeof(uint32_t), c->stream));
+    c->fcount_zero = true;
+    c->fine_g      = g;
+    c->fine_nf     = (uint32_t)nf;
+    c->fine_nlarge = nlarge;
+    c->fine        = true;
+    return GB_OK;
+}
+
 // candidate pairs (particles, then obstacles): count -> scan -> fill, with no
 // host round trip: the total stays on the device (off[n]); a total beyond the
 // capacity aborts the step (kFlagCapacity) and the host replays it larger
@@ -755,11 +831,52 @@ int build_pairs(gb_ctx* c)
         geo.mn[k] = c->cfg.origin[k];
     geo.cell = c->cell;
     geo.rmax = c->rmax;
-    GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_spos,
-                 spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], geo, c->d_count,
-                 c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob,
-                 (const int*)c->d_flags));
-    c->launches += 1;
+    if(!c->fine_planned)
+        GB_TRY(fine_plan(c));
+    if(c->fine)
+    {
+        // the finer grid of the small particles, then the count passes
+        const FineGrid& g   = c->fine_g;
+        float4*         f32 = c->prec == GB_MIXED ? c->d_fpos32 : nullptr;
+        if(!c->fcount_zero)
+            GB_CK(cudaMemsetAsync(c->d_fcount, 0, ((size_t)c->fine_nf + 1) * sizeof(uint32_t), s));
+        GB_CK(launch(c->pdl, k_fine_hash, nb, kBlock, s, n, (const double*)c->d_pos,
+                     (const double*)c->d_pos + n, (const double*)c->d_pos + 2 * (size_t)n,
+                     (const uint32_t*)c->d_rb_id, (const double*)c->d_rcirc64, g, c->d_fkey,
+                     c->d_fcount, (const int*)c->d_flags));
+        GB_TRY(scan_u32(c, c->d_fcount, c->d_fstart, (int64_t)c->fine_nf + 1, nullptr,
+                        c->d_flags));
+        GB_CK(launch(c->pdl, k_fine_scatter, nb, kBlock, s, n, (const uint32_t*)c->d_fkey,
+                     (const uint32_t*)c->d_fstart, c->d_fcount, (const double*)c->d_pos,
+                     (const double*)c->d_pos + n, (const double*)c->d_pos + 2 * (size_t)n,
+                     (const uint32_t*)c->d_rb_id, (const double*)c->d_rcirc64,
+                     (const uint32_t*)c->d_sorted_of, c->d_fskey, c->d_fids, c->d_fref, c->d_fpos,
+                     f32, (const int*)c->d_flags));
+        c->fcount_zero = true; // each particle took back the count it added
+        GB_CK(launch(c->pdl, k_pair_count_fine<S>, nb, kBlock, s, n,
+                     (const uint32_t*)c->d_fstart, g, (const uint32_t*)c->d_fskey,
+                     (const uint32_t*)c->d_fids, (const uint32_t*)c->d_fref,
+                     (const double4*)c->d_fpos, (const float4*)f32, c->d_count,
+                     c->d_count + n + 1, c->d_slot, (const uint32_t*)c->d_obsmask_id, c->nob,
+                     (const int*)c->d_flags));
+        const int nbl = std::max(1, blocks((int64_t)c->fine_nlarge * 32, kBlock));
+        GB_CK(launch(c->pdl, k_pair_count_large<S>, nbl, kBlock, s, n,
+                     (const uint32_t*)c->d_fstart, g, (const uint32_t*)c->d_fids,
+                     (const uint32_t*)c->d_fref, (const double4*)c->d_fpos, (const float4*)f32,
+                     (const uint32_t*)c->d_skeys, (const uint32_t*)c->d_sids,
+                     (const double4*)c->d_spos, spos32, (const uint32_t*)c->d_cstart, c->dims[0],
+                     c->dims[1], c->dims[2], c->d_count, c->d_count + n + 1, c->d_slot,
+                     (const uint32_t*)c->d_obsmask_id, c->nob, (const int*)c->d_flags));
+        c->launches += 4;
+    }
+    else
+    {
+        GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids,
+                     c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], geo,
+                     c->d_count, c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob,
+                     (const int*)c->d_flags));
+        c->launches += 1;
+    }
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));
     mark(c, 4);
@@ -1037,6 +1154,7 @@ void restore(gb_ctx* c, const StepSnap& s)
     c->steps_done     = s.steps_done;
     c->count_zero     = false; // an aborted fill pass may have left counts behind
     c->ccount_zero    = false; // ... and an aborted scatter pass cell counts
+    c->fcount_zero    = false; // ... or fine-cell counts
 }
 
 // Launches n_steps detects (PHASE_DETECT) or fused steps (PHASE_STEP) with no
@@ -1258,7 +1376,9 @@ int gb_destroy(gb_ctx* c)
                     c->d_off[0], c->d_off[1], c->d_pb[0], c->d_pb[1], c->d_pa, c->d_pf, c->d_pc,
                     c->d_info, c->d_xi[0], c->d_xi[1], c->d_flags, c->d_counters, c->d_done,
                     c->d_contacts,
-                    c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn};
+                    c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn,
+                    c->d_fkey, c->d_fcount, c->d_fstart, c->d_fskey, c->d_fids, c->d_fref,
+                    c->d_fpos, c->d_fpos32};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);
@@ -1322,6 +1442,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
     if(!c || !rbs || n_vertices < 0 || (n_vertices && !vertices))
         return GB_E_INVALID_ARG;
     c->rbs.assign(rbs, rbs + c->nrb);
+    c->fine_planned = false;
     c->verts.assign(vertices, vertices + 3 * n_vertices);
     c->props.resize(c->nrb);
     double rmax = 0.0;
@@ -1473,6 +1594,8 @@ int gb_set_rigid_body_ids(gb_ctx* c, const uint32_t* ids)
         if(ids[i] >= (uint32_t)c->nrb)
             return GB_E_INVALID_ARG;
     GB_CK(cudaMemcpy(c->d_rb_id, ids, c->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    c->h_rb_id.assign(ids, ids + c->n);
+    c->fine_planned = false;
     c->ids_set     = true;
     c->mask_valid  = false;
     c->rb_identity = c->nrb == c->n;
@@ -1961,7 +2084,12 @@ int gb_device_pointer(gb_ctx* c, const char* name, void** ptr)
             return *ptr = (char*)c->d_trq + k * n * ss, GB_OK;
     }
     if(s == "rb_id")
+    {
+        // written by the caller from now on: the host copy no longer holds
+        c->h_rb_id.clear();
+        c->fine_planned = false;
         return c->rb_identity = false, *ptr = c->d_rb_id, GB_OK;
+    }
     if(s == "rotation")
         return *ptr = c->d_rot, GB_OK;
     return GB_E_INVALID_ARG;

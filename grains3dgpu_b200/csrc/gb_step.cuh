@@ -506,6 +506,234 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
     }
 }
 
+// ---- candidate search on a finer grid (polydisperse packings) -----------------
+// The reference's cell is twice the LARGEST bounding radius, so in a
+// polydisperse packing a particle's 27 cells hold hundreds of others (~960 in
+// the 2.2 mm bed of 0.5-2 mm grains, 7.2 mm cells).  The same candidate set
+// is found with far fewer tests on a second grid of cell h >= 2 r_s, r_s a
+// bounding radius that most particles do not exceed ("small"; the others are
+// "large"):
+//   small-small pairs: |d| < rA + rB <= 2 r_s <= h, adjacent fine cells --
+//     the half stencil of k_pair_count on the fine grid (k_pair_count_fine);
+//   small-large pairs: the large particle scans the fine cells within its
+//     reach rL + r_s (k_pair_count_large, one warp per large particle);
+//   large-large pairs: the large particle scans its 27 reference cells for
+//     large partners after it in the reference's sorted order.
+// Each unordered pair is tested once, with the same symmetric test
+// (pretest_rejects + exact_hit), and recorded for both particles into the
+// same slots and counts (by reference sorted position and id) as
+// k_pair_count: the fill pass's sort restores the reference's order, so
+// the pair list is the same, bit for bit.  Large particles go to a bucket
+// past the fine cells (key nf), so the fine cells hold small ones only.
+struct FineGrid
+{
+    double   mn[3];
+    double   h;  // fine cell edge
+    double   rs; // the small particles' bounding-radius limit
+    uint32_t nx, ny, nz;
+};
+
+GB_D uint32_t fine_axis(double x, double mn, double h, uint32_t n)
+{
+    const double f = (x - mn) / h; // NaN falls to cell 0
+    return f >= 0.0 ? (f < (double)n ? (uint32_t)f : n - 1u) : 0u;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_fine_hash(int n, const double* __restrict__ px, const double* __restrict__ py,
+                const double* __restrict__ pz, const uint32_t* __restrict__ rb_id,
+                const double* __restrict__ rcirc, FineGrid g, uint32_t* __restrict__ fkey,
+                uint32_t* __restrict__ fcount, const int* abort_flags)
+{
+    grid_dep_sync();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n || step_aborted(abort_flags))
+        return;
+    uint32_t key = g.nx * g.ny * g.nz; // the large particles' bucket
+    if(!(rcirc[rb_id[i]] > g.rs))
+        key = (fine_axis(pz[i], g.mn[2], g.h, g.nz) * g.ny + fine_axis(py[i], g.mn[1], g.h, g.ny))
+                  * g.nx
+              + fine_axis(px[i], g.mn[0], g.h, g.nx);
+    fkey[i] = key;
+    atomicAdd(&fcount[key], 1u);
+}
+
+// each particle into a free slot of its fine cell (any order within a cell:
+// the fill pass sorts), with its key, id, reference sorted position and
+// positions (put_sorted); leaves the counts at zero
+__global__ void __launch_bounds__(kBlock)
+    k_fine_scatter(int n, const uint32_t* __restrict__ fkey, const uint32_t* __restrict__ fstart,
+                   uint32_t* __restrict__ fcount, const double* __restrict__ px,
+                   const double* __restrict__ py, const double* __restrict__ pz,
+                   const uint32_t* __restrict__ rb_id, const double* __restrict__ rcirc,
+                   const uint32_t* __restrict__ sorted_of, uint32_t* __restrict__ fskey,
+                   uint32_t* __restrict__ fids, uint32_t* __restrict__ fref,
+                   double4* __restrict__ fpos, float4* __restrict__ fpos32, const int* abort_flags)
+{
+    grid_dep_sync();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n || step_aborted(abort_flags))
+        return;
+    const uint32_t key  = fkey[i];
+    const uint32_t slot = fstart[key] + atomicSub(&fcount[key], 1u) - 1u;
+    fskey[slot]         = key;
+    fids[slot]          = (uint32_t)i;
+    fref[slot]          = sorted_of[i];
+    put_sorted(slot, (uint32_t)i, px, py, pz, rb_id, rcirc, fpos, fpos32);
+}
+
+// a hit between fine entries: both particles' slots and counts, by reference
+// sorted position and id, as k_pair_count records them
+GB_D void record_pair(uint32_t u, uint32_t id_u, uint32_t v, uint32_t id_v,
+                      uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
+                      uint32_t* __restrict__ slot)
+{
+    uint32_t k = atomicAdd(pslot + u, 1u);
+    if(k < kPairSlots)
+        slot[(size_t)u * kPairSlots + k] = v;
+    atomicAdd(count + id_u, 1u);
+    k = atomicAdd(pslot + v, 1u);
+    if(k < kPairSlots)
+        slot[(size_t)v * kPairSlots + k] = u;
+    atomicAdd(count + id_v, 1u);
+}
+
+// small particles: k_pair_count's half stencil on the fine grid (whose cells
+// hold small particles only); one thread per fine sorted position
+template <typename S>
+__global__ void __launch_bounds__(kBlock, 6)
+    k_pair_count_fine(int n, const uint32_t* __restrict__ fstart, FineGrid g,
+                      const uint32_t* __restrict__ fskey, const uint32_t* __restrict__ fids,
+                      const uint32_t* __restrict__ fref, const double4* __restrict__ fpos,
+                      const float4* __restrict__ fpos32, uint32_t* __restrict__ count,
+                      uint32_t* __restrict__ pslot, uint32_t* __restrict__ slot,
+                      const uint32_t* __restrict__ mask_by_id, int n_obs,
+                      const int* abort_flags)
+{
+    grid_dep_sync();
+    constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
+    const int      f      = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nx = g.nx, ny = g.ny, nz = g.nz;
+    if(f >= n || step_aborted(abort_flags) || (uint32_t)f >= fstart[nx * ny * nz])
+        return;
+    const uint32_t a = fids[f];
+    if(n_obs)
+    {
+        const int obs = obstacle_candidates(mask_by_id[a], n_obs);
+        if(obs)
+            atomicAdd(count + a, (uint32_t)obs);
+    }
+    const uint32_t key = fskey[f], sa = fref[f];
+    const double4  pa  = fpos[f];
+    float4         pa32;
+    if constexpr(PRE32)
+        pa32 = fpos32[f];
+    const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+    for(int r = 4; r < 9; ++r)
+    {
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        const int z = cz + dz, y = cy + dy;
+        if(z >= (int)nz || y < 0 || y >= (int)ny)
+            continue;
+        const bool     left = cx > 0, right = cx + 1 < (int)nx;
+        const uint32_t row  = ((uint32_t)z * ny + (uint32_t)y) * nx;
+        const uint32_t t0 = r == 4 ? (uint32_t)f + 1 : fstart[row + (uint32_t)(left ? cx - 1 : cx)];
+        const uint32_t t1 = fstart[row + (uint32_t)(right ? cx + 2 : cx + 1)];
+#pragma unroll 2
+        for(uint32_t t = t0; t < t1; ++t)
+        {
+            if constexpr(PRE32)
+                if(pretest_rejects<PRE32>(pa32, fpos32[t]))
+                    continue;
+            if(exact_hit<STRICT>(pa, fpos[t]))
+                record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
+        }
+    }
+}
+
+// large particles (the bucket past the fine cells), one warp each: small
+// partners from the fine cells within reach rL + r_s, large partners after it
+// in the reference's sorted order from its 27 reference cells
+template <typename S>
+__global__ void __launch_bounds__(kBlock)
+    k_pair_count_large(int n, const uint32_t* __restrict__ fstart, FineGrid g,
+                       const uint32_t* __restrict__ fids, const uint32_t* __restrict__ fref,
+                       const double4* __restrict__ fpos, const float4* __restrict__ fpos32,
+                       const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
+                       const double4* __restrict__ spos, const float4* __restrict__ spos32,
+                       const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny,
+                       uint32_t nz, uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
+                       uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
+                       int n_obs, const int* abort_flags)
+{
+    grid_dep_sync();
+    constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
+    const unsigned lane = threadIdx.x & 31u;
+    const int64_t  f = (int64_t)fstart[g.nx * g.ny * g.nz]
+                      + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    if(f >= n || step_aborted(abort_flags)) // warp-uniform
+        return;
+    const uint32_t a = fids[f], sa = fref[f];
+    if(n_obs && lane == 0)
+    {
+        const int obs = obstacle_candidates(mask_by_id[a], n_obs);
+        if(obs)
+            atomicAdd(count + a, (uint32_t)obs);
+    }
+    const double4 pa = fpos[f];
+    float4        pa32;
+    if constexpr(PRE32)
+        pa32 = fpos32[f];
+    // small partners: the fine cells of the box [x - reach, x + reach]
+    const double reach = (pa.w + g.rs) * (1.0 + 1e-6) + 1e-6 * g.h;
+    const uint32_t x0 = fine_axis(pa.x - reach, g.mn[0], g.h, g.nx);
+    const uint32_t x1 = fine_axis(pa.x + reach, g.mn[0], g.h, g.nx);
+    const uint32_t y0 = fine_axis(pa.y - reach, g.mn[1], g.h, g.ny);
+    const uint32_t y1 = fine_axis(pa.y + reach, g.mn[1], g.h, g.ny);
+    const uint32_t z0 = fine_axis(pa.z - reach, g.mn[2], g.h, g.nz);
+    const uint32_t z1 = fine_axis(pa.z + reach, g.mn[2], g.h, g.nz);
+    for(uint32_t z = z0; z <= z1; ++z)
+        for(uint32_t y = y0; y <= y1; ++y)
+        {
+            const uint32_t row = (z * g.ny + y) * g.nx;
+            const uint32_t t1  = fstart[row + x1 + 1];
+            for(uint32_t t = fstart[row + x0] + lane; t < t1; t += 32)
+            {
+                if constexpr(PRE32)
+                    if(pretest_rejects<PRE32>(pa32, fpos32[t]))
+                        continue;
+                if(exact_hit<STRICT>(pa, fpos[t]))
+                    record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
+            }
+        }
+    // large partners after it: the 27 reference cells (every pair within
+    // 2 x the largest radius), partners with a radius above r_s
+    const uint32_t key = skeys[sa];
+    const int      cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+    const double4  ps = spos[sa];
+    float4         ps32;
+    if constexpr(PRE32)
+        ps32 = spos32[sa];
+    for(int r = 0; r < 9; ++r)
+    {
+        uint32_t t0, t1;
+        neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
+        if(t0 < sa + 1)
+            t0 = sa + 1;
+        for(uint32_t t = t0 + lane; t < t1; t += 32)
+        {
+            const double4 pb = spos[t];
+            if(!(pb.w > g.rs))
+                continue;
+            if constexpr(PRE32)
+                if(pretest_rejects<PRE32>(ps32, spos32[t]))
+                    continue;
+            if(exact_hit<STRICT>(ps, pb))
+                record_pair(sa, a, t, sids[t], count, pslot, slot);
+        }
+    }
+}
+
 // Ascending sort of t[0, N) in registers by a bitonic network (Batcher, 1968):
 // every index is a compile-time constant once unrolled.
 template <int N, int M>
