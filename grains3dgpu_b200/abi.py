@@ -85,7 +85,8 @@ class Stats(C.Structure):
                 ("status_flags", C.c_int32), ("n_cells", C.c_int32),
                 ("cells_per_dir", C.c_int32 * 3), ("key_bits", C.c_int32),
                 ("cell_size", C.c_double), ("grid_max", C.c_double * 3),
-                ("kernel_launches", C.c_int64), ("gjk_fp64_calls", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("gjk_fp64_calls", C.c_int64),
+                ("fine_grid_cells", C.c_int64)]
 
 
 class Contact(C.Structure):

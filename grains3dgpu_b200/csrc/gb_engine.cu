@@ -184,6 +184,7 @@ struct gb_ctx
     unsigned long long  tickets      = 0;
     uint32_t            scan_epoch   = 0;
     uint32_t            scan_spin_limit = kScanSpinLimit; // GB_DEBUG_SCAN_SPIN_LIMIT
+    int                 fine_mode       = -1; // GB_DEBUG_FINE_GRID: 0 off, 1 on, -1 by crowding
 
     // pairs (double-buffered for the tangential history)
     uint32_t* d_count = nullptr;
@@ -740,12 +741,16 @@ int redo_with_radix(gb_ctx* c)
 // ids are known on the host, and its cell count stays moderate.  The split
 // only decides which kernel tests a pair, never whether it is tested, so a
 // stale plan costs time, not results.
+// the mean reference-cell occupancy seen by a particle above which the finer
+// grid pays for its extra passes (~27 x 8 = 216 candidates per particle)
+constexpr double kFineCrowding = 8.0;
+
 int fine_plan(gb_ctx* c)
 {
     c->fine_planned = true;
     c->fine         = false;
     const int n     = c->n;
-    if(n < 1024 || (int)c->h_rb_id.size() != n || c->props.empty())
+    if(c->fine_mode == 0 || n < 1024 || (int)c->h_rb_id.size() != n || c->props.empty())
         return GB_OK;
     std::vector<double> r(n);
     for(int i = 0; i < n; ++i)
@@ -757,8 +762,9 @@ int fine_plan(gb_ctx* c)
     if(!(rs > 0.0) || !(rs < 0.7 * c->rmax))
         return GB_OK;
     FineGrid g{};
-    g.rs = rs;
-    g.h  = 2.0 * rs * (1.0 + 1e-9);
+    g.rs   = rs;
+    g.rmax = c->rmax;
+    g.h    = 2.0 * rs * (1.0 + 1e-9);
     uint64_t nf = 1;
     uint32_t dim[3];
     for(int a = 0; a < 3; ++a)
@@ -770,18 +776,37 @@ int fine_plan(gb_ctx* c)
         dim[a] = (uint32_t)e;
         nf *= dim[a];
     }
-    if(nf + 1 > kMaxCells || nf > 16ull * (uint64_t)n + 4096)
+    if(2 * nf + 1 > kMaxCells || nf > 16ull * (uint64_t)n + 4096)
         return GB_OK;
     g.nx = dim[0], g.ny = dim[1], g.nz = dim[2];
+    if(c->fine_mode < 0)
+    {
+        // worth it where the reference cells are crowded: a particle shares
+        // its cell with sum(n_c^2) / n others on average (the cell starts of
+        // this step's sort, read once per plan)
+        std::vector<uint32_t> cs((size_t)c->ncells + 1);
+        GB_CK(cudaMemcpyAsync(cs.data(), c->d_cstart, cs.size() * sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, c->stream));
+        GB_CK(cudaStreamSynchronize(c->stream));
+        double sq = 0.0;
+        for(uint32_t k = 0; k < c->ncells; ++k)
+        {
+            const double m = cs[k + 1] >= cs[k] ? double(cs[k + 1] - cs[k]) : 0.0;
+            sq += m * m;
+        }
+        if(sq < kFineCrowding * (double)n)
+            return GB_OK;
+    }
     uint32_t nlarge = 0;
     for(int i = 0; i < n; ++i)
         nlarge += r[i] > rs;
-    if(nf + 1 > c->fine_nf + 1 || !c->d_fcount)
+    // keys: the small particles' fine cells, then the large particles' (+ nf)
+    if(nf > c->fine_nf || !c->d_fcount)
     {
         dfree(c->d_fcount);
         dfree(c->d_fstart);
-        GB_TRY(dalloc(&c->d_fcount, (size_t)nf + 1));
-        GB_TRY(dalloc(&c->d_fstart, (size_t)nf + 1));
+        GB_TRY(dalloc(&c->d_fcount, 2 * (size_t)nf + 1));
+        GB_TRY(dalloc(&c->d_fstart, 2 * (size_t)nf + 1));
     }
     if(!c->d_fkey)
     {
@@ -792,7 +817,7 @@ int fine_plan(gb_ctx* c)
         GB_TRY(dalloc(&c->d_fpos, n));
         GB_TRY(dalloc(&c->d_fpos32, n));
     }
-    GB_CK(cudaMemsetAsync(c->d_fcount, 0, ((size_t)nf + 1) * sizeof(uint32_t), c->stream));
+    GB_CK(cudaMemsetAsync(c->d_fcount, 0, (2 * (size_t)nf + 1) * sizeof(uint32_t), c->stream));
     c->fcount_zero = true;
     c->fine_g      = g;
     c->fine_nf     = (uint32_t)nf;
@@ -839,12 +864,13 @@ int build_pairs(gb_ctx* c)
         const FineGrid& g   = c->fine_g;
         float4*         f32 = c->prec == GB_MIXED ? c->d_fpos32 : nullptr;
         if(!c->fcount_zero)
-            GB_CK(cudaMemsetAsync(c->d_fcount, 0, ((size_t)c->fine_nf + 1) * sizeof(uint32_t), s));
+            GB_CK(cudaMemsetAsync(c->d_fcount, 0, (2 * (size_t)c->fine_nf + 1) * sizeof(uint32_t),
+                                  s));
         GB_CK(launch(c->pdl, k_fine_hash, nb, kBlock, s, n, (const double*)c->d_pos,
                      (const double*)c->d_pos + n, (const double*)c->d_pos + 2 * (size_t)n,
                      (const uint32_t*)c->d_rb_id, (const double*)c->d_rcirc64, g, c->d_fkey,
                      c->d_fcount, (const int*)c->d_flags));
-        GB_TRY(scan_u32(c, c->d_fcount, c->d_fstart, (int64_t)c->fine_nf + 1, nullptr,
+        GB_TRY(scan_u32(c, c->d_fcount, c->d_fstart, 2 * (int64_t)c->fine_nf + 1, nullptr,
                         c->d_flags));
         GB_CK(launch(c->pdl, k_fine_scatter, nb, kBlock, s, n, (const uint32_t*)c->d_fkey,
                      (const uint32_t*)c->d_fstart, c->d_fcount, (const double*)c->d_pos,
@@ -863,10 +889,8 @@ int build_pairs(gb_ctx* c)
         GB_CK(launch(c->pdl, k_pair_count_large<S>, nbl, kBlock, s, n,
                      (const uint32_t*)c->d_fstart, g, (const uint32_t*)c->d_fids,
                      (const uint32_t*)c->d_fref, (const double4*)c->d_fpos, (const float4*)f32,
-                     (const uint32_t*)c->d_skeys, (const uint32_t*)c->d_sids,
-                     (const double4*)c->d_spos, spos32, (const uint32_t*)c->d_cstart, c->dims[0],
-                     c->dims[1], c->dims[2], c->d_count, c->d_count + n + 1, c->d_slot,
-                     (const uint32_t*)c->d_obsmask_id, c->nob, (const int*)c->d_flags));
+                     c->d_count, c->d_count + n + 1, c->d_slot, (const uint32_t*)c->d_obsmask_id,
+                     c->nob, (const int*)c->d_flags));
         c->launches += 4;
     }
     else
@@ -1321,6 +1345,10 @@ gb_ctx* gb_create(const gb_config* cfg, int* status)
     // run out, which a step reports as GB_E_CUDA with the state untouched
     if(const char* lim = std::getenv("GB_DEBUG_SCAN_SPIN_LIMIT"))
         c->scan_spin_limit = (uint32_t)std::strtoul(lim, nullptr, 10);
+    // test knob: the finer candidate grid off (0) or on wherever it applies
+    // (1) instead of where the reference cells are crowded
+    if(const char* fg = std::getenv("GB_DEBUG_FINE_GRID"))
+        c->fine_mode = std::atoi(fg) ? 1 : 0;
     c->prec   = cfg->precision;
     c->n      = cfg->n_particles;
     c->nrb    = cfg->n_rigid_bodies;
@@ -1903,6 +1931,7 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
         const bool stage32 = c->prec == GB_MIXED && c->cfg.gjk_variant == GB_GJK_JH;
         o->gjk_calls       = c->detect_valid ? (int64_t)q[0] : 0;
         o->gjk_fp64_calls  = c->detect_valid ? (int64_t)q[stage32 ? 1 : 0] : 0;
+        o->fine_grid_cells = c->fine ? (int64_t)c->fine_nf : 0;
     }
     if(c->detect_valid && c->npairs > 0)
     {
@@ -1912,14 +1941,16 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
         GB_CK(cudaMemcpy(pc.data(), c->d_pc, c->npairs, cudaMemcpyDeviceToHost));
         GB_CK(cudaMemcpy(pb.data(), c->d_pb[c->cur], c->npairs * sizeof(uint32_t),
                          cudaMemcpyDeviceToHost));
-        int64_t k = 0, obs = 0;
+        int64_t k = 0, obs = 0, ko = 0;
         for(int64_t p = 0; p < c->npairs; ++p)
         {
             k += pc[p] == kContactParticle;
+            ko += pc[p] == kContactObstacle;
             obs += (pb[p] & kObstacleBit) != 0;
         }
-        o->contacts        = k;
-        o->candidate_pairs = c->npairs - obs;
+        o->contacts          = k;
+        o->obstacle_contacts = ko; // of the last step, as the particle contacts
+        o->candidate_pairs   = c->npairs - obs;
     }
     o->status_flags = c->last.status_flags;
     o->n_cells      = (int32_t)c->ncells;

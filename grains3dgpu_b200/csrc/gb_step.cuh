@@ -517,19 +517,21 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
 //     the half stencil of k_pair_count on the fine grid (k_pair_count_fine);
 //   small-large pairs: the large particle scans the fine cells within its
 //     reach rL + r_s (k_pair_count_large, one warp per large particle);
-//   large-large pairs: the large particle scans its 27 reference cells for
-//     large partners after it in the reference's sorted order.
+//   large-large pairs: the large particle scans the fine cells within its
+//     reach rL + r_max for large partners after it in the fine order.
 // Each unordered pair is tested once, with the same symmetric test
 // (pretest_rejects + exact_hit), and recorded for both particles into the
 // same slots and counts (by reference sorted position and id) as
 // k_pair_count: the fill pass's sort restores the reference's order, so
-// the pair list is the same, bit for bit.  Large particles go to a bucket
-// past the fine cells (key nf), so the fine cells hold small ones only.
+// the pair list is the same, bit for bit.  A large particle's key is its
+// fine cell plus nf (the fine cell count): the fine order holds the small
+// particles by cell, then the large ones by cell.
 struct FineGrid
 {
     double   mn[3];
-    double   h;  // fine cell edge
-    double   rs; // the small particles' bounding-radius limit
+    double   h;    // fine cell edge
+    double   rs;   // the small particles' bounding-radius limit
+    double   rmax; // the largest bounding radius
     uint32_t nx, ny, nz;
 };
 
@@ -549,11 +551,11 @@ __global__ void __launch_bounds__(kBlock)
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n || step_aborted(abort_flags))
         return;
-    uint32_t key = g.nx * g.ny * g.nz; // the large particles' bucket
-    if(!(rcirc[rb_id[i]] > g.rs))
-        key = (fine_axis(pz[i], g.mn[2], g.h, g.nz) * g.ny + fine_axis(py[i], g.mn[1], g.h, g.ny))
-                  * g.nx
-              + fine_axis(px[i], g.mn[0], g.h, g.nx);
+    uint32_t key = (fine_axis(pz[i], g.mn[2], g.h, g.nz) * g.ny + fine_axis(py[i], g.mn[1], g.h, g.ny))
+                       * g.nx
+                   + fine_axis(px[i], g.mn[0], g.h, g.nx);
+    if(rcirc[rb_id[i]] > g.rs)
+        key += g.nx * g.ny * g.nz; // the large particles' cells
     fkey[i] = key;
     atomicAdd(&fcount[key], 1u);
 }
@@ -651,26 +653,23 @@ __global__ void __launch_bounds__(kBlock, 6)
     }
 }
 
-// large particles (the bucket past the fine cells), one warp each: small
-// partners from the fine cells within reach rL + r_s, large partners after it
-// in the reference's sorted order from its 27 reference cells
+// large particles (keys past the small ones'), one warp each: small partners
+// from the fine cells within reach rL + r_s, then large partners after it in
+// the fine order from the large particles' cells within reach rL + r_max
 template <typename S>
 __global__ void __launch_bounds__(kBlock)
     k_pair_count_large(int n, const uint32_t* __restrict__ fstart, FineGrid g,
                        const uint32_t* __restrict__ fids, const uint32_t* __restrict__ fref,
                        const double4* __restrict__ fpos, const float4* __restrict__ fpos32,
-                       const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ sids,
-                       const double4* __restrict__ spos, const float4* __restrict__ spos32,
-                       const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny,
-                       uint32_t nz, uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
+                       uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
                        uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
                        int n_obs, const int* abort_flags)
 {
     grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
     const unsigned lane = threadIdx.x & 31u;
-    const int64_t  f = (int64_t)fstart[g.nx * g.ny * g.nz]
-                      + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint32_t nf   = g.nx * g.ny * g.nz;
+    const int64_t  f    = (int64_t)fstart[nf] + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     if(f >= n || step_aborted(abort_flags)) // warp-uniform
         return;
     const uint32_t a = fids[f], sa = fref[f];
@@ -684,53 +683,34 @@ __global__ void __launch_bounds__(kBlock)
     float4        pa32;
     if constexpr(PRE32)
         pa32 = fpos32[f];
-    // small partners: the fine cells of the box [x - reach, x + reach]
-    const double reach = (pa.w + g.rs) * (1.0 + 1e-6) + 1e-6 * g.h;
-    const uint32_t x0 = fine_axis(pa.x - reach, g.mn[0], g.h, g.nx);
-    const uint32_t x1 = fine_axis(pa.x + reach, g.mn[0], g.h, g.nx);
-    const uint32_t y0 = fine_axis(pa.y - reach, g.mn[1], g.h, g.ny);
-    const uint32_t y1 = fine_axis(pa.y + reach, g.mn[1], g.h, g.ny);
-    const uint32_t z0 = fine_axis(pa.z - reach, g.mn[2], g.h, g.nz);
-    const uint32_t z1 = fine_axis(pa.z + reach, g.mn[2], g.h, g.nz);
-    for(uint32_t z = z0; z <= z1; ++z)
-        for(uint32_t y = y0; y <= y1; ++y)
-        {
-            const uint32_t row = (z * g.ny + y) * g.nx;
-            const uint32_t t1  = fstart[row + x1 + 1];
-            for(uint32_t t = fstart[row + x0] + lane; t < t1; t += 32)
-            {
-                if constexpr(PRE32)
-                    if(pretest_rejects<PRE32>(pa32, fpos32[t]))
-                        continue;
-                if(exact_hit<STRICT>(pa, fpos[t]))
-                    record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
-            }
-        }
-    // large partners after it: the 27 reference cells (every pair within
-    // 2 x the largest radius), partners with a radius above r_s
-    const uint32_t key = skeys[sa];
-    const int      cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
-    const double4  ps = spos[sa];
-    float4         ps32;
-    if constexpr(PRE32)
-        ps32 = spos32[sa];
-    for(int r = 0; r < 9; ++r)
+    for(int large = 0; large < 2; ++large)
     {
-        uint32_t t0, t1;
-        neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
-        if(t0 < sa + 1)
-            t0 = sa + 1;
-        for(uint32_t t = t0 + lane; t < t1; t += 32)
-        {
-            const double4 pb = spos[t];
-            if(!(pb.w > g.rs))
-                continue;
-            if constexpr(PRE32)
-                if(pretest_rejects<PRE32>(ps32, spos32[t]))
-                    continue;
-            if(exact_hit<STRICT>(ps, pb))
-                record_pair(sa, a, t, sids[t], count, pslot, slot);
-        }
+        // the fine cells of the box [x - reach, x + reach]
+        const double   reach = (pa.w + (large ? g.rmax : g.rs)) * (1.0 + 1e-6) + 1e-6 * g.h;
+        const uint32_t base  = large ? nf : 0u;
+        const uint32_t x0    = fine_axis(pa.x - reach, g.mn[0], g.h, g.nx);
+        const uint32_t x1    = fine_axis(pa.x + reach, g.mn[0], g.h, g.nx);
+        const uint32_t y0    = fine_axis(pa.y - reach, g.mn[1], g.h, g.ny);
+        const uint32_t y1    = fine_axis(pa.y + reach, g.mn[1], g.h, g.ny);
+        const uint32_t z0    = fine_axis(pa.z - reach, g.mn[2], g.h, g.nz);
+        const uint32_t z1    = fine_axis(pa.z + reach, g.mn[2], g.h, g.nz);
+        for(uint32_t z = z0; z <= z1; ++z)
+            for(uint32_t y = y0; y <= y1; ++y)
+            {
+                const uint32_t row = base + (z * g.ny + y) * g.nx;
+                uint32_t       t0  = fstart[row + x0];
+                const uint32_t t1  = fstart[row + x1 + 1];
+                if(large && t0 < (uint32_t)f + 1)
+                    t0 = (uint32_t)f + 1; // each large pair once
+                for(uint32_t t = t0 + lane; t < t1; t += 32)
+                {
+                    if constexpr(PRE32)
+                        if(pretest_rejects<PRE32>(pa32, fpos32[t]))
+                            continue;
+                    if(exact_hit<STRICT>(pa, fpos[t]))
+                        record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
+                }
+            }
     }
 }
 

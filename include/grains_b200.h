@@ -167,7 +167,7 @@ typedef struct gb_stats {
     int64_t obstacle_contacts;
     int64_t gjk_calls;        /* particle pairs past the bounding tests and GJK's first
                                  iteration (queued for the GJK pass)           */
-    int64_t gjk_iterations;
+    int64_t gjk_iterations;   /* summed over the steps of the last gb_step call */
     int32_t status_flags; /* bit i set: device-side error (1 << -GB_E_x)    */
     int32_t n_cells;
     int32_t cells_per_dir[3];
@@ -177,6 +177,8 @@ typedef struct gb_stats {
     int64_t kernel_launches; /* kernels launched by this context so far */
     int64_t gjk_fp64_calls;  /* particle pairs solved by the FP64 GJK (GB_MIXED: those its
                                 FP32 stage leaves open; otherwise gjk_calls) */
+    int64_t fine_grid_cells; /* cells of the finer candidate grid of a polydisperse packing
+                                (0: candidates from the linked cells alone) */
 } gb_stats;
 
 /* ---- debug dump kinds -------------------------------------------------------- */

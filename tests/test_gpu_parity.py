@@ -112,6 +112,39 @@ def test_broad_phase_and_pairs_bit_exact_polyhedra_200k(gb, oracle):
     o.close()
 
 
+@pytest.mark.parametrize("workload,knob", [("bed", None), ("dilute", "1"), ("bed", "0")])
+def test_fine_grid_pairs_bit_exact(gb, oracle, monkeypatch, workload, knob):
+    """Candidates of a polydisperse packing on the finer grid (cell twice the
+    95th-percentile bounding radius; the largest 5 % of grains by warp): the
+    dense bed of the headline workload (200,000 of its grains on the 2.2 mm
+    lattice) takes it by itself, the dilute packing when forced, and the bed
+    can be held to the linked cells alone.  Either way the cell starts,
+    candidate and contact pairs equal the oracle's, in both FP64-strict and
+    mixed precision."""
+    if knob is not None:
+        monkeypatch.setenv("GB_DEBUG_FINE_GRID", knob)
+    # the bed on its 2.2 mm lattice; the dilute packing at the 1,000,000-grain
+    # workload's spacing (a fifth of its box)
+    kw = {"pitch": 2.2e-3} if workload == "bed" else {"box": (0.3, 0.3, 0.24)}
+    scene = scenes.polydisperse_superquadrics(seed=5, n=200_000, **kw)
+    systems = [scenes.System(gb, scene, precision=p) for p in (abi.GB_FP64_STRICT, abi.GB_MIXED)]
+    o = scenes.System(oracle, scene)
+    share_props(systems[0], o, oracle)
+    o.detect()
+    dumps = [abi.GB_DUMP_CELL_START, abi.GB_DUMP_CANDIDATE_PAIRS, abi.GB_DUMP_CONTACT_PAIRS]
+    want = {k: o.dump(k) for k in dumps}
+    assert want[abi.GB_DUMP_CANDIDATE_PAIRS].shape[0] > (100_000 if workload == "bed" else 100)
+    for g in systems:
+        g.detect()
+        fine = g.stats().fine_grid_cells
+        assert (fine > 0) == (knob != "0"), fine
+        for kind_, b in want.items():
+            a = g.dump(kind_)
+            assert a.shape == b.shape and np.array_equal(a, b), f"dump {kind_} differs"
+        g.close()
+    o.close()
+
+
 @pytest.mark.parametrize("kind", ["sphere", "box-on-walls", "polyhedron"])
 def test_single_step_torce_bit_exact(gb, oracle, kind):
     scene = make_scene(kind)
