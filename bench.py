@@ -146,12 +146,12 @@ def max_over_ranks(value, torch, world, device):
 
 
 # ---------------------------------------------------------------------------
-def run_engine(args, scene, precision, steps, warmup, torch, rank, world, timing=True):
+def run_engine(args, scene, precision, steps, warmup, torch, rank, world, timing=True, **cfg):
     from grains3dgpu_b200 import engine
     lib = engine.load()
-    flags = abi.GB_FLAG_PHASE_TIMING if timing else 0
+    flags = (abi.GB_FLAG_PHASE_TIMING if timing else 0) | cfg.pop("flags", 0)
     sysm = scenes.System(lib, scene, precision=precision, device=torch.cuda.current_device(),
-                         flags=flags, contact_law=LAW)
+                         flags=flags, contact_law=LAW, **cfg)
     stream = torch.cuda.current_stream()
     assert lib.set_stream(sysm.ctx, abi.C.c_void_p(stream.cuda_stream)) == 0
     for _ in range(warmup):
@@ -306,17 +306,25 @@ def measure_drum(args, torch):
     of radius 0.1 m turning at 30 rpm, its length scaled for the grains to
     fill 40% of it, the tangential-history law, grain-wall friction 0.6:
     `drum_steps` mixed steps in one gb_step call, and a shorter FP64 run of
-    the same drum for the ratio."""
+    the same drum for the ratio.  Two choices of the run keep it finite and
+    its contacts real: the signed-volume GJK (the reference's GJK-JH, with its
+    absolute determinant threshold, misses most contacts of mm grains) and
+    GB_FLAG_CRUST_BOUNDS (the reference's OBB pre-filter lets two cubes reach
+    GJK only once they intersect, where the contact normal is 0/0: the state
+    turns non-finite at the first cube-cube collision)."""
     scene = scenes.rotating_drum(n=args.drum_n, margin=1.7e-3, v_sigma=0.1)
+    cfg = dict(gjk_variant=abi.GB_GJK_SV, flags=abi.GB_FLAG_CRUST_BOUNDS)
     out = {"workload": f"{scene.n:,} grains (40% spheres r=1 mm, 30% cubes 1.6 mm as "
                        "polyhedra, 30% superquadrics n=6 1x1x0.7 mm) in a drum of radius "
                        f"0.1 m turning at 30 rpm, {scene.notes}, wall mu 0.6, dt 1e-6 s; "
                        "initial velocities N(0, 0.1 m/s) per component so that neighbours "
-                       "0.13 mm apart on the lattice collide within the run",
+                       "0.13 mm apart on the lattice collide within the run; signed-volume "
+                       "GJK, crust-inclusive bounding tests (GB_FLAG_CRUST_BOUNDS)",
            "n_particles": scene.n}
     for prec, key, k in ((abi.GB_MIXED, "mixed", args.drum_steps),
                          (abi.GB_FP64, "fp64", max(1, args.drum_steps // 10))):
-        s, el, _, _, _, st = run_engine(args, scene, prec, k, 3, torch, 0, 1, timing=False)
+        s, el, _, _, _, st = run_engine(args, scene, prec, k, 3, torch, 0, 1, timing=False,
+                                        **dict(cfg))
         tr = s.transforms()
         out[key] = {"steps": k, "value": scene.n * k / el, "ms_per_step": el / k * 1e3,
                     "contacts_last_step": int(st.contacts),

@@ -26,6 +26,7 @@ GB_MAX_POLY_VERTICES = 64
 GB_FP64, GB_MIXED, GB_FP64_STRICT = 0, 1, 2
 GB_FLAG_RECORD_CONTACT_INFO = 1
 GB_FLAG_PHASE_TIMING = 2
+GB_FLAG_CRUST_BOUNDS = 4
 GB_RAW_COORDINATION_NUMBER = 1
 PHASES = ["hash", "sort", "cell_start", "pair_count", "pair_fill", "narrow", "particle"]
 GB_N_PHASES = len(PHASES)

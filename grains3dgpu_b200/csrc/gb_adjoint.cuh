@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kBlock)
                                 const_cast<double*>(lft) + 4 * (size_t)n,
                                 const_cast<double*>(lft) + 5 * (size_t)n};
         const uint32_t   ri = st.rb_id[i];
-        const double     r_i = shape[ri].rcirc, m_i = in[ri].mass;
+        const double     r_i = shape[ri].p[0], m_i = in[ri].mass; // the sphere's radius
         const int        mat_i = shape[ri].material;
         const V3<double> xi = ld3(st.pos, i), vi = ld3(st.vel, i), wi = ld3(st.omg, i);
         const V3<double> lfi = ld3(lf_, i), lti = ld3(lt_, i);
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(kBlock)
                 continue;
             }
             const uint32_t   rj = st.rb_id[b];
-            const double     r_j = shape[rj].rcirc, m_j = in[rj].mass;
+            const double     r_j = shape[rj].p[0], m_j = in[rj].mass;
             const int        l   = adj_law_index(mat_i, shape[rj].material);
             const double     avm = m_i * m_j / (m_i + m_j);
             const V3<double> xj = ld3(st.pos, b), vj = ld3(st.vel, b), wj = ld3(st.omg, b);

@@ -35,18 +35,19 @@ GB_D Contact<S> no_contact()
 // working coordinates (xA, xB absolute; or 0, xB-xA relative); d = xB - xA.
 // VAR selects the GJK (GB_GJK_JH, the reference's choice, or GB_GJK_SV /
 // GB_GJK_NESTEROV).
-// closestPointsSpheres (CollisionDetection.cpp:26-48)
+// closestPointsSpheres (CollisionDetection.cpp:26-48); a sphere's radius is
+// its circumscribed radius, p[0] (the table's rcirc may include the crust)
 template <typename S>
 GB_D Contact<S> closest_spheres(const Body<S>& A, const Body<S>& B, const V3<S>& oA,
                                 const V3<S>& oB)
 {
     V3<S>   vba     = oB - oA;
-    const S overlap = norm(vba) - A.rcirc - B.rcirc;
+    const S overlap = norm(vba) - A.p[0] - B.p[0];
     vba             = vba / norm(vba);
     if(overlap < S(0.0))
     {
         Contact<S> c;
-        c.pt      = oA + (A.rcirc + S(0.5) * overlap) * vba;
+        c.pt      = oA + (A.p[0] + S(0.5) * overlap) * vba;
         c.vec     = overlap * vba;
         c.overlap = overlap;
         return c;

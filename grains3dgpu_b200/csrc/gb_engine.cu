@@ -325,9 +325,20 @@ Tables<S> tables_of(gb_ctx* c)
     return t;
 }
 
-template <typename St>
-RBShape<St> shape_record(const gb_rigid_body_desc& d, const gb_rigid_body_props& p)
+bool crust_bounds(const gb_ctx* c) { return (c->cfg.flags & GB_FLAG_CRUST_BOUNDS) != 0; }
+
+// the bounding radius of rigid body i in the candidate test and the cell size
+double bound_radius(const gb_ctx* c, int i)
 {
+    return c->props[i].circumscribed_radius + (crust_bounds(c) ? c->rbs[i].crust_thickness : 0.0);
+}
+
+template <typename St>
+RBShape<St> shape_record(const gb_rigid_body_desc& d, const gb_rigid_body_props& p,
+                         bool crust_bounds)
+{
+    // the bounding tests' radius and half-extents (GB_FLAG_CRUST_BOUNDS)
+    const double grow = crust_bounds ? d.crust_thickness : 0.0;
     RBShape<St> r;
     std::memset(&r, 0, sizeof(r));
     r.type       = d.convex.type;
@@ -349,9 +360,9 @@ RBShape<St> shape_record(const gb_rigid_body_desc& d, const gb_rigid_body_props&
         r.k[7] = (St)(1.0 / n1);
     }
     r.crust    = (St)d.crust_thickness;
-    r.rcirc    = (St)p.circumscribed_radius;
+    r.rcirc    = (St)(p.circumscribed_radius + grow);
     for(int k = 0; k < 3; ++k)
-        r.bb[k] = (St)p.bounding_box[k];
+        r.bb[k] = (St)(p.bounding_box[k] + grow);
     r.material = d.material;
     return r;
 }
@@ -364,7 +375,7 @@ int upload_tables(gb_ctx* c)
     std::vector<double>        rc(c->nrb);
     for(int i = 0; i < c->nrb; ++i)
     {
-        sh[i] = shape_record<St>(c->rbs[i], c->props[i]);
+        sh[i] = shape_record<St>(c->rbs[i], c->props[i], crust_bounds(c));
         std::memset(&in[i], 0, sizeof(in[i]));
         in[i].mass = (St)c->props[i].mass;
         for(int k = 0; k < 6; ++k)
@@ -374,7 +385,7 @@ int upload_tables(gb_ctx* c)
         }
         for(int k = 0; k < 3; ++k)
             in[i].bb[k] = sh[i].bb[k];
-        rc[i] = c->props[i].circumscribed_radius;
+        rc[i] = bound_radius(c, i);
     }
     const size_t nv = c->verts.size() / 3;
     std::vector<Vert<St>> vv(std::max<size_t>(nv, 1));
@@ -428,7 +439,7 @@ int upload_obstacles(gb_ctx* c)
     std::vector<double>      mass(std::max(c->nob, 1), 0.0);
     for(int i = 0; i < c->nob; ++i)
     {
-        sh[i]   = shape_record<St>(c->obs[i], c->obs_props[i]);
+        sh[i]   = shape_record<St>(c->obs[i], c->obs_props[i], crust_bounds(c));
         mass[i] = c->obs_props[i].mass;
     }
     dfree(c->d_obs_shape);
@@ -754,7 +765,7 @@ int fine_plan(gb_ctx* c)
         return GB_OK;
     std::vector<double> r(n);
     for(int i = 0; i < n; ++i)
-        r[i] = c->props[c->h_rb_id[i]].circumscribed_radius;
+        r[i] = bound_radius(c, c->h_rb_id[i]);
     std::vector<double> q(r);
     const size_t k = (size_t)(0.95 * (n - 1));
     std::nth_element(q.begin(), q.begin() + k, q.end());
@@ -1485,7 +1496,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
         if(rbs[i].material < 0 || rbs[i].material >= c->nmat)
             return GB_E_INVALID_ARG;
         GB_TRY(gb_rigid_body_properties(&rbs[i], vertices, &c->props[i]));
-        rmax = std::max(rmax, c->props[i].circumscribed_radius); // Grains.cpp:226-231
+        rmax = std::max(rmax, bound_radius(c, i)); // Grains.cpp:226-231
     }
     // linked cell: cell = factor * 2 * max circumscribed radius (Grains.cpp:233-246)
     double coeff = c->cfg.cell_size_factor;

@@ -90,7 +90,7 @@ GB_D Contact<float> closest_spheres_mixed(const Tables<float>& tb, uint32_t ra, 
                                           const double xa[3], const double xb[3])
 {
     const V3<double> d64 = mk<double>(xb[0] - xa[0], xb[1] - xa[1], xb[2] - xa[2]);
-    const double     rA = tb.shape64[ra].rcirc, rB = tb.shape64[rb].rcirc;
+    const double     rA = tb.shape64[ra].p[0], rB = tb.shape64[rb].p[0]; // the radii
     const double     nd = norm(d64), overlap = nd - rA - rB;
     if(!(overlap < 0.0))
         return no_contact<float>();

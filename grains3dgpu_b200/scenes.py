@@ -363,6 +363,44 @@ def sphere_bed(seed=1, n=60, box=(0.009, 0.009, 0.016), pitch=2.05e-3, sink=0.55
     return scene
 
 
+def cube_collision(seed=6, speed=0.4, gap=0.1e-3, tilt=0.1, shape="polyhedron"):
+    """Two cubes of the drum's kind (edge 1.6 mm, crust 0.04 mm, density 2500;
+    convex polyhedra of 8 vertices, or boxes) meeting head on along x at a
+    relative speed `speed`, their faces `gap` apart at the start, each turned
+    by random angles up to `tilt` rad; no gravity, no walls.  The cube's
+    bounding box is the cube, so the reference's OBB pre-filter passes the
+    pair only once the cubes intersect (GB_FLAG_CRUST_BOUNDS)."""
+    rng = np.random.default_rng(seed)
+    rbs = np.zeros(1, RB_DTYPE)
+    rbs["density"] = 2500.0
+    rbs[0]["crust"] = 0.04e-3
+    h = 0.8e-3
+    if shape == "polyhedron":
+        rbs[0]["type"] = abi.GB_POLYHEDRON
+        rbs[0]["n_vertices"] = 8
+        verts = np.array([[sx * h, sy * h, sz * h] for sx in (-1, 1) for sy in (-1, 1)
+                          for sz in (-1, 1)], float)
+    else:
+        rbs[0]["type"] = abi.GB_BOX
+        rbs[0]["p"][:3] = h
+        verts = np.zeros((0, 3))
+    q = np.concatenate([np.ones((2, 1)), rng.uniform(-0.5 * tilt, 0.5 * tilt, (2, 3))], 1)
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    tr = np.zeros((2, 12))
+    tr[:, :9] = quat_to_matrix(q)
+    c = np.array([0.01, 0.01, 0.01])
+    tr[0, 9:] = c - [h + 0.5 * gap, 0, 0]
+    tr[1, 9:] = c + [h + 0.5 * gap, 0, 0]
+    vel = np.zeros((2, 6))
+    vel[0, 0], vel[1, 0] = 0.5 * speed, -0.5 * speed
+    cfg = dict(n_particles=2, n_rigid_bodies=1, n_obstacles=0, n_materials=1,
+               origin=(0, 0, 0), max_coordinate=(0.02, 0.02, 0.02), dt=1e-6,
+               gravity=(0, 0, 0))
+    return Scene("cube_collision", cfg, rbs, verts, np.zeros(2, np.uint32), tr, vel,
+                 np.zeros(0, RB_DTYPE), np.zeros((0, 12)), [law()],
+                 notes=f"relative speed {speed} m/s, gap {gap * 1e3} mm")
+
+
 def drum_obstacles(radius, length, centre, material=1):
     """A drum about the world y axis through `centre`: the cylindrical wall
     (GB_DRUM, radius, half-length; frame z = world y) and the two end caps

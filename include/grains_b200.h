@@ -148,6 +148,16 @@ typedef struct gb_config {
 /* gb_config.flags */
 #define GB_FLAG_RECORD_CONTACT_INFO 1 /* keep per-pair contact info for dumps   */
 #define GB_FLAG_PHASE_TIMING 2        /* CUDA-event timing of each step phase */
+/* Bounding tests that include the crust: the circumscribed radius and the
+ * bounding box's half-extents of every rigid body grow by its crust thickness
+ * in the candidate test, the linked-cell size and the OBB pre-filter.  Off
+ * (the reference's rule), those bound the shapes alone while a contact starts
+ * once the shapes come within the crusts' sum, so a body whose box is tight
+ * (a cube as a box or polyhedron) first reaches the closest-point solver
+ * when it already intersects its neighbour, where the contact normal is 0/0
+ * (CollisionDetection.cpp:208-245).  The sphere-sphere closed form keeps the
+ * radius. */
+#define GB_FLAG_CRUST_BOUNDS 4
 
 /* Step phases timed under GB_FLAG_PHASE_TIMING (gb_get_phase_times). */
 #define GB_PHASE_HASH 0       /* cell hash per particle                       */

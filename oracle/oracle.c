@@ -1291,8 +1291,9 @@ static void no_contact(or_contact* o)
 static void closest_spheres(const body_view* A, const body_view* B,
                             const double a2w[12], const double b2w[12], or_contact* o)
 {
-    /* closestPointsSpheres (CollisionDetection.cpp:26-48) */
-    const double rA = A->rcirc, rB = B->rcirc;
+    /* closestPointsSpheres (CollisionDetection.cpp:26-48); a sphere's radius
+       is its circumscribed radius, p[0] (rcirc may include the crust) */
+    const double rA = A->cv->p[0], rB = B->cv->p[0];
     double       cen[3], vba[3];
     copy3(a2w + 9, cen);
     sub3(b2w + 9, cen, vba);
@@ -1438,14 +1439,18 @@ static void closest_points(const body_view* A, const body_view* B,
     no_contact(o);
 }
 
+/* crust_bounds (GB_FLAG_CRUST_BOUNDS): the bounding tests' radius and
+   half-extents grow by the crust thickness */
 static void view_of(body_view* v, const gb_rigid_body_desc* rb,
-                    const gb_rigid_body_props* pr, const double* verts)
+                    const gb_rigid_body_props* pr, const double* verts, int crust_bounds)
 {
+    const double grow = crust_bounds ? rb->crust_thickness : 0.0;
     v->cv    = &rb->convex;
     v->verts = verts;
     v->crust = rb->crust_thickness;
-    v->rcirc = pr->circumscribed_radius;
-    copy3(pr->bounding_box, v->bb);
+    v->rcirc = pr->circumscribed_radius + grow;
+    for(int k = 0; k < 3; ++k)
+        v->bb[k] = pr->bounding_box[k] + grow;
 }
 
 int or_closest_points(const gb_rigid_body_desc* rb_a, const double* verts_a,
@@ -1461,8 +1466,8 @@ int or_closest_points(const gb_rigid_body_desc* rb_a, const double* verts_a,
     if(st)
         return st;
     body_view A, B;
-    view_of(&A, rb_a, &pa, verts_a);
-    view_of(&B, rb_b, &pb, verts_b);
+    view_of(&A, rb_a, &pa, verts_a, 0);
+    view_of(&B, rb_b, &pb, verts_b, 0);
     closest_points(&A, &B, a2w, b2w, gjk_variant, out);
     return GB_OK;
 }
@@ -1993,14 +1998,22 @@ int or_set_threads(or_ctx* c, int32_t n_threads)
     return GB_OK;
 }
 
+/* the bounding radius of rigid body i in the candidate test and the cell
+   size: the circumscribed radius, plus the crust under GB_FLAG_CRUST_BOUNDS */
+static double bound_radius(const or_ctx* c, int32_t i)
+{
+    return c->rbp[i].circumscribed_radius
+           + ((c->cfg.flags & GB_FLAG_CRUST_BOUNDS) ? c->rbs[i].crust_thickness : 0.0);
+}
+
 static int build_linked_cell(or_ctx* c)
 {
     /* Grains::Construction (Grains/Base/src/Grains.cpp:226-246): cell size is
        CellSizeFactor * 2 * max circumscribed radius over particles. */
     double lc = 0.0;
     for(int32_t i = 0; i < c->nrb; ++i)
-        if(c->rbp[i].circumscribed_radius > lc)
-            lc = c->rbp[i].circumscribed_radius;
+        if(bound_radius(c, i) > lc)
+            lc = bound_radius(c, i);
     double coeff = c->cfg.cell_size_factor;
     if(coeff < 1.0)
         coeff = 1.0;
@@ -2265,6 +2278,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
     const int64_t n       = c->n;
     const int     hist    = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
     const int     variant = c->cfg.gjk_variant;
+    const int     cb      = (c->cfg.flags & GB_FLAG_CRUST_BOUNDS) != 0;
 
     /* enumeration pass 1: bounding-sphere candidates per particle, in the
        reference's order (27 neighbour cells in k, j, i order; ids ascending) */
@@ -2273,7 +2287,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
     {
         c->pair_off[a]        = (uint32_t)total;
         const uint32_t* nbl   = c->nbr + 27 * (size_t)c->hash[a];
-        const double    ra    = c->rbp[c->rb_id[a]].circumscribed_radius;
+        const double    ra    = bound_radius(c, c->rb_id[a]);
         for(int i = 0; i < 27; ++i)
         {
             if(nbl[i] == UINT32_MAX)
@@ -2285,7 +2299,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
                     continue;
                 double d[3];
                 sub3(c->tr + 12 * b + 9, c->tr + 12 * a + 9, d);
-                if(norm3(d) - (ra + c->rbp[c->rb_id[b]].circumscribed_radius) < 0.0)
+                if(norm3(d) - (ra + bound_radius(c, c->rb_id[b])) < 0.0)
                     ++total;
             }
         }
@@ -2308,7 +2322,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
         double*                    F    = c->torce + 6 * a;
         double*                    Tq   = F + 3;
         body_view                  A;
-        view_of(&A, rbA, prA, c->verts);
+        view_of(&A, rbA, prA, c->verts, cb);
         const uint32_t* nbl = c->nbr + 27 * (size_t)c->hash[a];
         int64_t         slot = c->pair_off[a];
         for(int i = 0; i < 27; ++i)
@@ -2324,7 +2338,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
                 const gb_rigid_body_props* prB = &c->rbp[c->rb_id[b]];
                 const double*              trB = c->tr + 12 * b;
                 body_view                  B;
-                view_of(&B, rbB, prB, c->verts);
+                view_of(&B, rbB, prB, c->verts, cb);
                 double d[3];
                 sub3(trB + 9, trA + 9, d);
                 const int cand = norm3(d) - (A.rcirc + B.rcirc) < 0.0;
@@ -2380,7 +2394,7 @@ int or_detect_collision_and_compute_contact_forces(or_ctx* c, int32_t* result)
         for(int32_t o = 0; o < c->nob; ++o)
         {
             body_view O;
-            view_of(&O, &c->obs[o], &c->obp[o], NULL);
+            view_of(&O, &c->obs[o], &c->obp[o], NULL, cb);
             const double* trO = c->obs_tr + 12 * o;
             or_contact    ci;
             closest_points(&A, &O, trA, trO, variant, &ci);

@@ -273,7 +273,9 @@ ref_ctx* ref_create(const gb_config* cfg, int* status)
             *status = GB_E_INVALID_ARG;
         return nullptr;
     }
-    if(cfg->contact_law != GB_LAW_HOOKE || cfg->integrator != GB_FIRST_ORDER_EXPLICIT)
+    // the reference's own law, integrator and bounding tests only
+    if(cfg->contact_law != GB_LAW_HOOKE || cfg->integrator != GB_FIRST_ORDER_EXPLICIT
+       || (cfg->flags & GB_FLAG_CRUST_BOUNDS))
     {
         if(status)
             *status = GB_E_UNSUPPORTED;

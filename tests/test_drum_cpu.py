@@ -57,3 +57,44 @@ def test_wall_surface_velocity_enters_the_law(oracle, law):
     assert out[0][1] == out[1][1] > 3
     assert np.array_equal(out[1][0], out[2][0])
     assert np.abs(out[0][0] - out[1][0]).max() > 1e-3 * np.abs(out[1][0]).max()
+
+
+def run_cubes(oracle, flags, shape, steps=600):
+    """The head-on cube collision (scenes.cube_collision) in the oracle with the
+    signed-volume GJK: the first contact's overlap, the steps in contact, and
+    the final velocities (NaN once the state is non-finite)."""
+    sc = scenes.cube_collision(shape=shape, gap=0.2e-3, tilt=0.05)
+    s = scenes.System(oracle, sc, flags=flags | abi.GB_FLAG_RECORD_CONTACT_INFO,
+                      contact_law=abi.GB_LAW_HOOKE_HISTORY, gjk_variant=abi.GB_GJK_SV)
+    first, in_contact = None, 0
+    for k in range(steps):
+        s.step(1)
+        if s.stats().contacts:
+            in_contact += 1
+            if first is None:
+                first = s.dump(abi.GB_DUMP_CONTACT_INFO)[0, 6]
+        kin = s.velocities()
+        if not np.isfinite(kin).all():
+            break
+    s.close()
+    return first, in_contact, kin
+
+
+@pytest.mark.parametrize("shape", ["polyhedron", "box"])
+def test_cube_contact_needs_the_crust_in_the_bounding_tests(oracle, shape):
+    """The reference's OBB pre-filter bounds a cube by the cube itself, while
+    the contact starts once the cubes come within the crusts' sum: the pair
+    first reaches GJK with the cubes intersecting (overlap = -crust sum), whose
+    normal is 0/0, and the state turns non-finite.  With GB_FLAG_CRUST_BOUNDS
+    the contact starts at an overlap of less than a step's approach (0.4 um)
+    and the cubes part again, slower (restitution 0.7; some of the energy
+    goes into the spin the tilted faces give them)."""
+    first, _, kin = run_cubes(oracle, 0, shape)
+    assert first == pytest.approx(-0.08e-3, rel=1e-3)
+    assert not np.isfinite(kin).all()
+    first, in_contact, kin = run_cubes(oracle, abi.GB_FLAG_CRUST_BOUNDS, shape)
+    assert -0.4e-6 < first < 0.0
+    assert 50 < in_contact < 400
+    assert np.isfinite(kin).all()
+    assert kin[0, 0] < 0.0 < kin[1, 0]                 # moving apart
+    assert abs(kin[1, 0] - kin[0, 0]) < 0.4            # slower than they met
