@@ -163,6 +163,8 @@ struct gb_ctx
     uint32_t* d_gjkq   = nullptr; // the step's pairs that need GJK (pair capacity; the
                                   // mixed mode: a second queue for its FP64 GJK after it)
     uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
+    uint32_t* d_ovf    = nullptr; // particles with more partners than pair slots
+    int       ovf_phase = 0;      // which of d_gjkn[2], [3] counts them this step
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
     // the finer candidate grid of polydisperse packings (k_pair_count_fine)
     bool      fine_planned = false, fine = false, fcount_zero = false;
@@ -518,8 +520,11 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_contacts, n));
     GB_TRY(dalloc(&c->d_flags, 1));
     GB_TRY(dalloc(&c->d_counters, 4));
-    GB_TRY(dalloc(&c->d_gjkn, 2));
-    GB_CK(cudaMemset(c->d_gjkn, 0, 2 * sizeof(uint32_t)));
+    // [0], [1]: the GJK queues' lengths; [2], [3]: the fill pass's overflow
+    // counts, alternating by step
+    GB_TRY(dalloc(&c->d_gjkn, 4));
+    GB_CK(cudaMemset(c->d_gjkn, 0, 4 * sizeof(uint32_t)));
+    GB_TRY(dalloc(&c->d_ovf, n));
     if(!c->d_ticket)
     {
         GB_TRY(dalloc(&c->d_ticket, 1));
@@ -915,12 +920,19 @@ int build_pairs(gb_ctx* c)
     GB_CK(cudaGetLastError());
     GB_TRY(scan_u32(c, c->d_count, off, n, off + n, c->d_flags));
     mark(c, 4);
+    c->ovf_phase ^= 1;
     GB_CK(launch(c->pdl, k_pair_fill<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_sorted_of,
                  c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
                  c->d_slot, c->d_obsmask_id, c->nob, off, c->d_pa, c->d_pb[c->cur], c->cap,
-                 c->d_flags, c->d_gjkn, c->d_count + n + 1));
+                 c->d_flags, c->d_gjkn, c->d_count + n + 1, c->d_ovf, c->ovf_phase));
     c->count_zero = true; // the fill pass zeroes each count it reads
-    c->launches += 1;
+    GB_CK(launch(c->pdl, k_pair_fill_overflow<S>, 4 * c->sms, 128, s,
+                 (const uint32_t*)c->d_gjkn + 2 + c->ovf_phase, (const uint32_t*)c->d_ovf,
+                 (const uint32_t*)c->d_skeys, (const uint32_t*)c->d_sids,
+                 (const uint32_t*)c->d_sorted_of, (const double4*)c->d_spos, spos32,
+                 (const uint32_t*)c->d_cstart, c->dims[0], c->dims[1], c->dims[2],
+                 (const uint32_t*)off, c->d_pa, c->d_pb[c->cur], (const int*)c->d_flags));
+    c->launches += 2;
     GB_CK(cudaGetLastError());
     mark(c, 5);
     return GB_OK;
@@ -1417,7 +1429,7 @@ int gb_destroy(gb_ctx* c)
                     c->d_contacts,
                     c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn,
                     c->d_fkey, c->d_fcount, c->d_fstart, c->d_fskey, c->d_fids, c->d_fref,
-                    c->d_fpos, c->d_fpos32};
+                    c->d_fpos, c->d_fpos32, c->d_ovf};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);

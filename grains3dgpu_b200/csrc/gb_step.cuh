@@ -753,16 +753,20 @@ __global__ void __launch_bounds__(kBlock)
                 const uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
                 int n_obs, const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
-                uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot)
+                uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot,
+                uint32_t* __restrict__ ovf_list, int ovf_phase)
 {
     grid_dep_sync();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if(a == 0)
     {
         // the narrow phase's GJK queues of this step start empty: [0] the
-        // cull pass's, [1] the mixed mode's FP32 stage's
-        gjk_count[0] = 0;
-        gjk_count[1] = 0;
+        // cull pass's, [1] the mixed mode's FP32 stage's; [2 + phase] counts
+        // this step's overflowing particles, [3 - phase] (last step's, read
+        // by its overflow pass) starts the next step at zero
+        gjk_count[0]             = 0;
+        gjk_count[1]             = 0;
+        gjk_count[3 - ovf_phase] = 0;
     }
     if(a >= n || step_aborted(flags))
         return;
@@ -820,12 +824,12 @@ __global__ void __launch_bounds__(kBlock)
         out += cp;
     }
     else
-        for_each_candidate<is_strict<S>(), is_mixed<S>()>(s, skeys, spos, spos32, cstart, nx, ny,
-                                                          nz, [&](uint32_t t) {
-                                                              pair_a[out] = a;
-                                                              pair_b[out] = sids[t];
-                                                              ++out;
-                                                          });
+    {
+        // more partners than slots (the largest grains of a polydisperse
+        // packing): k_pair_fill_overflow writes them, a warp per particle
+        ovf_list[atomicAdd(gjk_count + 2 + ovf_phase, 1u)] = (uint32_t)a;
+        out += cp;
+    }
     for(int o = 0; o < n_obs; ++o)
         if(o >= kMaskObstacles || ((mask >> o) & 1u))
         {
@@ -833,6 +837,63 @@ __global__ void __launch_bounds__(kBlock)
             pair_b[out] = kObstacleBit | (uint32_t)o;
             ++out;
         }
+}
+
+// The particle pairs of the particles whose partners overflowed their slots,
+// one warp per particle: the 27 cells in the reference's order (as
+// for_each_candidate walks them), 32 candidates a round, the hits of a round
+// written in lane order (ballot + prefix count), so the list is the one
+// for_each_candidate writes.
+template <typename S>
+__global__ void __launch_bounds__(128)
+    k_pair_fill_overflow(const uint32_t* __restrict__ ovf_count,
+                         const uint32_t* __restrict__ ovf_list, const uint32_t* __restrict__ skeys,
+                         const uint32_t* __restrict__ sids, const uint32_t* __restrict__ sorted_of,
+                         const double4* __restrict__ spos, const float4* __restrict__ spos32,
+                         const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
+                         const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
+                         uint32_t* __restrict__ pair_b, const int* __restrict__ flags)
+{
+    grid_dep_sync();
+    constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
+    if(step_aborted(flags))
+        return;
+    const unsigned lane  = threadIdx.x & 31u;
+    const uint32_t total = *ovf_count;
+    const uint32_t warps = gridDim.x * (blockDim.x / 32);
+    for(uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) / 32; w < total; w += warps)
+    {
+        const uint32_t a   = ovf_list[w];
+        const uint32_t s   = sorted_of[a];
+        uint32_t       out = offset[a];
+        const uint32_t key = skeys[s];
+        const double4  pa  = spos[s];
+        float4         pa32;
+        if constexpr(PRE32)
+            pa32 = spos32[s];
+        const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
+        for(int r = 0; r < 9; ++r)
+        {
+            uint32_t t0, t1;
+            neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
+            for(uint32_t base = t0; base < t1; base += 32)
+            {
+                const uint32_t t   = base + lane;
+                bool           hit = t < t1 && t != s;
+                if constexpr(PRE32)
+                    hit = hit && !pretest_rejects<PRE32>(pa32, spos32[t]);
+                hit                 = hit && exact_hit<STRICT>(pa, spos[t]);
+                const unsigned bits = __ballot_sync(0xffffffffu, hit);
+                if(hit)
+                {
+                    const uint32_t k = out + __popc(bits & ((1u << lane) - 1u));
+                    pair_a[k]        = a;
+                    pair_b[k]        = sids[t];
+                }
+                out += __popc(bits);
+            }
+        }
+    }
 }
 
 // ---- narrow phase + contact law, one thread per candidate pair ---------------
