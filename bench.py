@@ -60,14 +60,15 @@ def measured_hbm():
 # FP64 in every mode; S = 4 in the mixed mode, 8 in FP64).  The HBM-rated
 # stages, as the hot-path scope defines them:
 #   broad phase (hash, sort, cell start): N (3 S_p + 4 + 4 + 8 + 8 + 4) + 8 C
-#   integration (the per-particle kernel): N (6 S_p + 30 S)
+#   integration (the per-particle kernel): N (6 S_p + 30 S), and in the mixed
+#     mode the orientation's FP32 remainder read and written, N (2 x 4 S)
 # and candidate enumeration (the count kernel and its scan): the sorted key,
 # FP64 position + radius, FP32 copy (mixed), id, count and the scan's read and
 # write, N (4 + 32 + 16 + 4 + 4 + 8) + 4 C.  The narrow phase is latency-bound
 # and is rated in pairs and GJK iterations per second instead.
 def stage_bytes(n, c, s):
     return {"broad_phase": n * (3 * 8 + 4 + 4 + 8 + 8 + 4) + 8 * c,
-            "integration": n * (6 * 8 + 30 * s),
+            "integration": n * (6 * 8 + 30 * s + (8 * s if s == 4 else 0)),
             "pair_count": n * (4 + 32 + (16 if s == 4 else 0) + 4 + 4 + 8) + 4 * c}
 
 

@@ -164,6 +164,7 @@ struct gb_ctx
                                   // mixed mode: a second queue for its FP64 GJK after it)
     uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
     uint32_t* d_ovf    = nullptr; // particles with more partners than pair slots
+    uint32_t* d_pcount = nullptr; // contacts per particle of the step (cleared as read)
     int       ovf_phase = 0;      // which of d_gjkn[2], [3] counts them this step
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
     // the finer candidate grid of polydisperse packings (k_pair_count_fine)
@@ -525,6 +526,8 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_gjkn, 4));
     GB_CK(cudaMemset(c->d_gjkn, 0, 4 * sizeof(uint32_t)));
     GB_TRY(dalloc(&c->d_ovf, n));
+    GB_TRY(dalloc(&c->d_pcount, n));
+    GB_CK(cudaMemset(c->d_pcount, 0, (size_t)n * sizeof(uint32_t)));
     if(!c->d_ticket)
     {
         GB_TRY(dalloc(&c->d_ticket, 1));
@@ -952,6 +955,7 @@ PairOut<store_t<S>> pair_out(gb_ctx* c)
         po.xi[k] = c->d_xi[c->cur] ? (St*)c->d_xi[c->cur] + k * cap : nullptr;
     }
     po.contact  = c->d_pc;
+    po.pcount   = c->d_pcount;
     po.info     = c->d_info;
     const int prev = 1 - c->cur;
     po.prev_off = c->d_off[prev];
@@ -1202,6 +1206,9 @@ void restore(gb_ctx* c, const StepSnap& s)
     c->count_zero     = false; // an aborted fill pass may have left counts behind
     c->ccount_zero    = false; // ... and an aborted scatter pass cell counts
     c->fcount_zero    = false; // ... or fine-cell counts
+    // ... and an aborted step its contact counts per particle
+    if(c->d_pcount)
+        cudaMemsetAsync(c->d_pcount, 0, (size_t)c->n * sizeof(uint32_t), c->stream);
 }
 
 // Launches n_steps detects (PHASE_DETECT) or fused steps (PHASE_STEP) with no
@@ -1429,7 +1436,7 @@ int gb_destroy(gb_ctx* c)
                     c->d_contacts,
                     c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn,
                     c->d_fkey, c->d_fcount, c->d_fstart, c->d_fskey, c->d_fids, c->d_fref,
-                    c->d_fpos, c->d_fpos32, c->d_ovf};
+                    c->d_fpos, c->d_fpos32, c->d_ovf, c->d_pcount};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);

@@ -242,8 +242,12 @@ GB_D void obstacle_frame(const Tables<S>& tb, int o, const double xa[3], V3<S>& 
 // farther than that from the plane (plus a bound on the rounding of both
 // sides) cannot touch it, and the full test of closest_rectangle would reject
 // it too.  Other obstacle types are always candidates.
-template <typename S>
-GB_D uint32_t obstacle_mask_at(const Tables<S>& tb, uint32_t r, const M3<S>& RA, const double xa[3])
+// The box's extent along any unit normal is at most |bb| (Cauchy-Schwarz), so
+// a centre farther than |bb| from every plane is decided without the
+// rotation: `rot` (a callable returning RA) runs only for the planes within
+// that reach.
+template <typename S, typename Rot>
+GB_D uint32_t obstacle_mask_at(const Tables<S>& tb, uint32_t r, Rot&& rot, const double xa[3])
 {
     const int nm = tb.n_obs < kMaskObstacles ? tb.n_obs : kMaskObstacles;
     if(nm == 0)
@@ -256,22 +260,51 @@ GB_D uint32_t obstacle_mask_at(const Tables<S>& tb, uint32_t r, const M3<S>& RA,
                           (double)tb.inertia[r].bb[2]};
     const double ax    = fabs(xa[0]) + fabs(xa[1]) + fabs(xa[2]);
     uint32_t     mask  = ~tb.obs_rect & ((nm == 32) ? ~0u : ((1u << nm) - 1u));
+    const double reach = sqrt(bb[0] * bb[0] + bb[1] * bb[1] + bb[2] * bb[2]);
+    bool         have  = false;
+    M3<S>        RA;
     for(int o = 0; o < nm; ++o)
     {
         if(!((tb.obs_rect >> o) & 1u))
             continue;
         const double4 pl = tb.obs_plane[o];
         const double  dc = fabs(pl.x * xa[0] + pl.y * xa[1] + pl.z * xa[2] - pl.w);
-        double        hb = 0.0;
-#pragma unroll
-        for(int k = 0; k < 3; ++k)
+        if(dc - reach > 1e-6 * reach + 1e-12 * (1.0 + ax + fabs(pl.w)))
+            continue; // beyond the box's reach whatever its orientation
+        if(!have)
         {
-            // (RA^T n)_k = sum_j RA[j][k] n_j
-            const double nk = to_d(RA.m[k]) * pl.x + to_d(RA.m[3 + k]) * pl.y
-                              + to_d(RA.m[6 + k]) * pl.z;
-            hb += bb[k] * fabs(nk);
+            RA   = rot();
+            have = true;
         }
-        const double slack = 1e-6 * hb + 1e-12 * (1.0 + ax + fabs(pl.w));
+        double hb, slack;
+        if constexpr(is_mixed<S>())
+        {
+            // the extent from the FP32 rotation in FP32: each |(RA^T n)_k|
+            // is off by a few 1e-7 (its rounding, and the FP32 rotation's
+            // distance from the FP64 one), so the slack takes 1e-6 of the
+            // box's half-extents' sum
+            const float n32[3] = {(float)pl.x, (float)pl.y, (float)pl.z};
+            float       h32    = 0.0f;
+#pragma unroll
+            for(int k = 0; k < 3; ++k)
+                h32 += (float)bb[k]
+                       * fabsf(RA.m[k] * n32[0] + RA.m[3 + k] * n32[1] + RA.m[6 + k] * n32[2]);
+            hb    = (double)h32;
+            slack = 1e-6 * (bb[0] + bb[1] + bb[2]) + 1e-12 * (1.0 + ax + fabs(pl.w));
+        }
+        else
+        {
+            hb = 0.0;
+#pragma unroll
+            for(int k = 0; k < 3; ++k)
+            {
+                // (RA^T n)_k = sum_j RA[j][k] n_j
+                const double nk = to_d(RA.m[k]) * pl.x + to_d(RA.m[3 + k]) * pl.y
+                                  + to_d(RA.m[6 + k]) * pl.z;
+                hb += bb[k] * fabs(nk);
+            }
+            slack = 1e-6 * hb + 1e-12 * (1.0 + ax + fabs(pl.w));
+        }
         if(!(dc - hb > slack))
             mask |= 1u << o;
     }
@@ -289,7 +322,7 @@ __global__ void __launch_bounds__(kBlock)
     if(i >= n)
         return;
     const double xa[3] = {st.pos[0][i], st.pos[1][i], st.pos[2][i]};
-    mask[i]            = obstacle_mask_at<S>(tb, st.rb_id[i], load_rot<S>(st, i), xa);
+    mask[i] = obstacle_mask_at<S>(tb, st.rb_id[i], [&] { return load_rot<S>(st, i); }, xa);
 }
 
 GB_D int obstacle_candidates(uint32_t mask, int n_obs)
@@ -904,6 +937,8 @@ struct PairOut
     St*      t[3];
     St*      m[3];     // rolling moment (only when some kr != 0)
     uint8_t* contact;  // kContactParticle / kContactObstacle when overlap < 0, else 0
+    uint32_t* pcount;  // contacts per particle id (zero before the narrow phase; the
+                       // per-particle kernel reads and clears them)
     double*  info;     // optional: 7 per pair (point, vector, overlap) in world frame
     // tangential history (history law): current step out, previous step in
     St*             xi[3];
@@ -1075,6 +1110,8 @@ GB_D void narrow_obstacle(int64_t p, uint32_t a, int o, const State<store_t<S>>&
     }
     store_pair<S>(po, p, F, zero3<S>(), hit ? kContactObstacle : uint8_t(0), law_kind, has_kr, ci,
                   xa);
+    if(hit)
+        atomicAdd(po.pcount + a, 1u);
     if(iters)
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
@@ -1428,6 +1465,8 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
     if((VAR & kGjkPaired) && (threadIdx.x & 1u))
         return;
     store_pair<S>(po, p, F, xi_new, hit ? kContactParticle : uint8_t(0), law_kind, has_kr, ci, xa);
+    if(hit)
+        atomicAdd(po.pcount + a, 1u);
     if(iters)
         atomicAdd(&counters[1], (unsigned long long)iters);
 }
@@ -1611,7 +1650,7 @@ __global__ void __launch_bounds__(128)
 // 256-thread blocks per SM, which measured faster than five blocks at 48 with
 // spills); the FP64 ones need about 100 registers and get two blocks.
 template <typename S>
-__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 3 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
                 uint32_t* __restrict__ mask_out, int* __restrict__ flags,
@@ -1623,7 +1662,31 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
         return;
     const uint32_t            r   = sp.rb_identity ? (uint32_t)i : st.rb_id[i];
     const RBInertia<store_t<S>>* in = tb.inertia + r;
-    const S                   m   = S(in->mass);
+    // the body record (mass, inertia, inverse inertia, box) in 16-byte loads
+    store_t<S> rec[16];
+    {
+        constexpr int per = 16 / sizeof(store_t<S>);
+        using Vec         = typename std::conditional<per == 4, float4, double2>::type;
+        const Vec* v4     = reinterpret_cast<const Vec*>(in);
+#pragma unroll
+        for(int k = 0; k < 16 / per; ++k)
+        {
+            const Vec x = __ldg(v4 + k);
+            if constexpr(per == 4)
+            {
+                rec[4 * k]     = x.x;
+                rec[4 * k + 1] = x.y;
+                rec[4 * k + 2] = x.z;
+                rec[4 * k + 3] = x.w;
+            }
+            else
+            {
+                rec[2 * k]     = x.x;
+                rec[2 * k + 1] = x.y;
+            }
+        }
+    }
+    const S                   m   = S(rec[0]);
     V3<S>                     F, T;
     V3<S>                     v = load3<S>(st.vel, i), w = load3<S>(st.omg, i);
     int                       nc = 0;
@@ -1633,7 +1696,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     const bool move = (sp.phases & PHASE_MOVE) != 0;
     S            I[6], I1[6];
     Quat<S>      q;
-    Quat<double> q64; // mixed: the compensated orientation
+    float        qlo[4]; // mixed: the orientation's FP32 remainder (q + qlo is the orientation)
     M3<S>        R;
     double       x0[3];
     if(move)
@@ -1641,14 +1704,16 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
 #pragma unroll
         for(int k = 0; k < 6; ++k)
         {
-            I[k]  = S(in->I[k]);
-            I1[k] = S(in->I1[k]);
+            I[k]  = S(rec[1 + k]);
+            I1[k] = S(rec[7 + k]);
         }
         if constexpr(is_mixed<S>())
         {
             q.w = S(st.rot[0][i]);
             q.v = mk<S>(S(st.rot[1][i]), S(st.rot[2][i]), S(st.rot[3][i]));
-            q64 = load_quat64(st, i);
+#pragma unroll
+            for(int k = 0; k < 4; ++k)
+                qlo[k] = st.rot[4 + k][i];
         }
         else
             R = load_rot<S>(st, i);
@@ -1670,8 +1735,13 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
             F = zero3<S>();
             T = zero3<S>();
         }
-        // the particle's pairs, then its obstacle pairs, in list order
-        for(uint32_t p = off[i]; p < off[i + 1]; ++p)
+        // the particle's pairs, then its obstacle pairs, in list order; most
+        // particles have no contact (the narrow phase counts them) and skip
+        // their list
+        const uint32_t ncon = po.pcount[i];
+        if(ncon)
+            po.pcount[i] = 0u;
+        for(uint32_t p = ncon ? off[i] : 0u, pe = ncon ? off[i + 1] : 0u; p < pe; ++p)
         {
             const uint8_t hit = po.contact[p];
             if(!hit)
@@ -1726,17 +1796,20 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
                 xn[k] = to_d(S(x0[k]) + tk[k]);
             st.pos[k][i] = xn[k];
         }
+        float hi[4]; // mixed: the new orientation's FP32 part
         if constexpr(is_mixed<S>())
         {
             // the increment from the FP32 angular velocity, composed with the
             // compensated orientation and renormalised in FP64
-            Quat<double> dq64;
+            Quat<double> dq64, q64;
             dq64.w          = (double)dq.w;
             dq64.v          = cvt3<double>(dq.v);
+            q64.w           = (double)q.w + (double)qlo[0];
+            q64.v           = mk<double>((double)q.v.x + (double)qlo[1], (double)q.v.y + (double)qlo[2],
+                                         (double)q.v.z + (double)qlo[3]);
             Quat<double> qn = qmul(dq64, q64);
-            const double nq = sqrt(qn.w * qn.w + norm2(qn.v));
-            const double c[4] = {qn.w / nq, qn.v.x / nq, qn.v.y / nq, qn.v.z / nq};
-            float        hi[4];
+            const double rn = 1.0 / sqrt(qn.w * qn.w + norm2(qn.v));
+            const double c[4] = {qn.w * rn, qn.v.x * rn, qn.v.y * rn, qn.v.z * rn};
 #pragma unroll
             for(int k = 0; k < 4; ++k)
             {
@@ -1744,8 +1817,6 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
                 st.rot[k][i]     = hi[k];
                 st.rot[4 + k][i] = (float)(c[k] - (double)hi[k]);
             }
-            if(mask_out)
-                R = quat_to_matrix<S>(hi[0], hi[1], hi[2], hi[3]);
         }
         else
         {
@@ -1756,7 +1827,15 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
         }
         // the obstacle candidates of the next detect, from the new pose
         if(mask_out)
-            mask_out[i] = obstacle_mask_at<S>(tb, r, R, xn);
+            mask_out[i] = obstacle_mask_at<S>(
+                tb, r,
+                [&] {
+                    if constexpr(is_mixed<S>())
+                        return quat_to_matrix<S>(hi[0], hi[1], hi[2], hi[3]);
+                    else
+                        return R;
+                },
+                xn);
         st.vel[0][i] = (store_t<S>)to_d(v.x);
         st.vel[1][i] = (store_t<S>)to_d(v.y);
         st.vel[2][i] = (store_t<S>)to_d(v.z);
