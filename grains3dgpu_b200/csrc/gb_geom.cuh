@@ -186,22 +186,27 @@ GB_D V3<S> support(const Body<S>& b, const V3<S>& v)
 }
 
 // Superquadric::support in FP32 in the log domain (the form of
-// support_sq_log), for the mixed mode's first-iteration test of GJK.  FP32
+// support_sq_log), for the mixed mode's FP32 stages (the first-iteration test
+// and the FP32 GJK), which only certify separation with a margin of 1e-4 of
+// the bounding radii.  The hardware approximations of log2 and of the
+// quotient (a few ulp; 2^-21.4 absolute for log2 near 1) and exp2f's 2 ulp
+// move a support point by ~1e-6 of its size, some 1e-9 m, far inside that
+// margin.  FP32
 // exponents overflow where FP64 ones do not (2^e for e > 128): a direction
 // whose chain would exceed 2^100 at any step, or with v.x = 0, gives NaN,
 // which sends the pair to the FP64 solve.
 GB_D V3<float> support_sq_log32(const Body<float>& b, const V3<float>& v)
 {
     const float abvx = fabsf(v.x), abvy = fabsf(v.y), abvz = fabsf(v.z);
-    const float la = b.k[4] * log2f(b.k[0] * abvy / abvx);
+    const float la = b.k[4] * __log2f(__fdividef(b.k[0] * abvy, abvx));
     const float ea = b.p[4] * la;
-    const float lt = log2f(1.0f + exp2f(ea));
-    const float lb = b.k[5] * lt + b.k[3] * log2f(b.k[1] * abvz / abvx);
+    const float lt = __log2f(1.0f + exp2f(ea));
+    const float lb = b.k[5] * lt + b.k[3] * __log2f(__fdividef(b.k[1] * abvz, abvx));
     const float e1 = b.k[6] * lt, e2 = b.p[3] * lb;
     if(!(abvx > 0.0f) || !(ea <= 100.0f) || !(e1 <= 100.0f) || !(e2 <= 100.0f)
        || !(la <= 100.0f) || !(lb <= 100.0f))
         return mk<float>(NAN, NAN, NAN);
-    const float xt = exp2f(-b.k[7] * log2f(exp2f(e1) + exp2f(e2)));
+    const float xt = exp2f(-b.k[7] * __log2f(exp2f(e1) + exp2f(e2)));
     return mk<float>(sgn(v.x) * b.p[0] * xt, sgn(v.y) * exp2f(la) * b.p[1] * xt,
                      sgn(v.z) * exp2f(lb) * b.p[2] * xt);
 }
