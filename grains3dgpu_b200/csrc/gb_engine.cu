@@ -1032,10 +1032,11 @@ int run_detect(gb_ctx* c, int phases)
                          total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
                          S(c->cfg.dt), c->d_counters, c->d_gjkq, c->d_gjkn));
             // the FP64 GJK's queue: the cull pass's, or in the mixed mode
-            // (GJK-JH) what the FP32 stage leaves of it
+            // what the FP32 stage leaves of it (its certificate, a lower
+            // bound on the distance, holds for every GJK variant)
             const uint32_t* q64 = c->d_gjkq;
             const uint32_t* n64 = c->d_gjkn;
-            if constexpr(is_mixed<S>() && VAR == GB_GJK_JH)
+            if constexpr(is_mixed<S>())
             {
                 GB_CK(launch(c->pdl, k_narrow_gjk32, one_wave((const void*)k_narrow_gjk32), 128, s,
                              (const uint32_t*)c->d_gjkn, (const int*)c->d_flags,
@@ -1958,7 +1959,7 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
         // tests and GJK's first iteration), and those solved by the FP64 GJK
         uint32_t q[2] = {0, 0};
         GB_CK(cudaMemcpy(q, c->d_gjkn, sizeof(q), cudaMemcpyDeviceToHost));
-        const bool stage32 = c->prec == GB_MIXED && c->cfg.gjk_variant == GB_GJK_JH;
+        const bool stage32 = c->prec == GB_MIXED;
         o->gjk_calls       = c->detect_valid ? (int64_t)q[0] : 0;
         o->gjk_fp64_calls  = c->detect_valid ? (int64_t)q[stage32 ? 1 : 0] : 0;
         o->fine_grid_cells = c->fine ? (int64_t)c->fine_nf : 0;

@@ -1164,7 +1164,10 @@ GB_D bool needs_gjk(const Body<S>& A, const Body<S>& B, const M3<S>& RA, const M
 // frames add a few 1e-9 m): a pair decided here is one that the FP64 GJK
 // also finds out of contact, so the mixed mode's contact set and contact
 // geometry stay those of its FP64 GJK.
-template <typename S>
+// The first rule holds for every GJK variant (each returns the norm of a
+// point of the Minkowski difference, at least the true distance, which g
+// bounds from below); the second is GJK-JH's own stopping rule (JH_RULE).
+template <typename S, bool JH_RULE = true>
 GB_D bool gjk_first_iteration_separates(const Body<S>& A, const Body<S>& B, const M3<S>& RA,
                                         const M3<S>& RB, const V3<S>& d)
 {
@@ -1183,7 +1186,7 @@ GB_D bool gjk_first_iteration_separates(const Body<S>& A, const Body<S>& B, cons
                                        : S(1e-9) * (A.rcirc + B.rcirc) + S(1e-15);
     if(g > ct + margin)
         return true;
-    return g < -margin && dist - ct > margin;
+    return JH_RULE && g < -margin && dist - ct > margin;
 }
 
 // ---- the mixed mode's FP32 GJK stage ------------------------------------------
@@ -1405,7 +1408,9 @@ GB_D void narrow_pair(int64_t p, const uint32_t* __restrict__ pair_a,
                 ci = closest_spheres(A, B, oA, oB);
         }
         else if(!needs_gjk<S>(A, B, RA, RB, xa, xb, d)
-                || (JH && gjk_first_iteration_separates<S>(A, B, RA, RB, d)))
+                || (JH && gjk_first_iteration_separates<S, true>(A, B, RA, RB, d))
+                || (!JH && is_mixed<S>()
+                    && gjk_first_iteration_separates<S, false>(A, B, RA, RB, d)))
             ci = no_contact<S>();
         else
         {
