@@ -72,6 +72,8 @@ def stage_bytes(n, c, s):
             "pair_count": n * (4 + 32 + (16 if s == 4 else 0) + 4 + 4 + 8) + 4 * c}
 
 
+STAGE_KERNEL = {"broad_phase": "k_hash_count + k_scan_onepass + k_cell_scatter + k_cell_rank",
+                "integration": "k_particles"}
 STAGE_PHASES = {"broad_phase": ("hash", "sort", "cell_start"), "integration": ("particle",),
                 "pair_count": ("pair_count",)}
 
@@ -306,8 +308,8 @@ def measure_drum(args, torch):
     (40% spheres, 30% cubes as polyhedra, 30% n = 6 superquadrics) in a drum
     of radius 0.1 m turning at 30 rpm, its length scaled for the grains to
     fill 40% of it, the tangential-history law, grain-wall friction 0.6:
-    `drum_steps` mixed steps in one gb_step call, and a shorter FP64 run of
-    the same drum for the ratio.  Two choices of the run keep it finite and
+    `drum_steps` steps in one gb_step call, mixed and then FP64 from the same
+    initial state, for the ratio.  Two choices of the run keep it finite and
     its contacts real: the signed-volume GJK (the reference's GJK-JH, with its
     absolute determinant threshold, misses most contacts of mm grains) and
     GB_FLAG_CRUST_BOUNDS (the reference's OBB pre-filter lets two cubes reach
@@ -323,7 +325,7 @@ def measure_drum(args, torch):
                        "GJK, crust-inclusive bounding tests (GB_FLAG_CRUST_BOUNDS)",
            "n_particles": scene.n}
     for prec, key, k in ((abi.GB_MIXED, "mixed", args.drum_steps),
-                         (abi.GB_FP64, "fp64", max(1, args.drum_steps // 10))):
+                         (abi.GB_FP64, "fp64", args.drum_steps)):
         s, el, _, _, _, st = run_engine(args, scene, prec, k, 3, torch, 0, 1, timing=False,
                                         **dict(cfg))
         tr = s.transforms()
@@ -598,11 +600,20 @@ def main():
     hbm, hbm_kind = measured_hbm()
     per_step = ms / max(nsteps, 1)
     stages = stage_report(per_step, scene.n, st.n_cells, 4, hbm)
-    top = max(stages, key=lambda k: stages[k]["ms"])
-    roofline = {"kernel": top, "bound": "hbm", "achieved": stages[top]["achieved_gbs"],
+    # the roofline of the HBM-bound stages (broad phase and integration): the
+    # one with the larger share of the step; the step's largest kernels (the
+    # narrow phase, the candidate search) are issue- and latency-bound and are
+    # rated in `narrow` and `stages`
+    top = max(("broad_phase", "integration"), key=lambda k: stages[k]["ms"])
+    dominant = max((k for k in abi.PHASES), key=lambda k: float(per_step[abi.PHASES.index(k)]))
+    roofline = {"kernel": STAGE_KERNEL[top], "stage": top, "bound": "hbm",
+                "achieved": stages[top]["achieved_gbs"],
                 "peak": hbm, "unit": "GB/s", "frac": stages[top]["frac_of_measured_hbm"],
                 "traffic": traffic_bytes(top, scene.n), "peak_kind": hbm_kind,
-                "limiter": LIMITER.get(top)}
+                "limiter": LIMITER.get(top),
+                "step_dominant_phase": {"phase": dominant,
+                                        "ms": round(float(per_step[abi.PHASES.index(dominant)]), 4),
+                                        "limiter": LIMITER.get(dominant)}}
     narrow_ms = float(per_step[abi.PHASES.index("narrow")])
     narrow = {"ms": round(narrow_ms, 4), "candidate_pairs": int(st_ph.candidate_pairs),
               "pairs_per_s": st_ph.candidate_pairs / (narrow_ms * 1e-3) if narrow_ms else None,
@@ -710,22 +721,29 @@ def main():
     return 0
 
 
-# DRAM bytes (read + write) per particle of the HBM-rated kernels, from one
-# ncu capture of each on the bed with 200,000 grains (the summary of those
-# captures is committed beside the other profiles); their traffic scales with
-# the particle count at the bed's density.  The narrow phase's scales with
-# the pairs and is not extrapolated.
-TRAFFIC_PER_PARTICLE = {"integration": (32.71e6 + 0.13e6) / 200_000,
-                        "pair_count": (17.37e6 + 3.74e6) / 200_000}
+# DRAM bytes (read + write) per particle of the HBM-rated kernels, from ncu
+# captures of the bed at 600,000 grains (k_particles with --set full; the
+# broad-phase kernels' dram__bytes metrics), whose per-step working set
+# exceeds the L2 as the 1,000,000-grain bed's does; the summary is committed
+# beside the other profiles.  Their traffic scales with the particle count
+# at the bed's density.  Writes that stay in L2 when the kernel ends are not
+# counted by the capture.
+TRAFFIC_PER_PARTICLE = {"integration": (95.36e6 + 8.02e6) / 600_000,
+                        "broad_phase": (14.48e6 + 2.56e6 + 26.54e6 + 0.06e6) / 600_000}
 
 
-# what bounds each stage, from the captures named above
-LIMITER = {"pair_count": "memory latency of the neighbour walk: 11 long-scoreboard stalls per "
-                         "issue at 42% warps active, 43% issue slots; ~480 FP32 pre-tests per "
-                         "particle in 27 cells of 7.2 mm",
-           "integration": "memory latency: 38% warps active, 4.9 long-scoreboard stalls per "
-                          "issue, 164 B per particle moved",
-           "broad_phase": "launch and tail latency of short kernels"}
+# what bounds each stage or phase, from the same captures and those of the bed
+# at 200,000 grains
+LIMITER = {"integration": "issue and memory latency: 28% warps active (79 registers, three "
+                          "256-thread blocks per SM), 38% issue slots; 172 B per particle "
+                          "read from DRAM",
+           "broad_phase": "launch and tail latency of short dependent passes (hash 10 us, "
+                          "scan, scatter 9 us, rank 20 us at 600k grains); 73 B per particle "
+                          "read from DRAM",
+           "pair_count": "memory latency of the neighbour walk on the finer grid: 17 "
+                         "long-scoreboard stalls per issue at 46% warps active",
+           "narrow": "FP32 issue in the cull (42% issue slots, 24 of 32 lanes, 96 registers) "
+                     "and FP64 GJK chains at 10% warps active (220 registers)"}
 
 
 def traffic_bytes(phase, n):

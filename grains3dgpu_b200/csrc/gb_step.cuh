@@ -539,6 +539,42 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
     }
 }
 
+// A warp walks the concatenation of up to 32 ranges [t0, t1) of sorted
+// positions, lane r holding range r (lanes past the last range hold empty
+// ones), 32 entries a round in range order: visit(t, valid) runs on every
+// lane each round (warp-uniform).  All ranges' bounds are loaded at once, by
+// their lanes, and short ranges share rounds, where a range-at-a-time walk
+// pays a dependent load pair and a mostly idle round per range.
+template <typename Visit>
+GB_D void warp_ranges(uint32_t t0, uint32_t t1, Visit&& visit)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t len  = t1 > t0 ? t1 - t0 : 0u;
+    uint32_t       inc  = len; // inclusive prefix of the lengths
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if(lane >= (unsigned)o)
+            inc += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    const uint32_t exc   = inc - len;
+    for(uint32_t base = 0; base < total; base += 32)
+    {
+        const uint32_t idx = base + lane;
+        // the last range that starts at or before idx (exclusive prefixes
+        // do not decrease; an empty range shares its start with the next)
+        unsigned r = 0;
+#pragma unroll
+        for(unsigned step = 16; step >= 1; step >>= 1)
+            if(__shfl_sync(0xffffffffu, exc, r + step) <= idx)
+                r += step;
+        const uint32_t t = __shfl_sync(0xffffffffu, t0, r) + (idx - __shfl_sync(0xffffffffu, exc, r));
+        visit(t, idx < total);
+    }
+}
+
 // ---- candidate search on a finer grid (polydisperse packings) -----------------
 // The reference's cell is twice the LARGEST bounding radius, so in a
 // polydisperse packing a particle's 27 cells hold hundreds of others (~960 in
@@ -727,23 +763,31 @@ __global__ void __launch_bounds__(kBlock)
         const uint32_t y1    = fine_axis(pa.y + reach, g.mn[1], g.h, g.ny);
         const uint32_t z0    = fine_axis(pa.z - reach, g.mn[2], g.h, g.nz);
         const uint32_t z1    = fine_axis(pa.z + reach, g.mn[2], g.h, g.nz);
-        for(uint32_t z = z0; z <= z1; ++z)
-            for(uint32_t y = y0; y <= y1; ++y)
+        // the rows (z, y) of the box, 32 at a time, lane i holding row i of
+        // the chunk, walked as one sequence
+        const uint32_t wy = y1 - y0 + 1, rows = (z1 - z0 + 1) * wy;
+        for(uint32_t c0 = 0; c0 < rows; c0 += 32)
+        {
+            uint32_t t0 = 0, t1 = 0;
+            if(c0 + lane < rows)
             {
+                const uint32_t z   = z0 + (c0 + lane) / wy, y = y0 + (c0 + lane) % wy;
                 const uint32_t row = base + (z * g.ny + y) * g.nx;
-                uint32_t       t0  = fstart[row + x0];
-                const uint32_t t1  = fstart[row + x1 + 1];
+                t0                 = fstart[row + x0];
+                t1                 = fstart[row + x1 + 1];
                 if(large && t0 < (uint32_t)f + 1)
                     t0 = (uint32_t)f + 1; // each large pair once
-                for(uint32_t t = t0 + lane; t < t1; t += 32)
-                {
-                    if constexpr(PRE32)
-                        if(pretest_rejects<PRE32>(pa32, fpos32[t]))
-                            continue;
-                    if(exact_hit<STRICT>(pa, fpos[t]))
-                        record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
-                }
             }
+            warp_ranges(t0, t1, [&](uint32_t t, bool valid) {
+                if(!valid)
+                    return;
+                if constexpr(PRE32)
+                    if(pretest_rejects<PRE32>(pa32, fpos32[t]))
+                        return;
+                if(exact_hit<STRICT>(pa, fpos[t]))
+                    record_pair(sa, a, fref[t], fids[t], count, pslot, slot);
+            });
+        }
     }
 }
 
@@ -905,27 +949,24 @@ __global__ void __launch_bounds__(128)
         if constexpr(PRE32)
             pa32 = spos32[s];
         const int cx = key % nx, cy = (key / nx) % ny, cz = key / (nx * ny);
-        for(int r = 0; r < 9; ++r)
-        {
-            uint32_t t0, t1;
-            neighbour_row(cstart, nx, ny, nz, cx, cy, cz, r, t0, t1);
-            for(uint32_t base = t0; base < t1; base += 32)
+        // the 9 rows of 3 cells, lane r holding row r, walked as one sequence
+        uint32_t t0 = 0, t1 = 0;
+        if(lane < 9)
+            neighbour_row(cstart, nx, ny, nz, cx, cy, cz, (int)lane, t0, t1);
+        warp_ranges(t0, t1, [&](uint32_t t, bool valid) {
+            bool hit = valid && t != s;
+            if constexpr(PRE32)
+                hit = hit && !pretest_rejects<PRE32>(pa32, spos32[t]);
+            hit                 = hit && exact_hit<STRICT>(pa, spos[t]);
+            const unsigned bits = __ballot_sync(0xffffffffu, hit);
+            if(hit)
             {
-                const uint32_t t   = base + lane;
-                bool           hit = t < t1 && t != s;
-                if constexpr(PRE32)
-                    hit = hit && !pretest_rejects<PRE32>(pa32, spos32[t]);
-                hit                 = hit && exact_hit<STRICT>(pa, spos[t]);
-                const unsigned bits = __ballot_sync(0xffffffffu, hit);
-                if(hit)
-                {
-                    const uint32_t k = out + __popc(bits & ((1u << lane) - 1u));
-                    pair_a[k]        = a;
-                    pair_b[k]        = sids[t];
-                }
-                out += __popc(bits);
+                const uint32_t k = out + __popc(bits & ((1u << lane) - 1u));
+                pair_a[k]        = a;
+                pair_b[k]        = sids[t];
             }
-        }
+            out += __popc(bits);
+        });
     }
 }
 
