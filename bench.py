@@ -216,10 +216,11 @@ def adjoint_box(n, pitch=2.05e-3, margin=1.6e-3, layers=100):
     return (side, side, 2 * margin + (nz - 0.5) * pitch + 0.03)
 
 
-def measure_adjoint(torch, n, steps):
+def measure_adjoint(torch, n, steps, every):
     """Cost of the adjoint against the forward on the sphere bed in FP64:
     the plain forward (one gb_step call of `steps` steps), the checkpointed
-    trajectory's forward, and its backward (segment replays + adjoint steps),
+    trajectory's forward (a checkpoint every `every` steps), and its backward
+    (each segment replayed from its checkpoint, then the adjoint steps),
     each timed with CUDA events on the engine's stream."""
     from grains3dgpu_b200 import adjoint
     scene = scenes.sphere_bed(seed=4, n=n, box=adjoint_box(n))
@@ -240,7 +241,6 @@ def measure_adjoint(torch, n, steps):
     contacts = sim.sys.stats().contacts
     rng = np.random.default_rng(5)
     wts = [torch.tensor(rng.normal(size=(n, 3)), device=dev) for _ in range(3)]
-    every = adjoint.checkpoint_interval(sim, steps)
 
     def run():
         x0 = torch.tensor(scene.transforms[:, 9:], device=dev, requires_grad=True)
@@ -265,7 +265,8 @@ def measure_adjoint(torch, n, steps):
                         "in contact) settling in a closed box, Hooke law etat=3000 muc=0.05, "
                         "first-order explicit, FP64",
             "n_particles": n, "contacts_per_step": int(contacts), "steps": steps,
-            "checkpoint_every": every, "forward_ms_per_step": t_plain,
+            "checkpoint_every": every, "replayed_steps": steps - -(-steps // every),
+            "forward_ms_per_step": t_plain,
             "trajectory_forward_ms_per_step": t_fwd, "backward_ms_per_step": t_bwd,
             "adjoint_over_forward": t_bwd / t_plain}
 
@@ -526,7 +527,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-n", type=int, default=1_000_000)
-    ap.add_argument("--adjoint-steps", type=int, default=10)
+    ap.add_argument("--adjoint-steps", type=int, default=100)
+    ap.add_argument("--adjoint-every", type=int, default=10,
+                    help="checkpoint interval of the adjoint run (its backward replays the rest)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--shape-steps", type=int, default=10)
     ap.add_argument("--no-shapes", action="store_true")
@@ -665,7 +668,7 @@ def main():
 
     adj = None
     if world == 1 and not args.no_adjoint:
-        adj = measure_adjoint(torch, args.adjoint_n, args.adjoint_steps)
+        adj = measure_adjoint(torch, args.adjoint_n, args.adjoint_steps, args.adjoint_every)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

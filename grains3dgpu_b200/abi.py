@@ -161,6 +161,8 @@ ENGINE_API = {
     "rawdata_close": (C.c_int, [C.c_void_p]),
     "save_state": (C.c_int, [_P, C.c_void_p]),
     "load_state": (C.c_int, [_P, C.c_void_p]),
+    "save_contacts": (C.c_int, [_P, C.c_void_p, C.c_int64, _I64]),
+    "load_contacts": (C.c_int, [_P, C.c_void_p]),
 }
 
 

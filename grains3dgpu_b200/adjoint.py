@@ -6,10 +6,13 @@ velocities of the particles and the contact-law parameters (kn, en, etat,
 muc per material-pair law) to the final positions, velocities and angular
 velocities.  The forward pass stores the state every `every` steps; the
 backward pass replays each segment from its checkpoint, keeping the segment's
-states, and runs the adjoint steps backwards through it.  Device memory is
-(n_steps / every + every - 1) states of 18 doubles per particle; with
-every = 1 (the default while the states fit in a quarter of the free device
-memory) nothing is replayed.
+states and the contact set each replayed step found (gb_save_contacts), and
+runs the adjoint steps backwards through it: a replayed step's adjoint takes
+its saved contacts (gb_load_contacts) instead of detecting again, so a
+checkpoint interval costs one forward step per replayed step and no more.
+Device memory is (n_steps / every + every - 1) states of 18 doubles per
+particle plus every - 1 contact sets; with every = 1 (the default while the
+states fit in a quarter of the free device memory) nothing is replayed.
 
 Scope of the adjoint: spheres, the Hooke law with kr = 0, Rectangle walls,
 first-order explicit integration, FP64 (GB_FP64 or GB_FP64_STRICT).  The
@@ -58,6 +61,21 @@ class Simulation:
 
     def load(self, state):
         self._check(self.lib.load_state(self.sys.ctx, C.c_void_p(state.data_ptr())), "load_state")
+
+    def save_contacts(self, buf=None):
+        """The last detect's contact set in a device byte tensor (reused when
+        it is large enough)."""
+        size = C.c_int64(0)
+        self._check(self.lib.save_contacts(self.sys.ctx, None, 0, C.byref(size)), "save_contacts")
+        if buf is None or buf.numel() < size.value:
+            buf = torch.empty(size.value + size.value // 4, dtype=torch.uint8, device=self.dev)
+        self._check(self.lib.save_contacts(self.sys.ctx, C.c_void_p(buf.data_ptr()), buf.numel(),
+                                           C.byref(size)), "save_contacts")
+        return buf
+
+    def load_contacts(self, buf):
+        self._check(self.lib.load_contacts(self.sys.ctx, C.c_void_p(buf.data_ptr())),
+                    "load_contacts")
 
     def set_laws(self, params):
         """params: (n_laws, 4) tensor of kn, en, etat, muc."""
@@ -111,18 +129,26 @@ class Trajectory(torch.autograd.Function):
         grad = torch.zeros(4 * ctx.n_laws, dtype=torch.float64, device=dev)
         seg_states = [torch.empty((18, n), dtype=torch.float64, device=dev)
                       for _ in range(ctx.every - 1)]
+        seg_contacts = [None] * (ctx.every - 1)
         for seg in reversed(range(len(ctx.checkpoints))):
             t0 = seg * ctx.every
             t1 = min(t0 + ctx.every, ctx.n_steps)
-            # the segment's states: its checkpoint, then the replayed steps
+            # the segment's states: its checkpoint, then the replayed steps;
+            # stepping from state t found its contacts, kept for its adjoint
             states = [ctx.checkpoints[seg]]
+            contacts = [None] * (t1 - t0)
             if t1 - t0 > 1:
                 sim.load(states[0])
                 for t in range(t0 + 1, t1):
                     sim.step(1)
-                    states.append(sim.save(seg_states[t - t0 - 1]))
+                    k = t - t0 - 1
+                    seg_contacts[k] = sim.save_contacts(seg_contacts[k])
+                    contacts[k] = seg_contacts[k]
+                    states.append(sim.save(seg_states[k]))
             for t in reversed(range(t0, t1)):
                 sim.load(states[t - t0])
+                if contacts[t - t0] is not None:
+                    sim.load_contacts(contacts[t - t0])
                 sim.adjoint_step(adj, prev, grad)
                 adj, prev = prev, adj
         torch.cuda.synchronize(dev)

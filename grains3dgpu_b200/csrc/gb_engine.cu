@@ -213,6 +213,7 @@ struct gb_ctx
     int64_t             steps_done = 0;
     bool                verlet_started = false;
     bool                links_valid = false, detect_valid = false;
+    bool                contacts_loaded = false; // gb_load_contacts: the next adjoint step's
     gb_stats            last{};
 
     cudaStream_t own_stream = nullptr; // the context's stream (gb_set_stream may replace it)
@@ -1221,6 +1222,7 @@ void restore(gb_ctx* c, const StepSnap& s)
 // and launches the remaining steps again.
 int run_steps(gb_ctx* c, int32_t n_steps, int phases, int32_t* result)
 {
+    c->contacts_loaded = false; // a detect replaces a loaded contact set
     cudaStream_t s    = c->stream;
     const bool   hist = c->cfg.contact_law == GB_LAW_HOOKE_HISTORY;
     int32_t      done = 0;
@@ -1861,6 +1863,61 @@ int gb_load_state(gb_ctx* c, const double* src)
     GB_CK(cudaStreamSynchronize(s));
     c->tr_set = c->vel_set = true;
     c->links_valid = c->detect_valid = c->mask_valid = false;
+    c->contacts_loaded = false;
+    return GB_OK;
+}
+
+// A saved contact set: a 16-byte header (n, pair count as int64), the pair
+// offsets (n + 1 uint32), the partners (uint32 per pair), the contact flags
+// (one byte per pair).
+int gb_save_contacts(gb_ctx* c, void* buf, int64_t capacity, int64_t* size)
+{
+    if(!c || !size || capacity < 0)
+        return GB_E_INVALID_ARG;
+    if(!c->detect_valid)
+        return GB_E_NOT_READY;
+    const int64_t n = c->n, np = c->npairs;
+    const int64_t need = 16 + 4 * (n + 1) + 5 * np;
+    *size = need;
+    if(!buf)
+        return GB_OK;
+    if(capacity < need)
+        return GB_E_CAPACITY;
+    char*         b      = static_cast<char*>(buf);
+    const int64_t hdr[2] = {n, np};
+    cudaStream_t  s      = c->stream;
+    GB_CK(cudaMemcpyAsync(b, hdr, sizeof(hdr), cudaMemcpyHostToDevice, s));
+    GB_CK(cudaMemcpyAsync(b + 16, c->d_off[c->cur], 4 * (size_t)(n + 1),
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(b + 16 + 4 * (n + 1), c->d_pb[c->cur], 4 * (size_t)np,
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(b + 16 + 4 * (n + 1) + 4 * np, c->d_pc, (size_t)np,
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaStreamSynchronize(s));
+    return GB_OK;
+}
+
+int gb_load_contacts(gb_ctx* c, const void* buf)
+{
+    if(!c || !buf)
+        return GB_E_INVALID_ARG;
+    int64_t hdr[2];
+    GB_CK(cudaMemcpy(hdr, buf, sizeof(hdr), cudaMemcpyDeviceToHost));
+    if(hdr[0] != c->n || hdr[1] < 0 || hdr[1] > UINT32_MAX)
+        return GB_E_INVALID_ARG;
+    const int64_t n = c->n, np = hdr[1];
+    GB_TRY(ensure_pairs(c, np));
+    const char*  b = static_cast<const char*>(buf);
+    cudaStream_t s = c->stream;
+    GB_CK(cudaMemcpyAsync(c->d_off[c->cur], b + 16, 4 * (size_t)(n + 1),
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_pb[c->cur], b + 16 + 4 * (n + 1), 4 * (size_t)np,
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaMemcpyAsync(c->d_pc, b + 16 + 4 * (n + 1) + 4 * np, (size_t)np,
+                          cudaMemcpyDeviceToDevice, s));
+    GB_CK(cudaStreamSynchronize(s));
+    c->npairs          = np;
+    c->contacts_loaded = true;
     return GB_OK;
 }
 
@@ -1909,10 +1966,16 @@ int gb_adjoint_step(gb_ctx* c, const double* adj_next, double* adj_prev, double*
                           cudaMemcpyDeviceToDevice, s));
     const bool dirty = c->torce_dirty;
     c->torce_dirty   = false;
-    GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
-    const int st = run_steps(c, 1, PHASE_DETECT, nullptr);
-    if(st != GB_OK && st != GB_E_OUT_OF_DOMAIN)
-        return st;
+    int        st    = GB_OK;
+    if(c->contacts_loaded)
+        c->contacts_loaded = false; // the contacts of this state, saved when it was stepped
+    else
+    {
+        GB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+        st = run_steps(c, 1, PHASE_DETECT, nullptr);
+        if(st != GB_OK && st != GB_E_OUT_OF_DOMAIN)
+            return st;
+    }
     const State<double> state = state_of<double>(c);
     const auto*         in    = (const RBInertia<double>*)c->d_inertia;
     double*             lft   = c->d_adj;

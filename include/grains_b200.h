@@ -255,6 +255,15 @@ int gb_load_state(gb_ctx* ctx, const double* src_device);
  * etat, muc).  The contacts are those found at s; the state and the torces
  * are left as they were. */
 int gb_adjoint_step(gb_ctx* ctx, const double* adj_next, double* adj_prev, double* grad_laws);
+/* The contact set of the last detect (pair list and contact flags), so that a
+ * replayed step's adjoint need not detect again: gb_save_contacts copies it to
+ * `buf` (device memory of `capacity` bytes; NULL only queries) and sets *size
+ * to the bytes it needs (GB_E_CAPACITY when capacity is short); after
+ * gb_load_state of the state that detect was made on, gb_load_contacts puts it
+ * back, and the next gb_adjoint_step uses it instead of detecting.  Any step,
+ * detect or load_state drops a loaded set. */
+int gb_save_contacts(gb_ctx* ctx, void* buf, int64_t capacity, int64_t* size);
+int gb_load_contacts(gb_ctx* ctx, const void* buf);
 
 /* ---- the time step: the ComponentManager hot-path calls ---------------------- */
 /* ComponentManager::updateLinks (ComponentManagerCPU.cpp:278-296). */
