@@ -132,7 +132,20 @@ BED_PITCH = 2.2e-3  # lattice pitch of the bed
 def make_scene(args, rank, workload="bed"):
     if workload == "bed":
         return scenes.polydisperse_bed(seed=replica_seed(rank), n=args.n, pitch=BED_PITCH)
+    if workload == "polyhedra":
+        return scenes.polyhedra_box(n=args.n, hull_centroid=hull_centroid)
+    if workload == "spheres":
+        return scenes.sphere_bed(seed=4, n=args.n, box=adjoint_box(args.n))
     return scenes.polydisperse_superquadrics(seed=replica_seed(rank), n=args.n)
+
+
+def hull_centroid(v):
+    """Centroid of the convex hull of v (the engine's host geometry)."""
+    from grains3dgpu_b200 import engine
+    c, vol = np.zeros(3), abi.C.c_double(0.0)
+    assert engine.load().convex_hull_centroid(abi.dptr(np.ascontiguousarray(v)), v.shape[0],
+                                              abi.dptr(c), abi.C.byref(vol)) == 0
+    return c
 
 
 def aggregate(world, n_per_rank, steps, t_max):
@@ -276,17 +289,9 @@ def measure_shapes(args, torch):
     GPU: 200,000 convex polyhedra (hulls of 8-32 points on an ellipsoid, the
     polyhedra packing) and 1,000,000 spheres (the sphere bed, every lattice
     neighbour in contact)."""
-    from grains3dgpu_b200 import engine
-    lib = engine.load()
-
-    def centroid(v):
-        c, vol = np.zeros(3), abi.C.c_double(0.0)
-        assert lib.convex_hull_centroid(abi.dptr(np.ascontiguousarray(v)), v.shape[0],
-                                        abi.dptr(c), abi.C.byref(vol)) == 0
-        return c
-
     out = {}
-    cases = (("polyhedra_200k", lambda: scenes.polyhedra_box(n=200_000, hull_centroid=centroid)),
+    cases = (("polyhedra_200k", lambda: scenes.polyhedra_box(n=200_000,
+                                                             hull_centroid=hull_centroid)),
              ("spheres_1M", lambda: scenes.sphere_bed(seed=4, n=1_000_000,
                                                       box=adjoint_box(1_000_000))))
     for name, build in cases:
@@ -300,6 +305,10 @@ def measure_shapes(args, torch):
         res["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
         res["n_particles"] = scene.n
         res["candidate_pairs_last_step"] = int(st.candidate_pairs)
+        # the mixed mode's single-step error from the FP64 pose, on (up to)
+        # 200,000 of the packing's grains
+        res["mixed_vs_fp64_single_step"] = force_error(
+            scene.subset(np.arange(min(scene.n, 200_000))), torch)
         out[name] = res
     return out
 
@@ -540,8 +549,10 @@ def main():
                     help="run the headline's warm-up and timed steps only (for profilers)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="with --timed-only: the run mode")
-    ap.add_argument("--workload", default="bed", choices=["bed", "dilute"],
-                    help="with --timed-only: the packing")
+    ap.add_argument("--workload", default="bed",
+                    choices=["bed", "dilute", "polyhedra", "spheres"],
+                    help="with --timed-only: the packing (polyhedra: --n of the 200,000 "
+                         "convex hulls' packing; spheres: the sphere bed)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
