@@ -366,8 +366,24 @@ GB_D Quat<S> quaternion_change(const V3<S>& w, S dt)
     Quat<S> r;
     if(n > k_higheps<S>())
     {
-        const S c = s_cos(n * dt / S(2.0));
-        const S s = s_sin(n * dt / S(2.0));
+        const S h = n * dt / S(2.0);
+        S       c = S(1.0), s = S(0.0);
+        bool    small = false;
+        if constexpr(std::is_same<S, float>::value)
+            if(h < 0.05f)
+            {
+                // FP32: the rotation of a step is small; Taylor to x^5 and
+                // x^4 (the next terms are below 2e-11 of the leading one)
+                const float h2 = h * h;
+                s              = h * (1.0f - h2 * (1.0f / 6.0f) * (1.0f - h2 * 0.05f));
+                c              = 1.0f - h2 * 0.5f * (1.0f - h2 * (1.0f / 12.0f));
+                small          = true;
+            }
+        if(!small)
+        {
+            c = s_cos(h);
+            s = s_sin(h);
+        }
         r.v       = (s / n) * w;
         r.w       = c;
     }

@@ -1692,11 +1692,12 @@ __global__ void __launch_bounds__(128)
 
 // ---- per-particle kernel: segmented sum, gravity, integration -----------------
 // A latency-bound streaming kernel.  Its loads are all issued before the pair
-// loop; holding them takes the mixed instantiation to 64 registers (four
-// 256-thread blocks per SM, which measured faster than five blocks at 48 with
-// spills); the FP64 ones need about 100 registers and get two blocks.
+// loop; the mixed instantiation runs four 256-thread blocks per SM at 64
+// registers with a few spilled (measured 3% faster than three blocks at 79
+// registers without, and than five at 48); the FP64 ones need about 125
+// registers and get two blocks.
 template <typename S>
-__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 4 : 2)
     k_particles(int n, State<store_t<S>> st, Tables<S> tb, const uint32_t* __restrict__ off,
                 PairOut<store_t<S>> po, StepParams<S> sp, int* __restrict__ contacts_out,
                 uint32_t* __restrict__ mask_out, int* __restrict__ flags,
