@@ -87,7 +87,7 @@ class Stats(C.Structure):
                 ("cells_per_dir", C.c_int32 * 3), ("key_bits", C.c_int32),
                 ("cell_size", C.c_double), ("grid_max", C.c_double * 3),
                 ("kernel_launches", C.c_int64), ("gjk_fp64_calls", C.c_int64),
-                ("fine_grid_cells", C.c_int64)]
+                ("fine_grid_cells", C.c_int64), ("obstacle_candidates", C.c_int64)]
 
 
 class Contact(C.Structure):

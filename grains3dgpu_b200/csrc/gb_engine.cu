@@ -165,6 +165,13 @@ struct gb_ctx
     uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
     uint32_t* d_ovf    = nullptr; // particles with more partners than pair slots
     uint32_t* d_pcount = nullptr; // contacts per particle of the step (cleared as read)
+    // obstacles past the mask's 32, binned by linked cell (obstacle_cells)
+    uint32_t* d_cobs_start = nullptr;
+    uint32_t* d_cobs_ids   = nullptr;
+    bool      cobs_valid   = false;
+    bool      cobs_used    = false; // lists built (some obstacle is not a masked wall)
+    std::vector<uint32_t> h_cobs_ids;
+    int64_t   cobs_entries = 0;
     int       ovf_phase = 0;      // which of d_gjkn[2], [3] counts them this step
     uint32_t* d_sorted_of = nullptr; // sorted position of each particle id
     // the finer candidate grid of polydisperse packings (k_pair_count_fine)
@@ -846,6 +853,171 @@ int fine_plan(gb_ctx* c)
     return GB_OK;
 }
 
+// The obstacles that the wall mask does not decide (all but the Rectangles
+// among the first kMaskObstacles), binned by linked cell: an obstacle is
+// listed for every cell from which a particle's surface can reach it, so a
+// particle's candidates are its cell's list (the reference tests
+// every particle against every obstacle, ComponentManagerCPU.cpp:301-351;
+// the contact test is unchanged).  Reach = the largest particle bounding
+// radius plus crust, plus the obstacle's crust; a cell is a box (a boundary
+// cell reaches past the grid, where out-of-domain centres are clamped in).
+// Rectangles are met as their planes (closestPointsRectangle) and drums as
+// their cylinders, both from either side: a cell is listed when its box may
+// come within reach of the plane (separating-axis bound along the normal) or
+// of the cylinder (the radial distance is 1-Lipschitz: its centre's, within
+// the box's half-diagonal); other obstacles by their circumscribed spheres.
+int obstacle_cells(gb_ctx* c)
+{
+    c->cobs_valid = true;
+    c->cobs_used  = false;
+    if(c->props.empty())
+        return GB_OK;
+    auto listed = [&](int o) {
+        return !(o < kMaskObstacles && c->obs[o].convex.type == GB_RECTANGLE);
+    };
+    bool any = false;
+    for(int o = 0; o < c->nob; ++o)
+        any = any || listed(o);
+    if(!any)
+        return GB_OK;
+    const uint32_t nx = c->dims[0], ny = c->dims[1], nz = c->dims[2];
+    const uint32_t dn[3] = {nx, ny, nz};
+    const uint64_t nc = (uint64_t)nx * ny * nz;
+    double         rp = 0.0, cp = 0.0;
+    for(int i = 0; i < c->nrb; ++i)
+    {
+        rp = std::max(rp, bound_radius(c, i));
+        cp = std::max(cp, c->rbs[i].crust_thickness);
+    }
+    const double hd = 0.5 * c->cell * std::sqrt(3.0);
+    // is cell (x, y, z) within reach of obstacle o?
+    auto near = [&](int o, uint32_t x, uint32_t y, uint32_t z) {
+        const double* t      = c->obs_tr.data() + 12 * o;
+        const double  reach  = (rp + cp + c->obs[o].crust_thickness) * (1.0 + 1e-6) + 1e-9;
+        const int     type   = c->obs[o].convex.type;
+        const double  n[3]   = {t[2], t[5], t[8]}; // the frame's z axis
+        const double  org[3] = {t[9], t[10], t[11]};
+        const uint32_t ix[3] = {x, y, z};
+        double         ctr[3], hx[3];
+        bool           unbounded = false;
+        for(int k = 0; k < 3; ++k)
+        {
+            double lo = c->cfg.origin[k] + c->cell * ix[k], hi = lo + c->cell;
+            if(ix[k] == 0)
+                lo = -1e30;
+            if(ix[k] + 1 == dn[k])
+                hi = 1e30;
+            unbounded = unbounded || ix[k] == 0 || ix[k] + 1 == dn[k];
+            ctr[k]    = 0.5 * (lo + hi);
+            hx[k]     = 0.5 * (hi - lo);
+        }
+        if(type == GB_RECTANGLE)
+        {
+            double dc = 0.0, ext = 0.0;
+            for(int k = 0; k < 3; ++k)
+            {
+                dc += n[k] * (ctr[k] - org[k]);
+                ext += std::fabs(n[k]) * hx[k];
+            }
+            return ext > 1e29 || std::fabs(dc) - ext <= reach;
+        }
+        if(unbounded)
+            return true;
+        double d[3], a = 0.0, r2 = 0.0;
+        for(int k = 0; k < 3; ++k)
+        {
+            d[k] = ctr[k] - org[k];
+            a += n[k] * d[k];
+        }
+        if(type == GB_DRUM)
+        {
+            for(int k = 0; k < 3; ++k)
+                r2 += (d[k] - a * n[k]) * (d[k] - a * n[k]);
+            return std::fabs(std::sqrt(r2) - c->obs[o].convex.p[0]) <= reach + hd;
+        }
+        return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+               <= c->obs_props[o].circumscribed_radius + reach + hd;
+    };
+    // the cells worth testing: all for planes and drums, the box of the
+    // circumscribed sphere plus reach for the others
+    auto range = [&](int o, uint32_t lo[3], uint32_t hi[3]) {
+        const int type = c->obs[o].convex.type;
+        for(int k = 0; k < 3; ++k)
+        {
+            lo[k] = 0;
+            hi[k] = dn[k] - 1;
+        }
+        if(type == GB_RECTANGLE || type == GB_DRUM)
+            return;
+        const double* t = c->obs_tr.data() + 12 * o;
+        const double  r = c->obs_props[o].circumscribed_radius
+                         + (rp + cp + c->obs[o].crust_thickness) * 1.01 + c->cell;
+        for(int k = 0; k < 3; ++k)
+        {
+            const double a = std::floor((t[9 + k] - r - c->cfg.origin[k]) / c->cell);
+            const double b = std::floor((t[9 + k] + r - c->cfg.origin[k]) / c->cell);
+            lo[k] = a <= 0.0 ? 0u : (a >= dn[k] - 1.0 ? dn[k] - 1 : (uint32_t)a);
+            hi[k] = b <= 0.0 ? 0u : (b >= dn[k] - 1.0 ? dn[k] - 1 : (uint32_t)b);
+        }
+    };
+    // two passes over the listed obstacles in ascending order: counts per
+    // cell, then the lists at their offsets
+    std::vector<uint32_t> start(nc + 1, 0u);
+    for(int pass = 0; pass < 2; ++pass)
+    {
+        std::vector<uint32_t> fill;
+        if(pass == 1)
+        {
+            uint64_t run = 0;
+            for(uint64_t k = 0; k < nc; ++k)
+            {
+                const uint64_t m = start[k];
+                start[k]         = (uint32_t)run;
+                run += m;
+            }
+            if(run > 0xFFFFFFFFull)
+                return GB_OK; // too many entries for 32-bit offsets: every such obstacle
+                              // stays a candidate of every particle
+            start[nc] = (uint32_t)run;
+            fill.assign(start.begin(), start.end() - 1);
+        }
+        std::vector<uint32_t>& ids = c->h_cobs_ids;
+        if(pass == 1)
+            ids.assign(start[nc], 0u);
+        for(int o = 0; o < c->nob; ++o)
+        {
+            if(!listed(o))
+                continue;
+            uint32_t lo[3], hi[3];
+            range(o, lo, hi);
+            for(uint32_t z = lo[2]; z <= hi[2]; ++z)
+                for(uint32_t y = lo[1]; y <= hi[1]; ++y)
+                    for(uint32_t x = lo[0]; x <= hi[0]; ++x)
+                        if(near(o, x, y, z))
+                        {
+                            const uint64_t k = ((uint64_t)z * ny + y) * nx + x;
+                            if(pass == 0)
+                                ++start[k];
+                            else
+                                ids[fill[k]++] = (uint32_t)o;
+                        }
+        }
+    }
+    const std::vector<uint32_t>& ids = c->h_cobs_ids;
+    dfree(c->d_cobs_start);
+    dfree(c->d_cobs_ids);
+    GB_TRY(dalloc(&c->d_cobs_start, start.size()));
+    GB_TRY(dalloc(&c->d_cobs_ids, std::max<size_t>(ids.size(), 1)));
+    GB_CK(cudaMemcpy(c->d_cobs_start, start.data(), start.size() * sizeof(uint32_t),
+                     cudaMemcpyHostToDevice));
+    if(!ids.empty())
+        GB_CK(cudaMemcpy(c->d_cobs_ids, ids.data(), ids.size() * sizeof(uint32_t),
+                         cudaMemcpyHostToDevice));
+    c->cobs_entries = (int64_t)ids.size();
+    c->cobs_used    = true;
+    return GB_OK;
+}
+
 // candidate pairs (particles, then obstacles): count -> scan -> fill, with no
 // host round trip: the total stays on the device (off[n]); a total beyond the
 // capacity aborts the step (kFlagCapacity) and the host replays it larger
@@ -878,6 +1050,15 @@ int build_pairs(gb_ctx* c)
     geo.rmax = c->rmax;
     if(!c->fine_planned)
         GB_TRY(fine_plan(c));
+    if(!c->cobs_valid)
+        GB_TRY(obstacle_cells(c));
+    ObsCand oc;
+    oc.mask       = c->d_obsmask_id;
+    oc.n          = c->nob;
+    oc.rect       = c->obs_rect;
+    oc.cell_start = c->cobs_used ? c->d_cobs_start : nullptr;
+    oc.cell_ids   = c->d_cobs_ids;
+    oc.skeys      = c->d_skeys;
     if(c->fine)
     {
         // the finer grid of the small particles, then the count passes
@@ -903,22 +1084,19 @@ int build_pairs(gb_ctx* c)
                      (const uint32_t*)c->d_fstart, g, (const uint32_t*)c->d_fskey,
                      (const uint32_t*)c->d_fids, (const uint32_t*)c->d_fref,
                      (const double4*)c->d_fpos, (const float4*)f32, c->d_count,
-                     c->d_count + n + 1, c->d_slot, (const uint32_t*)c->d_obsmask_id, c->nob,
-                     (const int*)c->d_flags));
+                     c->d_count + n + 1, c->d_slot, oc, (const int*)c->d_flags));
         const int nbl = std::max(1, blocks((int64_t)c->fine_nlarge * 32, kBlock));
         GB_CK(launch(c->pdl, k_pair_count_large<S>, nbl, kBlock, s, n,
                      (const uint32_t*)c->d_fstart, g, (const uint32_t*)c->d_fids,
                      (const uint32_t*)c->d_fref, (const double4*)c->d_fpos, (const float4*)f32,
-                     c->d_count, c->d_count + n + 1, c->d_slot, (const uint32_t*)c->d_obsmask_id,
-                     c->nob, (const int*)c->d_flags));
+                     c->d_count, c->d_count + n + 1, c->d_slot, oc, (const int*)c->d_flags));
         c->launches += 4;
     }
     else
     {
         GB_CK(launch(c->pdl, k_pair_count<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids,
                      c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], geo,
-                     c->d_count, c->d_count + n + 1, c->d_slot, c->d_obsmask_id, c->nob,
-                     (const int*)c->d_flags));
+                     c->d_count, c->d_count + n + 1, c->d_slot, oc, (const int*)c->d_flags));
         c->launches += 1;
     }
     GB_CK(cudaGetLastError());
@@ -927,7 +1105,7 @@ int build_pairs(gb_ctx* c)
     c->ovf_phase ^= 1;
     GB_CK(launch(c->pdl, k_pair_fill<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_sorted_of,
                  c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
-                 c->d_slot, c->d_obsmask_id, c->nob, off, c->d_pa, c->d_pb[c->cur], c->cap,
+                 c->d_slot, oc, off, c->d_pa, c->d_pb[c->cur], c->cap,
                  c->d_flags, c->d_gjkn, c->d_count + n + 1, c->d_ovf, c->ovf_phase));
     c->count_zero = true; // the fill pass zeroes each count it reads
     GB_CK(launch(c->pdl, k_pair_fill_overflow<S>, 4 * c->sms, 128, s,
@@ -1439,7 +1617,8 @@ int gb_destroy(gb_ctx* c)
                     c->d_contacts,
                     c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn,
                     c->d_fkey, c->d_fcount, c->d_fstart, c->d_fskey, c->d_fids, c->d_fref,
-                    c->d_fpos, c->d_fpos32, c->d_ovf, c->d_pcount};
+                    c->d_fpos, c->d_fpos32, c->d_ovf, c->d_pcount, c->d_cobs_start,
+                    c->d_cobs_ids};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);
@@ -1504,6 +1683,7 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
         return GB_E_INVALID_ARG;
     c->rbs.assign(rbs, rbs + c->nrb);
     c->fine_planned = false;
+    c->cobs_valid   = false; // the cell size may change
     c->verts.assign(vertices, vertices + 3 * n_vertices);
     c->props.resize(c->nrb);
     double rmax = 0.0;
@@ -1624,6 +1804,7 @@ int gb_set_obstacles(gb_ctx* c, const gb_rigid_body_desc* obst, const double* tr
         return st;
     c->obs_set    = true;
     c->mask_valid = false;
+    c->cobs_valid = false;
     return GB_OK;
 }
 
@@ -2042,9 +2223,10 @@ int gb_get_stats(gb_ctx* c, gb_stats* o)
             ko += pc[p] == kContactObstacle;
             obs += (pb[p] & kObstacleBit) != 0;
         }
-        o->contacts          = k;
-        o->obstacle_contacts = ko; // of the last step, as the particle contacts
-        o->candidate_pairs   = c->npairs - obs;
+        o->contacts            = k;
+        o->obstacle_contacts   = ko; // of the last step, as the particle contacts
+        o->candidate_pairs     = c->npairs - obs;
+        o->obstacle_candidates = obs;
     }
     o->status_flags = c->last.status_flags;
     o->n_cells      = (int32_t)c->ncells;

@@ -52,12 +52,12 @@ struct Tables
 // ---- mixed precision narrow phase --------------------------------------------
 // The bounding-sphere and OBB tests run in FP32 on FP32 poses (their margins
 // are absolute: LOWEPS on the OBB axes, the crust-free bounding box), and every
-// pair that survives them is solved by the FP64 GJK of the FP64 mode, with
-// FP64 shape tables and the compensated quaternion: FP32 support points on
-// mm-size grains carry ~1e-10 m of rounding, the order of a resting contact's
-// overlap (m g / kn ~ 1e-8 m), so contact points and overlaps come from FP64.
-// (An FP32 GJK as a rejection stage before the FP64 solve measured slower than
-// the FP64 solve alone once its supports took the log-domain form.)
+// pair that survives them and that the FP32 stages (GJK's first iteration, the
+// FP32 GJK) do not certify as separated is solved by the FP64 GJK of the FP64
+// mode, with FP64 shape tables and the compensated quaternion: FP32 support
+// points on mm-size grains carry ~1e-10 m of rounding, the order of a resting
+// contact's overlap (m g / kn ~ 1e-8 m), so contact points and overlaps come
+// from FP64.
 
 GB_D Quat<double> load_quat64(const State<float>& st, uint32_t i)
 {
@@ -325,9 +325,67 @@ __global__ void __launch_bounds__(kBlock)
     mask[i] = obstacle_mask_at<S>(tb, st.rb_id[i], [&] { return load_rot<S>(st, i); }, xa);
 }
 
-GB_D int obstacle_candidates(uint32_t mask, int n_obs)
+// A particle's obstacle candidates, in ascending obstacle order (the order of
+// the reference's obstacle loop, ComponentManagerCPU.cpp:301-351).  The
+// Rectangles among the first kMaskObstacles are decided by the particle's
+// mask (walls within reach after the last move); every other obstacle comes
+// from its linked cell's list -- the obstacles whose surface a particle of
+// that cell may reach, binned on the host when the obstacles are set.
+// Without lists (every obstacle a Rectangle among the first 32, or none) the
+// mask decides alone; its bits of the other first-32 obstacles are set.
+struct ObsCand
 {
-    return __popc(mask) + (n_obs > kMaskObstacles ? n_obs - kMaskObstacles : 0);
+    const uint32_t* mask;       // by particle id
+    int             n;          // obstacles
+    uint32_t        rect;       // bit o: obstacle o (< 32) is a Rectangle
+    const uint32_t* cell_start; // C + 1 offsets into cell_ids, by linked cell (or null)
+    const uint32_t* cell_ids;   // the listed obstacles, ascending per cell
+    const uint32_t* skeys;      // linked-cell key by sorted position
+};
+
+GB_D int obstacle_candidates(const ObsCand& oc, uint32_t a, uint32_t s)
+{
+    if(!oc.n)
+        return 0;
+    if(oc.cell_start)
+    {
+        const uint32_t key = oc.skeys[s];
+        return __popc(oc.mask[a] & oc.rect) + (int)(oc.cell_start[key + 1] - oc.cell_start[key]);
+    }
+    return __popc(oc.mask[a]) + (oc.n > kMaskObstacles ? oc.n - kMaskObstacles : 0);
+}
+
+template <typename Visit>
+GB_D void for_each_obstacle_candidate(const ObsCand& oc, uint32_t a, uint32_t s, Visit&& visit)
+{
+    if(!oc.n)
+        return;
+    uint32_t mask = oc.mask[a];
+    if(oc.cell_start)
+    {
+        // the mask's Rectangles merged into the cell's list, both ascending
+        mask &= oc.rect;
+        const uint32_t key = oc.skeys[s];
+        for(uint32_t k = oc.cell_start[key]; k < oc.cell_start[key + 1]; ++k)
+        {
+            const uint32_t o = oc.cell_ids[k];
+            while(mask && (uint32_t)(__ffs(mask) - 1) < o)
+            {
+                visit((uint32_t)(__ffs(mask) - 1));
+                mask &= mask - 1u;
+            }
+            visit(o);
+        }
+        for(; mask; mask &= mask - 1u)
+            visit((uint32_t)(__ffs(mask) - 1));
+        return;
+    }
+    const int nm = oc.n < kMaskObstacles ? oc.n : kMaskObstacles;
+    for(int o = 0; o < nm; ++o)
+        if((mask >> o) & 1u)
+            visit((uint32_t)o);
+    for(int o = kMaskObstacles; o < oc.n; ++o)
+        visit((uint32_t)o);
 }
 
 template <typename S>
@@ -464,18 +522,17 @@ __global__ void __launch_bounds__(kBlock, sizeof(store_t<S>) == 4 ? 8 : 6)
                  const double4* __restrict__ spos, const float4* __restrict__ spos32,
                  const uint32_t* __restrict__ cstart, uint32_t nx, uint32_t ny, uint32_t nz,
                  CellGeometry geo, uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
-                 uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id, int n_obs,
-                 const int* abort_flags)
+                 uint32_t* __restrict__ slot, ObsCand oc, const int* abort_flags)
 {
     grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
     const int      s      = blockIdx.x * blockDim.x + threadIdx.x;
     if(s >= n || step_aborted(abort_flags))
         return;
-    if(n_obs)
+    if(oc.n)
     {
         const uint32_t a   = sids[s];
-        const int      obs = obstacle_candidates(mask_by_id[a], n_obs);
+        const int      obs = obstacle_candidates(oc, a, (uint32_t)s);
         if(obs)
             atomicAdd(count + a, (uint32_t)obs);
     }
@@ -678,8 +735,7 @@ __global__ void __launch_bounds__(kBlock, 6)
                       const uint32_t* __restrict__ fref, const double4* __restrict__ fpos,
                       const float4* __restrict__ fpos32, uint32_t* __restrict__ count,
                       uint32_t* __restrict__ pslot, uint32_t* __restrict__ slot,
-                      const uint32_t* __restrict__ mask_by_id, int n_obs,
-                      const int* abort_flags)
+                      ObsCand oc, const int* abort_flags)
 {
     grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
@@ -687,14 +743,14 @@ __global__ void __launch_bounds__(kBlock, 6)
     const uint32_t nx = g.nx, ny = g.ny, nz = g.nz;
     if(f >= n || step_aborted(abort_flags) || (uint32_t)f >= fstart[nx * ny * nz])
         return;
-    const uint32_t a = fids[f];
-    if(n_obs)
+    const uint32_t a = fids[f], sa = fref[f];
+    if(oc.n)
     {
-        const int obs = obstacle_candidates(mask_by_id[a], n_obs);
+        const int obs = obstacle_candidates(oc, a, sa);
         if(obs)
             atomicAdd(count + a, (uint32_t)obs);
     }
-    const uint32_t key = fskey[f], sa = fref[f];
+    const uint32_t key = fskey[f];
     const double4  pa  = fpos[f];
     float4         pa32;
     if constexpr(PRE32)
@@ -731,8 +787,7 @@ __global__ void __launch_bounds__(kBlock)
                        const uint32_t* __restrict__ fids, const uint32_t* __restrict__ fref,
                        const double4* __restrict__ fpos, const float4* __restrict__ fpos32,
                        uint32_t* __restrict__ count, uint32_t* __restrict__ pslot,
-                       uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
-                       int n_obs, const int* abort_flags)
+                       uint32_t* __restrict__ slot, ObsCand oc, const int* abort_flags)
 {
     grid_dep_sync();
     constexpr bool STRICT = is_strict<S>(), PRE32 = is_mixed<S>();
@@ -742,9 +797,9 @@ __global__ void __launch_bounds__(kBlock)
     if(f >= n || step_aborted(abort_flags)) // warp-uniform
         return;
     const uint32_t a = fids[f], sa = fref[f];
-    if(n_obs && lane == 0)
+    if(oc.n && lane == 0)
     {
-        const int obs = obstacle_candidates(mask_by_id[a], n_obs);
+        const int obs = obstacle_candidates(oc, a, sa);
         if(obs)
             atomicAdd(count + a, (uint32_t)obs);
     }
@@ -827,8 +882,8 @@ __global__ void __launch_bounds__(kBlock)
                 const uint32_t* __restrict__ sorted_of, const double4* __restrict__ spos,
                 const float4* __restrict__ spos32, const uint32_t* __restrict__ cstart,
                 uint32_t nx, uint32_t ny, uint32_t nz, uint32_t* __restrict__ count,
-                const uint32_t* __restrict__ slot, const uint32_t* __restrict__ mask_by_id,
-                int n_obs, const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
+                const uint32_t* __restrict__ slot, ObsCand oc,
+                const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
                 uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot,
                 uint32_t* __restrict__ ovf_list, int ovf_phase)
@@ -861,8 +916,7 @@ __global__ void __launch_bounds__(kBlock)
     // leaves them for the host's memset before its replay)
     count[a] = 0u;
     pslot[s] = 0u;
-    const uint32_t mask = n_obs ? mask_by_id[a] : 0u;
-    const uint32_t cp   = c - (uint32_t)obstacle_candidates(mask, n_obs);
+    const uint32_t cp = c - (uint32_t)obstacle_candidates(oc, a, (uint32_t)s);
     if(cp <= kPairSlots)
     {
         // the slots in registers (unused ones as 0xffffffff, above every
@@ -907,13 +961,11 @@ __global__ void __launch_bounds__(kBlock)
         ovf_list[atomicAdd(gjk_count + 2 + ovf_phase, 1u)] = (uint32_t)a;
         out += cp;
     }
-    for(int o = 0; o < n_obs; ++o)
-        if(o >= kMaskObstacles || ((mask >> o) & 1u))
-        {
-            pair_a[out] = a;
-            pair_b[out] = kObstacleBit | (uint32_t)o;
-            ++out;
-        }
+    for_each_obstacle_candidate(oc, a, (uint32_t)s, [&](uint32_t o) {
+        pair_a[out] = a;
+        pair_b[out] = kObstacleBit | o;
+        ++out;
+    });
 }
 
 // The particle pairs of the particles whose partners overflowed their slots,

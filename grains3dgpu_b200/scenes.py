@@ -363,6 +363,42 @@ def sphere_bed(seed=1, n=60, box=(0.009, 0.009, 0.016), pitch=2.05e-3, sink=0.55
     return scene
 
 
+def peg_board(seed=7, n=2000, pegs=64, box=(0.03, 0.03, 0.03), pitch=2.05e-3):
+    """Spheres of radius 1.1 mm among fixed spherical pegs of the same size
+    (obstacles of density 0), all on one 2.05 mm jittered lattice, so that
+    every grain next to a peg touches it from the first step; the six box
+    walls are obstacles 0-5 and the pegs 6 onwards, past the 32 that the
+    per-particle wall mask covers: the obstacles the linked-cell bins serve."""
+    rng = np.random.default_rng(seed)
+    pos, _ = lattice(box, pitch, 1.2e-3, n + pegs, rng, 0.05e-3)
+    pick = rng.permutation(n + pegs)
+    peg_pos, grain_pos = pos[pick[:pegs]], pos[pick[pegs:]]
+    rbs = np.zeros(1, RB_DTYPE)
+    rbs[0]["type"] = abi.GB_SPHERE
+    rbs[0]["p"][0] = 1.1e-3
+    rbs[0]["crust"] = 5e-5
+    rbs[0]["density"] = 2500.0
+    walls, wtr = box_walls(box)
+    pdesc = np.zeros(pegs, RB_DTYPE)
+    pdesc["type"] = abi.GB_SPHERE
+    pdesc["p"][:, 0] = 1.1e-3
+    pdesc["crust"] = 5e-5
+    pdesc["material"] = 1
+    ptr = np.zeros((pegs, 12))
+    ptr[:, [0, 4, 8]] = 1.0
+    ptr[:, 9:] = peg_pos
+    tr = np.zeros((n, 12))
+    tr[:, :9] = random_rotations(rng, n)
+    tr[:, 9:] = grain_pos
+    vel = np.zeros((n, 6))
+    vel[:, :3] = rng.normal(0.0, 0.05, size=(n, 3))
+    cfg = dict(n_particles=n, n_rigid_bodies=1, n_obstacles=6 + pegs, n_materials=2,
+               origin=(0, 0, 0), max_coordinate=box, dt=2e-6, gravity=(0, 0, -9.81))
+    return Scene("peg_board", cfg, rbs, np.zeros((0, 3)), np.zeros(n, np.uint32), tr, vel,
+                 np.concatenate([walls, pdesc]), np.concatenate([wtr, ptr]), [law()] * 3,
+                 notes=f"{n} spheres among {pegs} pegs")
+
+
 def cube_collision(seed=6, speed=0.4, gap=0.1e-3, tilt=0.1, shape="polyhedron"):
     """Two cubes of the drum's kind (edge 1.6 mm, crust 0.04 mm, density 2500;
     convex polyhedra of 8 vertices, or boxes) meeting head on along x at a

@@ -189,6 +189,8 @@ typedef struct gb_stats {
                                 FP32 stage leaves open; otherwise gjk_calls) */
     int64_t fine_grid_cells; /* cells of the finer candidate grid of a polydisperse packing
                                 (0: candidates from the linked cells alone) */
+    int64_t obstacle_candidates; /* particle-obstacle records of the last detect (the obstacles
+                                    past the first 32 come from linked-cell bins) */
 } gb_stats;
 
 /* ---- debug dump kinds -------------------------------------------------------- */
