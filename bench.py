@@ -313,6 +313,60 @@ def measure_shapes(args, torch):
     return out
 
 
+def full_length(args, torch):
+    """Long runs, each in one gb_step call from its generated state, with the
+    signed-volume GJK and crust-inclusive bounding tests (with the
+    reference's GJK-JH, which misses most contacts of mm grains, grains pass
+    into one another and every one of these runs goes non-finite): the 2,000
+    superquadrics of the column configuration as a five-layer bed (2.7 mm
+    pitch, 60 x 60 x 30 mm; at the stated 2.4 mm pitch randomly oriented
+    grains start with intersecting cores) for its 20,000 steps of 2e-6 s
+    (FP64 and mixed); the 200,000 polyhedra for their 50,000 steps of 1e-6 s
+    (mixed and FP64); the 1,000,000-grain bed for 20,000 of its 100,000
+    steps (mixed).  Per run: ms per step, the status, whether the state
+    stayed finite, the contacts of the last step and the mean height."""
+    from grains3dgpu_b200 import engine
+    lib = engine.load()
+
+    def run(scene, prec, steps):
+        s = scenes.System(lib, scene, precision=prec, device=torch.cuda.current_device(),
+                          contact_law=LAW, gjk_variant=abi.GB_GJK_SV,
+                          flags=abi.GB_FLAG_CRUST_BOUNDS)
+        stream = torch.cuda.current_stream()
+        assert lib.set_stream(s.ctx, abi.C.c_void_p(stream.cuda_stream)) == 0
+        # chunks of 1,000 steps, until the steps, a failed step or the cap
+        el, status = 0.0, 0
+        while s.stats().steps_done < steps and el < args.full_length_cap and status == 0:
+            k = int(min(1000, steps - s.stats().steps_done))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            status = lib.step(s.ctx, k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            el += e0.elapsed_time(e1) / 1e3
+            status = 0 if status == abi.GB_E_OUT_OF_DOMAIN else status
+        st, tr = s.stats(), s.transforms()
+        s.close()
+        return {"steps": steps, "status": engine.status_string(status) if status else "ok",
+                "steps_done": int(st.steps_done), "ms_per_step": el / max(st.steps_done, 1) * 1e3,
+                "finite": bool(np.isfinite(tr).all()), "contacts_last_step": int(st.contacts),
+                "wall_contacts_last_step": int(st.obstacle_contacts),
+                "mean_height_m": float(np.nanmean(tr[:, 11]))}
+    out = {"full_length": True, "law": "tangential-history",
+           "gjk": "signed volume, crust-inclusive bounding tests"}
+    col = scenes.superquadric_column(n=2000, pitch=2.7e-3, jitter=0.03e-3,
+                                     box=(0.060, 0.060, 0.030))
+    out["column_2000"] = {"fp64": run(col, abi.GB_FP64, 20_000),
+                          "mixed": run(col, abi.GB_MIXED, 20_000)}
+    poly = scenes.polyhedra_box(n=200_000, hull_centroid=hull_centroid)
+    out["polyhedra_200k"] = {"mixed": run(poly, abi.GB_MIXED, 50_000),
+                             "fp64": run(poly, abi.GB_FP64, 50_000)}
+    bed = scenes.polydisperse_bed(seed=replica_seed(0), n=1_000_000, pitch=BED_PITCH)
+    out["bed_1M"] = {"mixed": run(bed, abi.GB_MIXED, 20_000)}
+    return out
+
+
 def measure_drum(args, torch):
     """The rotating-drum configuration (scenes.rotating_drum): 2,000,000 grains
     (40% spheres, 30% cubes as polyhedra, 30% n = 6 superquadrics) in a drum
@@ -545,6 +599,10 @@ def main():
     ap.add_argument("--no-dilute", action="store_true")
     ap.add_argument("--drum-n", type=int, default=2_000_000)
     ap.add_argument("--drum-steps", type=int, default=5000)
+    ap.add_argument("--full-length", action="store_true",
+                    help="run the configurations at their full lengths instead (one JSON line)")
+    ap.add_argument("--full-length-cap", type=float, default=120.0,
+                    help="with --full-length: seconds of device time per run at most")
     ap.add_argument("--timed-only", action="store_true",
                     help="run the headline's warm-up and timed steps only (for profilers)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
@@ -566,6 +624,13 @@ def main():
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.full_length:
+        if rank == 0:
+            print(json.dumps(full_length(args, torch)))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
 
     if args.timed_only:
         scene = make_scene(args, rank, args.workload)

@@ -1,5 +1,5 @@
-"""Long-run statistics.  The mixed mode against the FP64 mode: 10,000
-superquadrics falling in a column onto a plate for 5,000 steps (10 ms), with
+"""Long-run statistics.  The mixed mode against the FP64 mode: 10,000 and
+100,000 superquadrics falling in a column onto a plate for 5,000 steps (10 ms), with
 the tangential-history law.  Trajectories of individual grains separate
 slowly (contact events amplify rounding), so the check is on the ensemble:
 mean height, translational and rotational kinetic energy, and the number of
@@ -38,8 +38,9 @@ def _run(gb, scene, precision, blocks=5, steps=1000):
     return out
 
 
-def test_mixed_statistics_follow_fp64(gb):
-    scene = scenes.superquadric_column_on_plate(n=10_000)
+@pytest.mark.parametrize("n", [10_000, 100_000])
+def test_mixed_statistics_follow_fp64(gb, n):
+    scene = scenes.superquadric_column_on_plate(n=n)
     ref = _run(gb, scene, abi.GB_FP64)
     mix = _run(gb, scene, abi.GB_MIXED)
     assert max(r["walls"] for r in ref) > 0  # the column does reach the plate
