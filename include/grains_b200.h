@@ -320,12 +320,11 @@ int gb_get_phase_times(gb_ctx* ctx, double* ms, int64_t* steps, int32_t reset);
  *   sorted_ids  device, n uint32: particle ids sorted by (cell, id)
  *   cell_start  device, dims[0]*dims[1]*dims[2]+1 uint32
  *   stream      cudaStream_t (NULL: the legacy default stream)
- * Returns GB_E_CAPACITY when n exceeds 262,144.  The first call on a device
- * looks up the scratch's device address (one cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the scratch: calls
- * whose work overlaps on the GPU race and must be serialised by the caller.
- * The call synchronises `stream` to report GB_E_OUT_OF_DOMAIN /
- * GB_E_NONFINITE like gb_update_links. */
+ * Returns GB_E_CAPACITY when n exceeds 262,144.  Every call synchronises
+ * `stream` to report GB_E_OUT_OF_DOMAIN / GB_E_NONFINITE like gb_update_links,
+ * so no call may be made while the stream is being captured into a CUDA
+ * graph.  All calls share the scratch: calls whose work overlaps on the GPU
+ * race and must be serialised by the caller. */
 int gb_linked_cell_sort_static(const double* pos, int32_t n, const double origin[3],
                                double cell_size, const int32_t dims[3], uint32_t* sorted_ids,
                                uint32_t* cell_start, void* stream);
