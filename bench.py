@@ -807,14 +807,14 @@ def main():
 # beside the other profiles.  Their traffic scales with the particle count
 # at the bed's density.  Writes that stay in L2 when the kernel ends are not
 # counted by the capture.
-TRAFFIC_PER_PARTICLE = {"integration": (95.36e6 + 8.02e6) / 600_000,
+TRAFFIC_PER_PARTICLE = {"integration": (95.4e6 + 12.2e6) / 600_000,
                         "broad_phase": (14.48e6 + 2.56e6 + 26.54e6 + 0.06e6) / 600_000}
 
 
 # what bounds each stage or phase, from the same captures and those of the bed
 # at 200,000 grains
-LIMITER = {"integration": "issue and memory latency: 28% warps active (79 registers, three "
-                          "256-thread blocks per SM), 38% issue slots; 172 B per particle "
+LIMITER = {"integration": "issue and memory latency: 40% warps active (64 registers, four "
+                          "256-thread blocks per SM), 42% issue slots; 159 B per particle "
                           "read from DRAM",
            "broad_phase": "launch and tail latency of short dependent passes (hash 10 us, "
                           "scan, scatter 9 us, rank 20 us at 600k grains); 73 B per particle "
