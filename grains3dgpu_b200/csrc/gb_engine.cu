@@ -883,6 +883,9 @@ int obstacle_cells(gb_ctx* c)
     const uint32_t nx = c->dims[0], ny = c->dims[1], nz = c->dims[2];
     const uint32_t dn[3] = {nx, ny, nz};
     const uint64_t nc = (uint64_t)nx * ny * nz;
+    if(nc > (1ull << 28))
+        return GB_OK; // a grid too large to bin on the host: those obstacles stay
+                      // candidates of every particle
     double         rp = 0.0, cp = 0.0;
     for(int i = 0; i < c->nrb; ++i)
     {
