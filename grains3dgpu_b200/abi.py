@@ -163,6 +163,7 @@ ENGINE_API = {
     "load_state": (C.c_int, [_P, C.c_void_p]),
     "save_contacts": (C.c_int, [_P, C.c_void_p, C.c_int64, _I64]),
     "load_contacts": (C.c_int, [_P, C.c_void_p]),
+    "set_integrator_phase": (C.c_int, [_P, C.c_int32]),
 }
 
 

@@ -15,8 +15,9 @@ particle plus every - 1 contact sets; with every = 1 (the default while the
 states fit in a quarter of the free device memory) nothing is replayed.
 
 Scope of the adjoint: spheres, the Hooke law with kr = 0, Rectangle walls,
-first-order explicit integration, FP64 (GB_FP64 or GB_FP64_STRICT).  The
-contacts of each step are those found at its start.
+first-order explicit or velocity-Verlet integration (a trajectory starts with
+the leapfrog's half kick), FP64 (GB_FP64 or GB_FP64_STRICT).  The contacts
+of each step are those found at its start.
 """
 import ctypes as C
 
@@ -35,10 +36,10 @@ def _dp(t):
 class Simulation:
     """One engine context for a scene, with device-side state access."""
 
-    def __init__(self, scene, precision=abi.GB_FP64, device=0):
+    def __init__(self, scene, precision=abi.GB_FP64, device=0, **config):
         self.lib = engine.load()
         self.scene = scene
-        self.sys = scenes.System(self.lib, scene, precision=precision, device=device)
+        self.sys = scenes.System(self.lib, scene, precision=precision, device=device, **config)
         self.n = scene.n
         self.laws = [dict(m) for m in scene.contact_models]
         self.dev = torch.device("cuda", device)
@@ -88,6 +89,12 @@ class Simulation:
     def step(self, k=1):
         self._check(self.lib.step(self.sys.ctx, k), "step")
 
+    def set_phase(self, started):
+        """Velocity Verlet: whether the next step is past a trajectory's first
+        (a full kick) or its first (a half kick)."""
+        self._check(self.lib.set_integrator_phase(self.sys.ctx, 1 if started else 0),
+                    "set_integrator_phase")
+
     def adjoint_step(self, adj_next, adj_prev, grad_laws):
         self._check(self.lib.adjoint_step(self.sys.ctx, _dp(adj_next), _dp(adj_prev),
                                           _dp(grad_laws)), "adjoint_step")
@@ -108,6 +115,7 @@ class Trajectory(torch.autograd.Function):
         state[12:15] = v0.detach().T
         state[15:18] = w0.detach().T
         sim.load(state)
+        sim.set_phase(False)  # the trajectory's first step (velocity Verlet's half kick)
         checkpoints = []
         for t in range(n_steps):
             if t % every == 0:
@@ -139,6 +147,7 @@ class Trajectory(torch.autograd.Function):
             contacts = [None] * (t1 - t0)
             if t1 - t0 > 1:
                 sim.load(states[0])
+                sim.set_phase(t0 > 0)
                 for t in range(t0 + 1, t1):
                     sim.step(1)
                     k = t - t0 - 1
@@ -147,6 +156,7 @@ class Trajectory(torch.autograd.Function):
                     states.append(sim.save(seg_states[k]))
             for t in reversed(range(t0, t1)):
                 sim.load(states[t - t0])
+                sim.set_phase(t > 0)
                 if contacts[t - t0] is not None:
                     sim.load_contacts(contacts[t - t0])
                 sim.adjoint_step(adj, prev, grad)

@@ -141,10 +141,14 @@ GB_D void sphere_pair_vjp(const V3<double>& xa, const V3<double>& xb, double rA,
 
 // integration: x' = x + dt v, v' = v + dt F/m, omega' = omega + dt T/I
 __global__ void __launch_bounds__(kBlock)
-    k_adj_integrate(int n, double dt, State<double> st, const RBInertia<double>* __restrict__ in,
+    k_adj_integrate(int n, double dt, double h, int verlet, State<double> st,
+                    const RBInertia<double>* __restrict__ in,
                     const double* __restrict__ adj_next, double* __restrict__ adj_prev,
                     double* __restrict__ lft)
 {
+    // FirstOrderExplicit: x' = x + dt v, v' = v + dt F/m, w' = w + dt T/I;
+    // velocity Verlet (leapfrog): v' = v + h F/m, x' = x + dt v', w' = w + h T/I,
+    // with h = dt/2 on a trajectory's first step and dt after it
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= n)
         return;
@@ -158,8 +162,8 @@ __global__ void __launch_bounds__(kBlock)
         adj_prev[(size_t)k * n + i]       = lx;
         adj_prev[(size_t)(3 + k) * n + i] = lv + dt * lx;
         adj_prev[(size_t)(6 + k) * n + i] = lw;
-        lft[(size_t)k * n + i]            = dt / m * lv;
-        lft[(size_t)(3 + k) * n + i]      = dt * i1 * lw;
+        lft[(size_t)k * n + i]            = verlet ? h / m * (lv + dt * lx) : dt / m * lv;
+        lft[(size_t)(3 + k) * n + i]      = (verlet ? h : dt) * i1 * lw;
     }
 }
 

@@ -2051,6 +2051,14 @@ int gb_load_state(gb_ctx* c, const double* src)
     return GB_OK;
 }
 
+int gb_set_integrator_phase(gb_ctx* c, int32_t started)
+{
+    if(!c || (started != 0 && started != 1))
+        return GB_E_INVALID_ARG;
+    c->verlet_started = started != 0;
+    return GB_OK;
+}
+
 // A saved contact set: a 16-byte header (n, pair count as int64), the pair
 // offsets (n + 1 uint32), the partners (uint32 per pair), the contact flags
 // (one byte per pair).
@@ -2111,8 +2119,7 @@ int gb_adjoint_step(gb_ctx* c, const double* adj_next, double* adj_prev, double*
     if(!adj_next || !adj_prev || !grad_laws)
         return GB_E_INVALID_ARG;
     const int nl = c->nmat * (c->nmat + 1) / 2;
-    if(c->prec == GB_MIXED || c->cfg.contact_law != GB_LAW_HOOKE
-       || c->cfg.integrator != GB_FIRST_ORDER_EXPLICIT || nl > kAdjMaxLaws)
+    if(c->prec == GB_MIXED || c->cfg.contact_law != GB_LAW_HOOKE || nl > kAdjMaxLaws)
         return GB_E_UNSUPPORTED;
     for(const auto& rb : c->rbs)
         if(rb.convex.type != GB_SPHERE)
@@ -2164,7 +2171,10 @@ int gb_adjoint_step(gb_ctx* c, const double* adj_next, double* adj_prev, double*
     const auto*         in    = (const RBInertia<double>*)c->d_inertia;
     double*             lft   = c->d_adj;
     double*             part  = c->d_adj + 6 * (size_t)n;
-    k_adj_integrate<<<nb, kBlock, 0, s>>>(n, c->cfg.dt, state, in, adj_next, adj_prev, lft);
+    const bool   verlet = c->cfg.integrator == GB_VELOCITY_VERLET;
+    const double h      = verlet && !c->verlet_started ? 0.5 * c->cfg.dt : c->cfg.dt;
+    k_adj_integrate<<<nb, kBlock, 0, s>>>(n, c->cfg.dt, h, verlet ? 1 : 0, state, in, adj_next,
+                                          adj_prev, lft);
     k_adj_contacts<<<nb, kBlock, 0, s>>>(n, state, (const RBShape<double>*)c->d_shape, in,
                                          c->d_off[c->cur], c->d_pb[c->cur], c->d_pc, lft,
                                          c->d_obs_tr, (const RBShape<double>*)c->d_obs_shape,

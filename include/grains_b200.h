@@ -249,8 +249,14 @@ int gb_set_torces(gb_ctx* ctx, const double* torce);
  * (3), Transform3 basis (9, row-major), velocity (3), angular velocity (3). */
 int gb_save_state(gb_ctx* ctx, double* dst_device);
 int gb_load_state(gb_ctx* ctx, const double* src_device);
+/* GB_VELOCITY_VERLET: started = 0 makes the next step a trajectory's first
+ * (a half kick of the velocities, dt/2), 1 a later one (a full kick, dt).  A
+ * context starts at 0 and every step sets 1; a trajectory replayed from a
+ * saved state sets the phase it had there. */
+int gb_set_integrator_phase(gb_ctx* ctx, int32_t started);
 /* Reverse-mode derivative of one step from the current state s, for spheres,
- * GB_LAW_HOOKE with kr = 0, GB_FIRST_ORDER_EXPLICIT and Rectangle walls
+ * GB_LAW_HOOKE with kr = 0, GB_FIRST_ORDER_EXPLICIT or GB_VELOCITY_VERLET (the
+ * step's kick as gb_set_integrator_phase left it) and Rectangle walls
  * (GB_E_UNSUPPORTED otherwise).  adj_next = dL/ds' and adj_prev = dL/ds are
  * 9 rows of n doubles on the device (position, velocity, angular velocity);
  * dL/dtheta is added to grad_laws (device, 4 doubles per contact law: kn, en,

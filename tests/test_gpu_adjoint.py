@@ -48,10 +48,10 @@ def test_adjoint_step_matches_oracle(gb, oracle):
     assert (grad_o != 0).sum() >= 7  # both laws; the particle friction is capped
 
 
-def _loss_and_grads(scene, every, weights):
+def _loss_and_grads(scene, every, weights, **config):
     torch = _torch()
     from grains3dgpu_b200 import adjoint
-    sim = adjoint.Simulation(scene, precision=abi.GB_FP64)
+    sim = adjoint.Simulation(scene, precision=abi.GB_FP64, **config)
     x0 = torch.tensor(scene.transforms[:, 9:], device="cuda", requires_grad=True)
     v0 = torch.tensor(scene.velocities[:, :3], device="cuda", requires_grad=True)
     w0 = torch.tensor(scene.velocities[:, 3:], device="cuda", requires_grad=True)
@@ -71,20 +71,21 @@ def _weights(n):
     return [torch.tensor(rng.normal(size=(n, 3)), device="cuda") for _ in range(3)]
 
 
-def test_checkpoint_interval_does_not_change_gradients():
+@pytest.mark.parametrize("integrator", [abi.GB_FIRST_ORDER_EXPLICIT, abi.GB_VELOCITY_VERLET])
+def test_checkpoint_interval_does_not_change_gradients(integrator):
     scene = sphere_bed()
     wts = _weights(scene.n)
-    ref = _loss_and_grads(scene, T, wts)
+    ref = _loss_and_grads(scene, T, wts, integrator=integrator)
     for every in (1, 3):
-        out = _loss_and_grads(scene, every, wts)
+        out = _loss_and_grads(scene, every, wts, integrator=integrator)
         for a, b in zip(ref[1:], out[1:]):
             assert np.array_equal(a, b)
 
 
-def _fd_loss(lib, scene, weights):
+def _fd_loss(lib, scene, weights, **config):
     """the same loss from a plain forward run of `lib` (engine or oracle)"""
-    s = scenes.System(lib, scene, precision=abi.GB_FP64) if lib.prefix == "gb_" else \
-        scenes.System(lib, scene)
+    s = scenes.System(lib, scene, precision=abi.GB_FP64, **config) if lib.prefix == "gb_" else \
+        scenes.System(lib, scene, **config)
     s.step(T)
     tr, kin = s.transforms(), s.velocities()
     s.close()
@@ -105,34 +106,39 @@ def _perturbed(scene, law=None, name=None, h=0.0, dv=None, dx=None):
     return s
 
 
-@pytest.mark.parametrize("fd_lib", ["engine", "oracle"])
-def test_trajectory_gradient_vs_finite_differences(gb, oracle, fd_lib):
+@pytest.mark.parametrize("fd_lib,integrator", [
+    ("engine", abi.GB_FIRST_ORDER_EXPLICIT), ("oracle", abi.GB_FIRST_ORDER_EXPLICIT),
+    ("engine", abi.GB_VELOCITY_VERLET), ("oracle", abi.GB_VELOCITY_VERLET)])
+def test_trajectory_gradient_vs_finite_differences(gb, oracle, fd_lib, integrator):
     """Central differences of the engine's forward (GPU) and of the FP64 CPU
-    oracle's forward agree with the adjoint gradients to 1e-4."""
+    oracle's forward agree with the adjoint gradients to 1e-4, with
+    first-order explicit and with velocity-Verlet integration (whose first
+    step is the leapfrog's half kick)."""
     lib = gb if fd_lib == "engine" else oracle
     scene = sphere_bed()
     wts = _weights(scene.n)
-    _, gx, gv, gw, glaw = _loss_and_grads(scene, 3, wts)
+    cfg = {"integrator": integrator}
+    _, gx, gv, gw, glaw = _loss_and_grads(scene, 3, wts, **cfg)
     checked = 0
     for l in range(glaw.shape[0]):
         for k, name in enumerate(("kn", "en", "etat", "muc")):
             if glaw[l, k] == 0.0:
                 continue
             h = 1e-5 * abs(scene.contact_models[l][name])
-            fd = (_fd_loss(lib, _perturbed(scene, l, name, h), wts)
-                  - _fd_loss(lib, _perturbed(scene, l, name, -h), wts)) / (2 * h)
+            fd = (_fd_loss(lib, _perturbed(scene, l, name, h), wts, **cfg)
+                  - _fd_loss(lib, _perturbed(scene, l, name, -h), wts, **cfg)) / (2 * h)
             assert abs(glaw[l, k] - fd) <= 1e-4 * abs(fd), (l, name, glaw[l, k], fd)
             checked += 1
     assert checked == 8
     rng = np.random.default_rng(11)
     dv = rng.normal(size=(scene.n, 6))
     h = 1e-7
-    fd = (_fd_loss(lib, _perturbed(scene, dv=h * dv), wts)
-          - _fd_loss(lib, _perturbed(scene, dv=-h * dv), wts)) / (2 * h)
+    fd = (_fd_loss(lib, _perturbed(scene, dv=h * dv), wts, **cfg)
+          - _fd_loss(lib, _perturbed(scene, dv=-h * dv), wts, **cfg)) / (2 * h)
     ad = (gv * dv[:, :3]).sum() + (gw * dv[:, 3:]).sum()
     assert abs(ad - fd) <= 1e-4 * abs(fd)
     dx = rng.normal(size=(scene.n, 3))
     h = 1e-9
-    fd = (_fd_loss(lib, _perturbed(scene, dx=h * dx), wts)
-          - _fd_loss(lib, _perturbed(scene, dx=-h * dx), wts)) / (2 * h)
+    fd = (_fd_loss(lib, _perturbed(scene, dx=h * dx), wts, **cfg)
+          - _fd_loss(lib, _perturbed(scene, dx=-h * dx), wts, **cfg)) / (2 * h)
     assert abs((gx * dx).sum() - fd) <= 1e-4 * abs(fd)
