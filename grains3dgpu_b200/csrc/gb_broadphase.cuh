@@ -460,12 +460,27 @@ __global__ void __launch_bounds__(kBlock)
     const int64_t  base = (int64_t)tile * kTile + (int64_t)threadIdx.x * kItems;
     uint32_t       v[kItems];
     uint32_t       s = 0;
+    // a thread's kItems (8) consecutive entries in two 16-byte loads where
+    // they lie wholly in range and the arrays are 16-byte aligned
+    const bool vec = kItems == 8 && base + kItems <= n
+                     && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u)
+                            == 0;
+    if(vec)
+    {
+        const uint4 a = *reinterpret_cast<const uint4*>(in + base);
+        const uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+        v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+    else
+    {
+#pragma unroll
+        for(int j = 0; j < kItems; ++j)
+            v[j] = base + j < n ? in[base + j] : 0u;
+    }
 #pragma unroll
     for(int j = 0; j < kItems; ++j)
-    {
-        v[j] = base + j < n ? in[base + j] : 0u;
         s += v[j];
-    }
     uint32_t       agg;
     const uint32_t ex = block_excl_scan(s, &agg);
     // the first warp looks back over 32 predecessors at a time: lane l reads
@@ -534,6 +549,19 @@ __global__ void __launch_bounds__(kBlock)
     }
     __syncthreads();
     uint32_t run = s_prefix + ex;
+    if(vec)
+    {
+        uint32_t o[kItems];
+#pragma unroll
+        for(int j = 0; j < kItems; ++j)
+        {
+            o[j] = run;
+            run += v[j];
+        }
+        *reinterpret_cast<uint4*>(out + base)     = make_uint4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        return;
+    }
 #pragma unroll
     for(int j = 0; j < kItems; ++j)
         if(base + j < n)
