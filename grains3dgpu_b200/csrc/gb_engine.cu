@@ -162,6 +162,7 @@ struct gb_ctx
     uint32_t* d_slot   = nullptr; // kPairSlots candidates per particle (count pass)
     uint32_t* d_gjkq   = nullptr; // the step's pairs that need GJK (pair capacity; the
                                   // mixed mode: a second queue for its FP64 GJK after it)
+    uint32_t* d_obsq   = nullptr; // the step's obstacle records (pair capacity)
     uint32_t* d_gjkn   = nullptr; // their numbers (reset by the fill pass)
     uint32_t* d_ovf    = nullptr; // particles with more partners than pair slots
     uint32_t* d_pcount = nullptr; // contacts per particle of the step (cleared as read)
@@ -530,9 +531,9 @@ int alloc_state(gb_ctx* c)
     GB_TRY(dalloc(&c->d_flags, 1));
     GB_TRY(dalloc(&c->d_counters, 4));
     // [0], [1]: the GJK queues' lengths; [2], [3]: the fill pass's overflow
-    // counts, alternating by step
-    GB_TRY(dalloc(&c->d_gjkn, 4));
-    GB_CK(cudaMemset(c->d_gjkn, 0, 4 * sizeof(uint32_t)));
+    // counts and [4], [5] its obstacle-record counts, alternating by step
+    GB_TRY(dalloc(&c->d_gjkn, 6));
+    GB_CK(cudaMemset(c->d_gjkn, 0, 6 * sizeof(uint32_t)));
     GB_TRY(dalloc(&c->d_ovf, n));
     GB_TRY(dalloc(&c->d_pcount, n));
     GB_CK(cudaMemset(c->d_pcount, 0, (size_t)n * sizeof(uint32_t)));
@@ -594,6 +595,8 @@ int ensure_pairs(gb_ctx* c, int64_t need)
     dfree(c->d_info);
     dfree(c->d_gjkq);
     GB_TRY(dalloc(&c->d_gjkq, (c->prec == GB_MIXED ? 2 : 1) * ncap));
+    dfree(c->d_obsq);
+    GB_TRY(dalloc(&c->d_obsq, ncap));
     GB_TRY(dalloc(&c->d_pa, ncap));
     GB_CK(cudaMalloc(&c->d_pf, 9 * ncap * ss));
     GB_TRY(dalloc(&c->d_pc, ncap));
@@ -1109,7 +1112,7 @@ int build_pairs(gb_ctx* c)
     GB_CK(launch(c->pdl, k_pair_fill<S>, nb, kBlock, s, n, c->d_skeys, c->d_sids, c->d_sorted_of,
                  c->d_spos, spos32, c->d_cstart, c->dims[0], c->dims[1], c->dims[2], c->d_count,
                  c->d_slot, oc, off, c->d_pa, c->d_pb[c->cur], c->cap,
-                 c->d_flags, c->d_gjkn, c->d_count + n + 1, c->d_ovf, c->ovf_phase));
+                 c->d_flags, c->d_gjkn, c->d_count + n + 1, c->d_ovf, c->ovf_phase, c->d_obsq));
     c->count_zero = true; // the fill pass zeroes each count it reads
     GB_CK(launch(c->pdl, k_pair_fill_overflow<S>, 4 * c->sms, 128, s,
                  (const uint32_t*)c->d_gjkn + 2 + c->ovf_phase, (const uint32_t*)c->d_ovf,
@@ -1201,6 +1204,8 @@ int run_detect(gb_ctx* c, int phases)
         // The two kernels write disjoint records (particle pairs, obstacle
         // pairs); both are latency-bound on few warps, so they run side by
         // side, the obstacle one on the auxiliary stream.
+        // the fill pass's count of this step's obstacle records
+        const uint32_t* nobs_rec = c->d_gjkn + 4 + c->ovf_phase;
         auto with_variant = [&](auto var) -> int {
             constexpr int VAR = decltype(var)::value;
             cudaStream_t  so  = s;
@@ -1240,13 +1245,13 @@ int run_detect(gb_ctx* c, int phases)
             if(!c->obs_gjk)
                 k_narrow_obstacles<S, false, GB_GJK_JH>
                     <<<one_wave((const void*)k_narrow_obstacles<S, false, GB_GJK_JH>), 128, 0, so>>>(
-                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
-                    S(c->cfg.dt), c->d_counters);
+                    nobs_rec, c->d_obsq, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law,
+                    kr, S(c->cfg.dt), c->d_counters);
             else
                 k_narrow_obstacles<S, true, VAR>
                     <<<one_wave((const void*)k_narrow_obstacles<S, true, VAR>), 128, 0, so>>>(
-                    total, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
-                    S(c->cfg.dt), c->d_counters);
+                    nobs_rec, c->d_obsq, c->d_flags, c->d_pa, c->d_pb[c->cur], st, tb, po, law,
+                    kr, S(c->cfg.dt), c->d_counters);
             c->launches += 1;
             GB_CK(cudaEventRecord(c->ev_join, so));
             GB_CK(cudaStreamWaitEvent(s, c->ev_join, 0));
@@ -1621,7 +1626,7 @@ int gb_destroy(gb_ctx* c)
                     c->d_stage,     c->d_adj, c->d_tile_state, c->d_ticket, c->d_gjkq, c->d_gjkn,
                     c->d_fkey, c->d_fcount, c->d_fstart, c->d_fskey, c->d_fids, c->d_fref,
                     c->d_fpos, c->d_fpos32, c->d_ovf, c->d_pcount, c->d_cobs_start,
-                    c->d_cobs_ids};
+                    c->d_cobs_ids, c->d_obsq};
     for(void* p : ptrs)
         if(p)
             cudaFree(p);

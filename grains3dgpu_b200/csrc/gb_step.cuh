@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(kBlock)
                 const uint32_t* __restrict__ offset, uint32_t* __restrict__ pair_a,
                 uint32_t* __restrict__ pair_b, int64_t cap, int* __restrict__ flags,
                 uint32_t* __restrict__ gjk_count, uint32_t* __restrict__ pslot,
-                uint32_t* __restrict__ ovf_list, int ovf_phase)
+                uint32_t* __restrict__ ovf_list, int ovf_phase, uint32_t* __restrict__ obs_queue)
 {
     grid_dep_sync();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -894,11 +894,13 @@ __global__ void __launch_bounds__(kBlock)
     {
         // the narrow phase's GJK queues of this step start empty: [0] the
         // cull pass's, [1] the mixed mode's FP32 stage's; [2 + phase] counts
-        // this step's overflowing particles, [3 - phase] (last step's, read
-        // by its overflow pass) starts the next step at zero
+        // this step's overflowing particles and [4 + phase] its obstacle
+        // records, [3 - phase] and [5 - phase] (last step's, read by its
+        // overflow and obstacle passes) start the next step at zero
         gjk_count[0]             = 0;
         gjk_count[1]             = 0;
         gjk_count[3 - ovf_phase] = 0;
+        gjk_count[5 - ovf_phase] = 0;
     }
     if(a >= n || step_aborted(flags))
         return;
@@ -960,6 +962,15 @@ __global__ void __launch_bounds__(kBlock)
         // packing): k_pair_fill_overflow writes them, a warp per particle
         ovf_list[atomicAdd(gjk_count + 2 + ovf_phase, 1u)] = (uint32_t)a;
         out += cp;
+    }
+    // the particle's obstacle records, contiguous after its particle pairs,
+    // into the obstacle pass's queue
+    const uint32_t k_obs = c - cp;
+    if(k_obs)
+    {
+        const uint32_t q = atomicAdd(gjk_count + 4 + ovf_phase, k_obs);
+        for(uint32_t j = 0; j < k_obs; ++j)
+            obs_queue[q + j] = (uint32_t)out + j;
     }
     for_each_obstacle_candidate(oc, a, (uint32_t)s, [&](uint32_t o) {
         pair_a[out] = a;
@@ -1727,18 +1738,19 @@ struct StepParams
 // for both would run both code paths in every warp.
 template <typename S, bool GEN, int VAR>
 __global__ void __launch_bounds__(128)
-    k_narrow_obstacles(const uint32_t* __restrict__ total, const int* __restrict__ flags,
+    k_narrow_obstacles(const uint32_t* __restrict__ n_obs_records,
+                       const uint32_t* __restrict__ obs_queue, const int* __restrict__ flags,
                        const uint32_t* __restrict__ pair_a, const uint32_t* __restrict__ pair_b,
                        State<store_t<S>> st, Tables<S> tb, PairOut<store_t<S>> po, int law_kind,
                        int has_kr, S dt, unsigned long long* __restrict__ counters)
 {
     if(step_aborted(flags))
         return;
-    for_each_pair(*total, [&](int64_t p) {
-        const uint32_t b = pair_b[p];
-        if(b & kObstacleBit)
-            narrow_obstacle<S, GEN, VAR>(p, pair_a[p], (int)(b & ~kObstacleBit), st, tb, po,
-                                         law_kind, has_kr, dt, counters);
+    // the step's obstacle records, queued by the fill pass
+    for_each_pair(*n_obs_records, [&](int64_t q) {
+        const uint32_t p = obs_queue[q];
+        narrow_obstacle<S, GEN, VAR>(p, pair_a[p], (int)(pair_b[p] & ~kObstacleBit), st, tb, po,
+                                     law_kind, has_kr, dt, counters);
     });
 }
 
