@@ -127,6 +127,7 @@ struct gb_ctx
     double4* d_obs_plane = nullptr; // Rectangle planes: normal, normal . origin
     uint32_t obs_rect    = 0u;      // bit o: obstacle o (< 32) is a Rectangle
     bool     obs_gjk     = false;   // some obstacle is neither a Rectangle nor a drum
+    bool     poly_bodies = false;   // some rigid body is a polyhedron
     std::vector<double> obs_vel;    // 6 per obstacle: velocity, angular velocity
     double*  d_obs_vel   = nullptr;
     double*  d_rcirc64 = nullptr;
@@ -1234,9 +1235,24 @@ int run_detect(gb_ctx* c, int phases)
                 q64 = c->d_gjkq + c->cap;
                 n64 = c->d_gjkn + 1;
             }
-            GB_CK(launch(c->pdl, k_narrow_gjk<S, VAR>, one_wave((const void*)k_narrow_gjk<S, VAR>),
-                         128, s, n64, c->d_flags, q64, c->d_pa, c->d_pb[c->cur], st,
-                         tb, po, law, kr, S(c->cfg.dt), c->d_counters));
+            auto launch_gjk = [&](auto kernel) -> int {
+                GB_CK(launch(c->pdl, kernel, one_wave((const void*)kernel), 128, s, n64,
+                             c->d_flags, q64, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
+                             S(c->cfg.dt), c->d_counters));
+                return GB_OK;
+            };
+            // the mixed mode's FP64 GJK at three blocks per SM where no body
+            // is a polyhedron (bed of superquadrics: 1.584 -> 1.550 ms per
+            // step; 200k polyhedra: 0.199 -> 0.206 ms, so not there)
+            bool gjk_three = false;
+            if constexpr(is_mixed<S>())
+            {
+                gjk_three = !c->poly_bodies;
+                if(gjk_three)
+                    GB_TRY(launch_gjk(k_narrow_gjk<S, VAR, 3>));
+            }
+            if(!gjk_three)
+                GB_TRY(launch_gjk(k_narrow_gjk<S, VAR>));
             c->launches += 2;
             if(!c->nob)
                 return GB_OK;
@@ -1695,9 +1711,11 @@ int gb_set_rigid_bodies(gb_ctx* c, const gb_rigid_body_desc* rbs, const double* 
     c->verts.assign(vertices, vertices + 3 * n_vertices);
     c->props.resize(c->nrb);
     double rmax = 0.0;
+    c->poly_bodies = false;
     for(int i = 0; i < c->nrb; ++i)
     {
         const gb_convex& cv = rbs[i].convex;
+        c->poly_bodies = c->poly_bodies || cv.type == GB_POLYHEDRON;
         if(cv.type == GB_POLYHEDRON
            && (cv.first_vertex < 0 || cv.first_vertex + cv.n_vertices > n_vertices))
             return GB_E_INVALID_ARG;

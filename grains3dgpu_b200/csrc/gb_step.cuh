@@ -1670,9 +1670,12 @@ __global__ void __launch_bounds__(128)
 // One queued pair per lane pair (kGjkPaired: the two supports of a GJK
 // iteration in parallel); a short queue is spread over all warps as in
 // for_each_pair, a long one walked with a stride.  Both lanes of a pair take
-// the same path throughout, so their shuffles always meet.
-template <typename S, int VAR>
-__global__ void __launch_bounds__(128)
+// the same path throughout, so their shuffles always meet.  MIN_BLOCKS > 1
+// caps its registers for more resident warps (Johnson's tables and some
+// values spill to local memory): faster where the supports are closed forms
+// (superquadrics), slower where they loop over polyhedron vertices.
+template <typename S, int VAR, int MIN_BLOCKS = 1>
+__global__ void __launch_bounds__(128, MIN_BLOCKS)
     k_narrow_gjk(const uint32_t* __restrict__ gjk_count, const int* __restrict__ flags,
                  const uint32_t* __restrict__ gjk_queue, const uint32_t* __restrict__ pair_a,
                  const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
