@@ -1297,7 +1297,10 @@ GB_D bool gjk_first_iteration_separates(const Body<S>& A, const Body<S>& B, cons
 // Closest point to the origin of the segment (a, b) or the triangle (a, b, c)
 // (Ericson, Real-Time Collision Detection, 5.1.2 and 5.1.5, by Voronoi
 // regions), with the vertices of the feature it lies on put in y0..y(n-1).
-GB_D V3<float> closest_on_segment(const V3<float>& a, const V3<float>& b, V3<float>& y0,
+// The vertices come by value: the callers pass the simplex they overwrite
+// (with references, an edge (b, c) result read b after y1 = c had replaced
+// it and returned c instead of the edge's closest point).
+GB_D V3<float> closest_on_segment(const V3<float> a, const V3<float> b, V3<float>& y0,
                                   V3<float>& y1, int& n)
 {
     const V3<float> ab = b - a;
@@ -1321,7 +1324,7 @@ GB_D V3<float> closest_on_segment(const V3<float>& a, const V3<float>& b, V3<flo
     return a + (t / den) * ab;
 }
 
-GB_D V3<float> closest_on_triangle(const V3<float>& a, const V3<float>& b, const V3<float>& c,
+GB_D V3<float> closest_on_triangle(const V3<float> a, const V3<float> b, const V3<float> c,
                                    V3<float>& y0, V3<float>& y1, V3<float>& y2, int& n)
 {
     const V3<float> ab = b - a, ac = c - a;
