@@ -1235,24 +1235,28 @@ int run_detect(gb_ctx* c, int phases)
                 q64 = c->d_gjkq + c->cap;
                 n64 = c->d_gjkn + 1;
             }
-            auto launch_gjk = [&](auto kernel) -> int {
+            auto launch_gjk = [&](auto kernel, uint32_t lo, uint32_t hi) -> int {
                 GB_CK(launch(c->pdl, kernel, one_wave((const void*)kernel), 128, s, n64,
                              c->d_flags, q64, c->d_pa, c->d_pb[c->cur], st, tb, po, law, kr,
-                             S(c->cfg.dt), c->d_counters));
+                             S(c->cfg.dt), c->d_counters, lo, hi));
                 return GB_OK;
             };
-            // the mixed mode's FP64 GJK at three blocks per SM where no body
-            // is a polyhedron (bed of superquadrics: 1.584 -> 1.550 ms per
-            // step; 200k polyhedra: 0.199 -> 0.206 ms, so not there)
-            bool gjk_three = false;
+            // The mixed mode's FP64 GJK at three blocks per SM where no body
+            // is a polyhedron and the queue outnumbers the lane pairs of the
+            // default form's wave (1M bed, ~75k pairs: 1.584 -> 1.550 ms per
+            // step; 200k bed, ~15k pairs, one round either way: 0.424 ->
+            // 0.441 ms; 200k polyhedra: 0.199 -> 0.206 ms).  Both forms are
+            // launched; the queue length, on the device, picks the one that
+            // works.
+            uint32_t split = UINT32_MAX;
             if constexpr(is_mixed<S>())
-            {
-                gjk_three = !c->poly_bodies;
-                if(gjk_three)
-                    GB_TRY(launch_gjk(k_narrow_gjk<S, VAR, 3>));
-            }
-            if(!gjk_three)
-                GB_TRY(launch_gjk(k_narrow_gjk<S, VAR>));
+                if(!c->poly_bodies)
+                {
+                    split = (uint32_t)(one_wave((const void*)k_narrow_gjk<S, VAR>) * 128 / 2);
+                    GB_TRY(launch_gjk(k_narrow_gjk<S, VAR, 3>, split, UINT32_MAX));
+                    c->launches += 1;
+                }
+            GB_TRY(launch_gjk(k_narrow_gjk<S, VAR>, 0u, split));
             c->launches += 2;
             if(!c->nob)
                 return GB_OK;

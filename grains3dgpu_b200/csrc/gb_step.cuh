@@ -1676,19 +1676,26 @@ __global__ void __launch_bounds__(128)
 // the same path throughout, so their shuffles always meet.  MIN_BLOCKS > 1
 // caps its registers for more resident warps (Johnson's tables and some
 // values spill to local memory): faster where the supports are closed forms
-// (superquadrics), slower where they loop over polyhedron vertices.
+// (superquadrics) and the queue outnumbers the default's lane pairs, slower
+// where they loop over polyhedron vertices or one round takes the queue.
+// The launch does its work only for a queue length in [min_queue,
+// max_queue), read on the device, so that the host can launch both forms
+// and let the queue pick one.
 template <typename S, int VAR, int MIN_BLOCKS = 1>
 __global__ void __launch_bounds__(128, MIN_BLOCKS)
     k_narrow_gjk(const uint32_t* __restrict__ gjk_count, const int* __restrict__ flags,
                  const uint32_t* __restrict__ gjk_queue, const uint32_t* __restrict__ pair_a,
                  const uint32_t* __restrict__ pair_b, State<store_t<S>> st, Tables<S> tb,
                  PairOut<store_t<S>> po, int law_kind, int has_kr, S dt,
-                 unsigned long long* __restrict__ counters)
+                 unsigned long long* __restrict__ counters, uint32_t min_queue,
+                 uint32_t max_queue)
 {
     grid_dep_sync();
     if(step_aborted(flags))
         return;
     const int64_t nq     = *gjk_count;
+    if(nq < (int64_t)min_queue || nq >= (int64_t)max_queue)
+        return;
     const int64_t nslots = ((int64_t)gridDim.x * blockDim.x) >> 1;
     const int64_t slot   = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 1;
     auto          one    = [&](int64_t q) {
