@@ -822,7 +822,8 @@ LIMITER = {"integration": "issue and memory latency: 40% warps active (64 regist
            "pair_count": "memory latency of the neighbour walk on the finer grid: 17 "
                          "long-scoreboard stalls per issue at 46% warps active",
            "narrow": "FP32 issue in the cull (42% issue slots, 24 of 32 lanes, 96 registers) "
-                     "and FP64 GJK chains at 10% warps active (220 registers)"}
+                     "and FP64 GJK chains at 10-15% warps active (220 registers, 168 in "
+                     "its three-block form for long queues)"}
 
 
 def traffic_bytes(phase, n):
